@@ -1,0 +1,189 @@
+"""ASTC LDR block-compression search on one NVIDIA B200.
+
+Host-side mirror of Jure-Z/ASTC_implementation's encoder facade over the C-ABI
+library ``libastcb200.so`` (include/astcb200.h):
+
+    enc = ASTCEncoder(device=0)            # ASTCEncoder(const wgpu::Device&)   astc.h:726
+    enc.init()                             # ASTCEncoder::init()                 compression_pipeline.cpp:219
+    enc.secondaryInit(w, h, bx, by)        # ASTCEncoder::secondaryInit(...)     compression_pipeline.cpp:263
+    blocks = enc.encode(rgba8)             # ASTCEncoder::encode(data, out, len) compression_pipeline.cpp:323
+    store_image(bx, by, w, h, blocks, path)  # store_image(...)                 astc_store.cpp:18
+
+Errors are raised as ASTCError carrying the library's status code (the
+reference throws std::runtime_error).  The CUDA library is required: nothing
+here falls back to a CPU path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["ASTCEncoder", "ASTCError", "store_image", "decode", "load_library", "VALID_FOOTPRINTS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libastcb200.so")
+_lib = None
+
+VALID_FOOTPRINTS = [(4, 4), (5, 4), (5, 5), (6, 5), (6, 6), (8, 5), (8, 6), (10, 5), (10, 6),
+                    (8, 8), (10, 8), (10, 10), (12, 10), (12, 12)]
+
+OK, INVALID_FOOTPRINT, BAD_ARG, OOM, CUDA_ERROR, TIMEOUT, NO_IMAGE, IO_ERROR = range(8)
+
+
+class ASTCError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (status %d)" % (message, status))
+        self.status = status
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("chunk_blocks", ctypes.c_uint32),
+                ("timeout_ms", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ms_wall", ctypes.c_double), ("ms_device", ctypes.c_double), ("blocks", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+                ("launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def load_library():
+    """Loads libastcb200.so, building it first when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        from . import build as _build
+        _build.build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    P, U32, I32, SZ = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_size_t
+    sig = {
+        "astcb200_create": (I32, [ctypes.POINTER(P), I32, ctypes.POINTER(_Config)]),
+        "astcb200_destroy": (I32, [P]),
+        "astcb200_set_image": (I32, [P, U32, U32, ctypes.c_uint8, ctypes.c_uint8]),
+        "astcb200_blocks": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+        "astcb200_encode": (I32, [P, P, P, SZ, ctypes.POINTER(Stats)]),
+        "astcb200_encode_device": (I32, [P, P, P, P]),
+        "astcb200_encode_symbolic": (I32, [P, P, P, SZ]),
+        "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
+        "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
+        "astcb200_status_string": (ctypes.c_char_p, [I32]),
+        "astcb200_last_error": (ctypes.c_char_p, [P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    _lib = lib
+    return lib
+
+
+def _check(rc, ctx=None):
+    if rc != OK:
+        lib = load_library()
+        msg = lib.astcb200_status_string(rc).decode()
+        if ctx:
+            detail = lib.astcb200_last_error(ctx).decode()
+            if detail:
+                msg += ": " + detail
+        raise ASTCError(rc, msg)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class ASTCEncoder:
+    """One encoder context bound to one GPU and one CUDA stream."""
+
+    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0):
+        lib = load_library()
+        cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, 0)
+        ctx = ctypes.c_void_p()
+        _check(lib.astcb200_create(ctypes.byref(ctx), device, ctypes.byref(cfg)))
+        self._ctx = ctx
+        self.device = device
+        self.blocksX = self.blocksY = self.numBlocks = 0
+        self.textureWidth = self.textureHeight = 0
+        self.blockXDim = self.blockYDim = 4
+        self.is_initialized = False
+        self.last_stats = None
+
+    def init(self):
+        """Kernels are compiled ahead of time; kept for the reference's call sequence."""
+        self.is_initialized = True
+
+    def secondaryInit(self, textureWidth, textureHeight, blockXDim, blockYDim):
+        lib = load_library()
+        _check(lib.astcb200_set_image(self._ctx, textureWidth, textureHeight, blockXDim, blockYDim), self._ctx)
+        bx, by = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib.astcb200_blocks(self._ctx, ctypes.byref(bx), ctypes.byref(by)), self._ctx)
+        self.textureWidth, self.textureHeight = textureWidth, textureHeight
+        self.blockXDim, self.blockYDim = blockXDim, blockYDim
+        self.blocksX, self.blocksY = bx.value, by.value
+        self.numBlocks = bx.value * by.value
+
+    def _image(self, imageData):
+        img = np.ascontiguousarray(imageData, dtype=np.uint8)
+        if img.size != self.textureWidth * self.textureHeight * 4:
+            raise ASTCError(BAD_ARG, "image must hold width*height*4 bytes")
+        return img
+
+    def encode(self, imageData, dataOut=None):
+        """Encodes an RGBA8 image; returns (and fills dataOut with) numBlocks*16 bytes."""
+        lib = load_library()
+        img = self._image(imageData)
+        out = dataOut if dataOut is not None else np.empty(self.numBlocks * 16, np.uint8)
+        if not (isinstance(out, np.ndarray) and out.dtype == np.uint8 and out.flags.c_contiguous):
+            raise ASTCError(BAD_ARG, "dataOut must be a contiguous uint8 array")
+        st = Stats()
+        _check(lib.astcb200_encode(self._ctx, _ptr(img), _ptr(out), out.size, ctypes.byref(st)), self._ctx)
+        self.last_stats = st
+        return out
+
+    def encode_symbolic(self, imageData):
+        """Returns the chosen SymbolicBlock per block (astc.h:639-655) as (numBlocks, 108) u32."""
+        lib = load_library()
+        img = self._image(imageData)
+        sym = np.empty((self.numBlocks, 108), np.uint32)
+        _check(lib.astcb200_encode_symbolic(self._ctx, _ptr(img), _ptr(sym), sym.size), self._ctx)
+        return sym
+
+    def encode_device(self, d_rgba8, d_out_blocks, stream=0):
+        """Queues the search on device buffers (integer device addresses); does not wait."""
+        lib = load_library()
+        _check(lib.astcb200_encode_device(self._ctx, ctypes.c_void_p(d_rgba8), ctypes.c_void_p(d_out_blocks),
+                                          ctypes.c_void_p(stream or None)), self._ctx)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            load_library().astcb200_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def store_image(block_x, block_y, dim_x, dim_y, data, filename):
+    """Writes the .astc container (astc_store.cpp:18-62)."""
+    lib = load_library()
+    buf = np.ascontiguousarray(data, dtype=np.uint8)
+    _check(lib.astcb200_store_image(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, os.fsencode(filename)))
+
+
+def decode(block_x, block_y, dim_x, dim_y, blocks):
+    """Decodes physical ASTC blocks to an (dim_y, dim_x, 4) uint8 image."""
+    lib = load_library()
+    buf = np.ascontiguousarray(blocks, dtype=np.uint8)
+    out = np.empty((dim_y, dim_x, 4), np.uint8)
+    _check(lib.astcb200_decode(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, _ptr(out)))
+    return out
+
+
+def psnr(a, b):
+    """PSNR in dB over all RGBA channels of two uint8 images."""
+    d = a.astype(np.float64) - b.astype(np.float64)
+    mse = float(np.mean(d * d))
+    return float("inf") if mse == 0 else 10.0 * np.log10(255.0 * 255.0 / mse)

@@ -1,0 +1,269 @@
+// C-ABI of the encoder (include/astcb200.h): context, device buffers, the
+// chunked launch sequence and the .astc writer.
+//
+// Launch sequence per chunk of blocks, all on the context's stream:
+//   k_partition_search -> k_front -> k_refine -> k_select_pack
+// The per-chunk intermediates (partition picks, 13 partitioned-block records
+// and 104 candidate snapshots per block) stay in device memory and are reused
+// by every chunk; only the RGBA8 input and the 16-byte blocks cross PCIe.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "astcb200.h"
+#include "kernels.h"
+#include "tables.h"
+
+using namespace astcb200;
+
+struct astcb200_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    astcb200_config cfg{};
+    uint32_t width = 0, height = 0, bx = 0, by = 0, nbx = 0, nby = 0, nblocks = 0;
+    bool have_image = false;
+    TableLayout L{};
+    int tables_bx = 0, tables_by = 0;
+    uint8_t* d_tables = nullptr;
+    uint32_t chunk = 65536;
+    PartPicks* d_picks = nullptr;
+    PBRec* d_pbrec = nullptr;
+    Snap* d_snaps = nullptr;
+    uint8_t* d_img = nullptr;
+    size_t img_cap = 0;
+    uint8_t* d_out = nullptr;
+    size_t out_cap = 0;
+    uint32_t* d_sym = nullptr;
+    size_t sym_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int cuda_fail(astcb200_ctx* c, cudaError_t e, const char* what) {
+    if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? ASTCB200_OOM : ASTCB200_CUDA_ERROR;
+}
+#define CK(call, what)                                    \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+template <class T>
+int ensure(astcb200_ctx* ctx, T*& p, size_t& cap, size_t need, const char* what) {
+    if (cap >= need && p) return ASTCB200_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)&p, need);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    cap = need;
+    return ASTCB200_OK;
+}
+
+// Bounded host wait on the context's stream (astcb200_config.timeout_ms).
+int wait_stream(astcb200_ctx* ctx) {
+    if (ctx->cfg.timeout_ms == 0) {
+        CK(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+        return ASTCB200_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) return ASTCB200_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "cudaStreamQuery");
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > ctx->cfg.timeout_ms) { ctx->err = "device work did not finish within timeout_ms"; return ASTCB200_TIMEOUT; }
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
+int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t* d_sym, cudaStream_t s, uint32_t* launches) {
+    KernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.img = d_img;
+    a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
+    a.tables = ctx->d_tables;
+    a.L = ctx->L;
+    a.picks = ctx->d_picks; a.pbrec = ctx->d_pbrec; a.snaps = ctx->d_snaps;
+    a.out_blocks = d_out; a.symbolic = d_sym;
+    uint32_t n = 0;
+    for (uint32_t first = 0; first < ctx->nblocks; first += ctx->chunk) {
+        a.block_first = (int)first;
+        a.nblocks = (int)std::min<uint32_t>(ctx->chunk, ctx->nblocks - first);
+        CK(launch_partition_search(a, s), "k_partition_search");
+        CK(launch_front(a, s), "k_front");
+        CK(launch_refine(a, s), "k_refine");
+        CK(launch_select_pack(a, s), "k_select_pack");
+        n += 4;
+    }
+    if (launches) *launches = n;
+    return ASTCB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* astcb200_status_string(int s) {
+    switch (s) {
+        case ASTCB200_OK: return "ok";
+        case ASTCB200_INVALID_FOOTPRINT: return "invalid block footprint";
+        case ASTCB200_BAD_ARG: return "bad argument";
+        case ASTCB200_OOM: return "out of memory";
+        case ASTCB200_CUDA_ERROR: return "CUDA error";
+        case ASTCB200_TIMEOUT: return "timeout";
+        case ASTCB200_NO_IMAGE: return "no image configured";
+        case ASTCB200_IO_ERROR: return "file write failed";
+        default: return "unknown status";
+    }
+}
+
+const char* astcb200_last_error(const astcb200_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int astcb200_create(astcb200_ctx** out, int device_ordinal, const astcb200_config* cfg) {
+    if (!out) return ASTCB200_BAD_ARG;
+    *out = nullptr;
+    astcb200_ctx* ctx = new (std::nothrow) astcb200_ctx();
+    if (!ctx) return ASTCB200_OOM;
+    if (cfg && cfg->struct_size) {
+        std::memcpy(&ctx->cfg, cfg, std::min<size_t>(cfg->struct_size, sizeof(astcb200_config)));
+    }
+    ctx->chunk = ctx->cfg.chunk_blocks ? ctx->cfg.chunk_blocks : 65536;
+    ctx->device = device_ordinal;
+    int rc = ASTCB200_OK;
+    cudaError_t e = cudaSetDevice(device_ordinal);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "create"); astcb200_destroy(ctx); return rc; }
+    *out = ctx;
+    return ASTCB200_OK;
+}
+
+int astcb200_destroy(astcb200_ctx* ctx) {
+    if (!ctx) return ASTCB200_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_tables); cudaFree(ctx->d_picks); cudaFree(ctx->d_pbrec); cudaFree(ctx->d_snaps);
+    cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ASTCB200_OK;
+}
+
+int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8_t block_x, uint8_t block_y) {
+    if (!ctx || width == 0 || height == 0) return ASTCB200_BAD_ARG;
+    if (!valid_footprint(block_x, block_y)) return ASTCB200_INVALID_FOOTPRINT;
+    const uint64_t nbx = (width + block_x - 1) / block_x, nby = (height + block_y - 1) / block_y;
+    if (nbx * nby > 0x7FFFFFFFull) return ASTCB200_BAD_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (ctx->tables_bx != block_x || ctx->tables_by != block_y || !ctx->d_tables) {
+        std::vector<uint8_t> blob;
+        TableLayout L;
+        if (!build_tables(block_x, block_y, L, blob)) return ASTCB200_INVALID_FOOTPRINT;
+        if (ctx->d_tables) { cudaFree(ctx->d_tables); ctx->d_tables = nullptr; }
+        CK(cudaMalloc((void**)&ctx->d_tables, blob.size()), "cudaMalloc tables");
+        CK(cudaMemcpy(ctx->d_tables, blob.data(), blob.size(), cudaMemcpyHostToDevice), "upload tables");
+        CK(configure_kernels(L), "configure kernels");
+        ctx->L = L;
+        ctx->tables_bx = block_x; ctx->tables_by = block_y;
+    }
+    ctx->width = width; ctx->height = height; ctx->bx = block_x; ctx->by = block_y;
+    ctx->nbx = (uint32_t)nbx; ctx->nby = (uint32_t)nby; ctx->nblocks = (uint32_t)(nbx * nby);
+    const size_t chunk = std::min<size_t>(ctx->chunk, ctx->nblocks);
+    size_t cap_picks = 0, cap_rec = 0, cap_snap = 0;
+    if (ctx->d_picks) { cudaFree(ctx->d_picks); ctx->d_picks = nullptr; }
+    if (ctx->d_pbrec) { cudaFree(ctx->d_pbrec); ctx->d_pbrec = nullptr; }
+    if (ctx->d_snaps) { cudaFree(ctx->d_snaps); ctx->d_snaps = nullptr; }
+    int rc;
+    if ((rc = ensure(ctx, ctx->d_picks, cap_picks, chunk * sizeof(PartPicks), "cudaMalloc picks"))) return rc;
+    if ((rc = ensure(ctx, ctx->d_pbrec, cap_rec, chunk * kSlotsPerBlock * sizeof(PBRec), "cudaMalloc records"))) return rc;
+    if ((rc = ensure(ctx, ctx->d_snaps, cap_snap, chunk * kSlotsPerBlock * kNumCand * sizeof(Snap), "cudaMalloc snapshots"))) return rc;
+    ctx->have_image = true;
+    return ASTCB200_OK;
+}
+
+int astcb200_blocks(const astcb200_ctx* ctx, uint32_t* bxo, uint32_t* byo) {
+    if (!ctx || !bxo || !byo) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    *bxo = ctx->nbx; *byo = ctx->nby;
+    return ASTCB200_OK;
+}
+
+int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d_out, void* stream) {
+    if (!ctx || !d_rgba8 || !d_out) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    if (((uintptr_t)d_rgba8 & 3) || ((uintptr_t)d_out & 15)) return ASTCB200_BAD_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return run_search(ctx, d_rgba8, d_out, nullptr, s, nullptr);
+}
+
+static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks, uint32_t* symbolic, astcb200_stats* stats) {
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t in_bytes = (size_t)ctx->width * ctx->height * 4, out_bytes = (size_t)ctx->nblocks * 16;
+    int rc;
+    if ((rc = ensure(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
+    if ((rc = ensure(ctx, ctx->d_out, ctx->out_cap, out_bytes, "cudaMalloc output"))) return rc;
+    if (symbolic && (rc = ensure(ctx, ctx->d_sym, ctx->sym_cap, (size_t)ctx->nblocks * 108 * 4, "cudaMalloc symbolic"))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
+    CK(cudaEventRecord(ctx->ev0, ctx->stream), "event");
+    uint32_t launches = 0;
+    if ((rc = run_search(ctx, ctx->d_img, ctx->d_out, symbolic ? ctx->d_sym : nullptr, ctx->stream, &launches))) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
+    if (out_blocks) CK(cudaMemcpyAsync(out_blocks, ctx->d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H blocks");
+    if (symbolic) CK(cudaMemcpyAsync(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H symbolic");
+    if ((rc = wait_stream(ctx))) return rc;
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->ms_device = ms;
+        stats->ms_wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->blocks = ctx->nblocks;
+        stats->h2d_bytes = in_bytes;
+        stats->d2h_bytes = (out_blocks ? out_bytes : 0) + (symbolic ? (size_t)ctx->nblocks * 108 * 4 : 0);
+        stats->launches = launches;
+    }
+    return ASTCB200_OK;
+}
+
+int astcb200_encode(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks, size_t out_len, astcb200_stats* stats) {
+    if (!ctx || !rgba8 || !out_blocks) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    if (out_len < (size_t)ctx->nblocks * 16) return ASTCB200_BAD_ARG;
+    return encode_host(ctx, rgba8, out_blocks, nullptr, stats);
+}
+
+int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* symbolic, size_t words) {
+    if (!ctx || !rgba8 || !symbolic) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    if (words < (size_t)ctx->nblocks * 108) return ASTCB200_BAD_ARG;
+    return encode_host(ctx, rgba8, nullptr, symbolic, nullptr);
+}
+
+// astc_store.cpp:18-62: magic 0x5CA1AB13, block dims, 24-bit image dims, then the blocks.
+int astcb200_store_image(uint32_t bx, uint32_t by, uint32_t dx, uint32_t dy, const uint8_t* data, size_t len, const char* filename) {
+    if (!filename || (!data && len)) return ASTCB200_BAD_ARG;
+    const uint32_t bz = 1, dz = 1, magic = 0x5CA1AB13u;
+    uint8_t h[16] = {(uint8_t)(magic & 0xFF), (uint8_t)((magic >> 8) & 0xFF), (uint8_t)((magic >> 16) & 0xFF), (uint8_t)(magic >> 24),
+                     (uint8_t)bx, (uint8_t)by, (uint8_t)bz,
+                     (uint8_t)(dx & 0xFF), (uint8_t)((dx >> 8) & 0xFF), (uint8_t)((dx >> 16) & 0xFF),
+                     (uint8_t)(dy & 0xFF), (uint8_t)((dy >> 8) & 0xFF), (uint8_t)((dy >> 16) & 0xFF),
+                     (uint8_t)(dz & 0xFF), (uint8_t)((dz >> 8) & 0xFF), (uint8_t)((dz >> 16) & 0xFF)};
+    FILE* f = std::fopen(filename, "wb");
+    if (!f) return ASTCB200_IO_ERROR;
+    bool ok = std::fwrite(h, 1, 16, f) == 16 && (len == 0 || std::fwrite(data, 1, len, f) == len);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? ASTCB200_OK : ASTCB200_IO_ERROR;
+}
+
+}  // extern "C"

@@ -1,0 +1,752 @@
+// Refinement and final-selection kernels of the ASTC encoder (sm_100a).
+//
+//   k_refine       passes 13-17 (shaders/pass13..pass17), six iterations as
+//                  driven by compression_pipeline.cpp:473-484: least-squares
+//                  endpoints, colour endpoint packing (every LDR encoding the
+//                  reference tries), unpacking, weight realignment, final
+//                  error with a best-so-far snapshot.  One thread owns one
+//                  candidate for all six iterations; the 8 candidates of a
+//                  partitioned block share a CTA and its staged texels.
+//   k_select_pack  pass18 plus the host argmin over candidates and partition
+//                  counts (compression_pipeline.cpp:500-519), then the ASTC
+//                  physical block layout (code/physical_compression.cpp:843)
+//                  written straight to the 16-byte output block.
+#include "device_math.cuh"
+#include "kernels.h"
+
+namespace astcb200 {
+
+using namespace dev;
+
+namespace {
+
+constexpr float ERR_DEFAULT = 1e37f;
+__constant__ int c_levels_r[21] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256};
+
+enum {
+    FMT_LUMINANCE = 0, FMT_LUMINANCE_DELTA = 1, FMT_LUMINANCE_ALPHA = 4, FMT_LUMINANCE_ALPHA_DELTA = 5,
+    FMT_RGB_SCALE = 6, FMT_RGB = 8, FMT_RGB_DELTA = 9, FMT_RGB_SCALE_ALPHA = 10, FMT_RGBA = 12, FMT_RGBA_DELTA = 13
+};
+
+struct I4 { int32_t x, y, z, w; };
+__device__ __forceinline__ int32_t ic(const I4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+__device__ __forceinline__ I4 ivec(float4 v) { return {f2i(v.x), f2i(v.y), f2i(v.z), f2i(v.w)}; }
+__device__ __forceinline__ float4 rnev(float4 v) { return make_float4(rintf(v.x), rintf(v.y), rintf(v.z), rintf(v.w)); }
+__device__ __forceinline__ int32_t shl1(int32_t v) { return (int32_t)((uint32_t)v << 1); }
+
+// ------------------------------------------------------------ pass14 colour endpoint packing
+struct Packer {
+    const uint8_t* cu2u;  // [17][512]
+    __device__ int32_t tab(uint32_t q, int32_t idx) const { return cu2u[(q - 4) * 512 + idx]; }
+    __device__ float enc_err(float4 u0, float4 u1, I4 q0, I4 q1) const {
+        const float4 e0 = u0 - make_float4((float)q0.x, (float)q0.y, (float)q0.z, (float)q0.w);
+        const float4 e1 = u1 - make_float4((float)q1.x, (float)q1.y, (float)q1.z, (float)q1.w);
+        const float4 e = e0 * e0 + e1 * e1;
+        return ((e.x + e.y) + e.z) + e.w;
+    }
+    __device__ I4 q3int(uint32_t q, I4 v) const { return {tab(q, v.x * 2 + 1), tab(q, v.y * 2 + 1), tab(q, v.z * 2 + 1), 0}; }
+    __device__ int32_t qf1(uint32_t q, int32_t v, float vf) const { return tab(q, v * 2 + ((vf - (float)v) >= -0.1f ? 1 : 0)); }
+    __device__ I4 q3flt(uint32_t q, I4 v, float4 vf) const { return {qf1(q, v.x, vf.x), qf1(q, v.y, vf.y), qf1(q, v.z, vf.z), 0}; }
+    __device__ uint32_t qint(uint32_t q, int32_t v) const { return (uint32_t)tab(q, v * 2 + 1); }
+    __device__ uint32_t qflt(uint32_t q, int32_t v, float vf) const { return (uint32_t)qf1(q, v, vf); }
+
+    // bit_transfer_signed(&a, &b) (pass14:355-369)
+    __device__ static void bts(I4& a, I4& b) {
+        int32_t* pa = &a.x; int32_t* pb = &b.x;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t a0 = (uint32_t)pa[c], b0 = (uint32_t)pb[c];
+            int32_t na = (int32_t)((a0 >> 1) & 0x3F);
+            if (na & 0x20) na -= 0x40;
+            pb[c] = (int32_t)((b0 >> 1) | (a0 & 0x80));
+            pa[c] = na;
+        }
+    }
+    __device__ static I4 uncontract(I4 v) { return {(v.x + v.z) >> 1, (v.y + v.z) >> 1, v.z, v.w}; }
+    __device__ static int32_t clamp255(int32_t v) { return min(max(v, 0), 255); }
+    __device__ static void delta_unpack(I4 i0, I4 i1, I4& o0, I4& o1) {
+        bts(i1, i0);
+        const int32_t s = i1.x + i1.y + i1.z;
+        i1 = {i1.x + i0.x, i1.y + i0.y, i1.z + i0.z, i1.w + i0.w};
+        if (s < 0) { I4 t = uncontract(i0); i0 = uncontract(i1); i1 = t; }
+        o0 = {clamp255(i0.x), clamp255(i0.y), clamp255(i0.z), clamp255(i0.w)};
+        o1 = {clamp255(i1.x), clamp255(i1.y), clamp255(i1.z), clamp255(i1.w)};
+    }
+    __device__ static void rgba_unpack(I4 i0, I4 i1, I4& o0, I4& o1) {
+        if ((i0.x + i0.y + i0.z) > (i1.x + i1.y + i1.z)) { I4 t = uncontract(i0); i0 = uncontract(i1); i1 = t; }
+        o0 = i0; o1 = i1;
+    }
+    __device__ static bool out_of_range(float4 c) {
+        return c.x < 0.0f || c.x > 255.0f || c.y < 0.0f || c.y > 255.0f || c.z < 0.0f || c.z > 255.0f || c.w < 0.0f || c.w > 255.0f;
+    }
+    __device__ static float4 inv_bc(float4 c) { return make_float4((c.x + c.x) - c.z, (c.y + c.y) - c.z, (c.z + c.z) - c.z, (c.w + c.w) - c.w); }
+
+    // try_quantize_rgb_delta(_blue_contract) body after the optional inverse contraction
+    __device__ bool rgb_delta(float4 c0, float4 c1, I4& o0, I4& o1, uint32_t q, bool want_bc) const {
+        I4 c0a = ivec(rnev(c0));
+        c0a = {shl1(c0a.x), shl1(c0a.y), shl1(c0a.z), shl1(c0a.w)};
+        I4 c0b = {c0a.x & 0xFF, c0a.y & 0xFF, c0a.z & 0xFF, c0a.w & 0xFF};
+        const I4 c0be = q3int(q, c0b);
+        c0b = {c0be.x | (c0a.x & 0x100), c0be.y | (c0a.y & 0x100), c0be.z | (c0a.z & 0x100), c0be.w | (c0a.w & 0x100)};
+        I4 c1d = ivec(rnev(c1));
+        c1d = {shl1(c1d.x) - c0b.x, shl1(c1d.y) - c0b.y, shl1(c1d.z) - c0b.z, 0};
+        if (c1d.x > 63 || c1d.x < -64 || c1d.y > 63 || c1d.y < -64 || c1d.z > 63 || c1d.z < -64) return false;
+        c1d = {(c1d.x & 0x7F) | ((c0b.x & 0x100) >> 1), (c1d.y & 0x7F) | ((c0b.y & 0x100) >> 1),
+               (c1d.z & 0x7F) | ((c0b.z & 0x100) >> 1), (c1d.w & 0x7F) | ((c0b.w & 0x100) >> 1)};
+        const I4 c1de = q3int(q, c1d);
+        if (((c1d.x ^ c1de.x) & 0xC0) || ((c1d.y ^ c1de.y) & 0xC0) || ((c1d.z ^ c1de.z) & 0xC0)) return false;
+        I4 e0 = c0be, e1 = c1de;
+        bts(e1, e0);
+        const int32_t s = e1.x + e1.y + e1.z;
+        if (want_bc ? (s >= 0) : (s < 0)) return false;
+        e0 = {e0.x + e1.x, e0.y + e1.y, e0.z + e1.z, e0.w + e1.w};
+        if (e0.x < 0 || e0.x > 0xFF || e0.y < 0 || e0.y > 0xFF || e0.z < 0 || e0.z > 0xFF || e0.w < 0 || e0.w > 0xFF) return false;
+        o0 = c0be; o1 = c1de;
+        return true;
+    }
+    __device__ bool try_rgb_delta_bc(float4 a0, float4 a1, I4& o0, I4& o1, uint32_t q) const {
+        const float4 c0 = inv_bc(a1), c1 = inv_bc(a0);
+        if (out_of_range(c0) || out_of_range(c1)) return false;
+        return rgb_delta(c0, c1, o0, o1, q, true);
+    }
+    __device__ bool try_rgb_bc(float4 a0, float4 a1, I4& o0, I4& o1, uint32_t q) const {
+        const float4 c0 = inv_bc(a0), c1 = inv_bc(a1);
+        if (out_of_range(c0) || out_of_range(c1)) return false;
+        const I4 c0i = q3flt(q, ivec(rnev(c0)), c0), c1i = q3flt(q, ivec(rnev(c1)), c1);
+        if ((c1i.x + c1i.y + c1i.z) <= (c0i.x + c0i.y + c0i.z)) return false;
+        o0 = c1i; o1 = c0i;
+        return true;
+    }
+    __device__ void quant_rgb(float4 c0, float4 c1, I4& o0, I4& o1, uint32_t q) const {
+        I4 c0i, c1i;
+        const float4 nudge = mk(0.2f);
+        for (int it = 0; it < 4096; it++) {  // ends once c0 <= 0 and c1 >= 255 at the latest (< 1300 steps)
+            I4 c0q = ivec(rnev(c0));
+            c0q = {max(c0q.x, 0), max(c0q.y, 0), max(c0q.z, 0), max(c0q.w, 0)};
+            c0i = q3flt(q, c0q, c0);
+            c0 = c0 - nudge;
+            I4 c1q = ivec(rnev(c1));
+            c1q = {min(c1q.x, 255), min(c1q.y, 255), min(c1q.z, 255), min(c1q.w, 255)};
+            c1i = q3flt(q, c1q, c1);
+            c1 = c1 + nudge;
+            if ((c0i.x + c0i.y + c0i.z) <= (c1i.x + c1i.y + c1i.z)) break;
+        }
+        o0 = c0i; o1 = c1i;
+    }
+    __device__ bool try_alpha_delta(float4 color0, float4 color1, I4& o0, I4& o1, uint32_t q) const {
+        const int32_t a0a = shl1(f2i(rintf(color0.w)));
+        int32_t a0b = a0a & 0xFF;
+        const int32_t a0be = (int32_t)qint(q, a0b);
+        a0b = a0be | (a0a & 0x100);
+        int32_t a1d = shl1(f2i(rintf(color1.w))) - a0b;
+        if (a1d > 63 || a1d < -64) return false;
+        a1d = (a1d & 0x7F) | ((a0b & 0x100) >> 1);
+        const int32_t a1de = (int32_t)qint(q, a1d);
+        if (((a1d ^ a1de) & 0xC0) != 0) return false;
+        int32_t a1du = a1de & 0x7F;
+        if (a1du & 0x40) a1du -= 0x80;
+        a1du += a0b;
+        if (a1du < 0 || a1du > 0x1FF) return false;
+        o0.w = a0be; o1.w = a1de;
+        return true;
+    }
+    __device__ void quant_rgbs(float4 color, uint32_t* out, uint32_t q) const {
+        const float scale = 1.0f / 257.0f;
+        const float r = clampf(color.x * scale, 0.0f, 255.0f), g = clampf(color.y * scale, 0.0f, 255.0f), b = clampf(color.z * scale, 0.0f, 255.0f);
+        const uint32_t ri = qflt(q, f2i(rintf(r)), r), gi = qflt(q, f2i(rintf(g)), g), bi = qflt(q, f2i(rintf(b)), b);
+        const float oldsum = ((color.x + color.y) + color.z) * scale;
+        const float newsum = (float)(ri + gi + bi);
+        const float sa = clampf((color.w * (oldsum + 1e-10f)) / (newsum + 1e-10f), 0.0f, 1.0f);
+        const int32_t si = min(max(f2i(rintf(sa * 256.0f)), 0), 255);
+        out[0] = ri; out[1] = gi; out[2] = bi; out[3] = qint(q, si);
+    }
+    __device__ bool try_la_delta(float4 c0, float4 c1, uint32_t* out, uint32_t q) const {
+        const float l0 = ((c0.x + c0.y) + c0.z) / 3.0f, l1 = ((c1.x + c1.y) + c1.z) / 3.0f;
+        const int32_t l0a = shl1(f2i(rintf(l0))), a0a = shl1(f2i(rintf(c0.w)));
+        const uint32_t l0be = qint(q, l0a & 0xFF), a0be = qint(q, a0a & 0xFF);
+        const int32_t l0b = (int32_t)l0be | (l0a & 0x100), a0b = (int32_t)a0be | (a0a & 0x100);
+        int32_t l1d = shl1(f2i(rintf(l1))) - l0b, a1d = shl1(f2i(rintf(c1.w))) - a0b;
+        if (l1d > 63 || l1d < -64 || a1d > 63 || a1d < -64) return false;
+        l1d = (l1d & 0x7F) | ((l0b & 0x100) >> 1);
+        a1d = (a1d & 0x7F) | ((a0b & 0x100) >> 1);
+        const uint32_t l1de = qint(q, l1d), a1de = qint(q, a1d);
+        int32_t l1du = (int32_t)l1de, a1du = (int32_t)a1de;
+        if (((l1d ^ l1du) & 0xC0) != 0) return false;
+        if (((a1d ^ a1du) & 0xC0) != 0) return false;
+        l1du &= 0x7F; a1du &= 0x7F;
+        if (l1du & 0x40) l1du -= 0x80;
+        if (a1du & 0x40) a1du -= 0x80;
+        l1du += l0b; a1du += a0b;
+        if (l1du < 0 || l1du > 0x1FF || a1du < 0 || a1du > 0x1FF) return false;
+        out[0] = l0be; out[1] = l1de; out[2] = a0be; out[3] = a1de;
+        return true;
+    }
+    // pack_color_endpoints_helper (pass14:917-1224)
+    __device__ uint32_t pack(float4 color0, float4 color1, float4 rgbs, uint32_t fmt, uint32_t q, uint32_t* out) const {
+        const float4 c0 = vmin(vmax(color0, mk(0.0f)), mk(65535.0f)) / mk(257.0f);
+        const float4 c1 = vmin(vmax(color1, mk(0.0f)), mk(65535.0f)) / mk(257.0f);
+        float best = ERR_DEFAULT;
+#pragma unroll
+        for (int i = 0; i < 8; i++) out[i] = 0;
+        uint32_t bf = FMT_LUMINANCE;
+        if (fmt == FMT_RGB || fmt == FMT_RGBA) {
+            const bool rgba = fmt == FMT_RGBA;
+            const uint32_t dfmt = rgba ? FMT_RGBA_DELTA : FMT_RGB_DELTA;
+            I4 o0 = {0, 0, 0, 0}, o1 = {0, 0, 0, 0}, p0 = {0, 0, 0, 0}, p1 = {0, 0, 0, 0}, u0, u1;
+            if (q <= 18) {
+                bool ok = try_rgb_delta_bc(c0, c1, o0, o1, q);
+                if (rgba && ok) ok = try_alpha_delta(c1, c0, o0, o1, q);
+                if (ok) { delta_unpack(o0, o1, u0, u1); bf = dfmt; best = enc_err(c0, c1, u0, u1); }
+                ok = rgb_delta(c0, c1, p0, p1, q, false);
+                if (rgba && ok) ok = try_alpha_delta(c0, c1, p0, p1, q);
+                if (ok) {
+                    delta_unpack(p0, p1, u0, u1);
+                    const float e = enc_err(c0, c1, u0, u1);
+                    if (e < best) { best = e; bf = dfmt; o0 = p0; o1 = p1; }
+                }
+            }
+            if (q < 20 && try_rgb_bc(c0, c1, p0, p1, q)) {
+                if (rgba) { p0.w = (int32_t)qflt(q, f2i(rintf(c1.w)), c1.w); p1.w = (int32_t)qflt(q, f2i(rintf(c0.w)), c0.w); }
+                rgba_unpack(p0, p1, u0, u1);
+                const float e = enc_err(c0, c1, u0, u1);
+                if (e < best) { best = e; bf = fmt; o0 = p0; o1 = p1; }
+            }
+            {
+                quant_rgb(c0, c1, p0, p1, q);
+                if (rgba) { p0.w = (int32_t)qflt(q, f2i(rintf(c0.w)), c0.w); p1.w = (int32_t)qflt(q, f2i(rintf(c1.w)), c1.w); }
+                rgba_unpack(p0, p1, u0, u1);
+                const float e = enc_err(c0, c1, u0, u1);
+                if (e < best) { best = e; bf = fmt; o0 = p0; o1 = p1; }
+            }
+            out[0] = (uint32_t)o0.x; out[1] = (uint32_t)o1.x; out[2] = (uint32_t)o0.y;
+            out[3] = (uint32_t)o1.y; out[4] = (uint32_t)o0.z; out[5] = (uint32_t)o1.z;
+            if (rgba) { out[6] = (uint32_t)o0.w; out[7] = (uint32_t)o1.w; }
+        } else if (fmt == FMT_RGB_SCALE) {
+            quant_rgbs(rgbs, out, q); bf = FMT_RGB_SCALE;
+        } else if (fmt == FMT_RGB_SCALE_ALPHA) {
+            out[4] = qflt(q, f2i(rintf(c0.w)), c0.w); out[5] = qflt(q, f2i(rintf(c1.w)), c1.w);
+            quant_rgbs(rgbs, out, q); bf = FMT_RGB_SCALE_ALPHA;
+        } else if (fmt == FMT_LUMINANCE_ALPHA) {
+            if (q <= 18 && try_la_delta(c0, c1, out, q)) {
+                bf = FMT_LUMINANCE_ALPHA_DELTA;
+            } else {
+                const float l0 = ((c0.x + c0.y) + c0.z) / 3.0f, l1 = ((c1.x + c1.y) + c1.z) / 3.0f;
+                out[0] = qflt(q, f2i(rintf(l0)), l0); out[1] = qflt(q, f2i(rintf(l1)), l1);
+                out[2] = qflt(q, f2i(rintf(c0.w)), c0.w); out[3] = qflt(q, f2i(rintf(c1.w)), c1.w);
+                bf = FMT_LUMINANCE_ALPHA;
+            }
+        } else {  // FMT_LUMINANCE and any other format
+            float l0 = ((c0.x + c0.y) + c0.z) / 3.0f, l1 = ((c1.x + c1.y) + c1.z) / 3.0f;
+            if (l0 > l1) { const float av = (l0 + l1) * 0.5f; l0 = av; l1 = av; }
+            out[0] = qflt(q, f2i(rintf(l0)), l0); out[1] = qflt(q, f2i(rintf(l1)), l1);
+            bf = FMT_LUMINANCE;
+        }
+        return bf;
+    }
+};
+
+// pass15: decode packed endpoints of one partition, scaled by 257.
+__device__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, int32_t* e0, int32_t* e1) {
+    I4 o0, o1;
+    auto I = [&](int k) { return (int32_t)v[k]; };
+    switch (fmt) {
+        case FMT_LUMINANCE_DELTA: {
+            const int32_t l0 = (I(0) >> 2) | (I(1) & 0xC0), l1 = min(l0 + (I(1) & 0x3F), 255);
+            o0 = {l0, l0, l0, 255}; o1 = {l1, l1, l1, 255}; break;
+        }
+        case FMT_LUMINANCE_ALPHA: o0 = {I(0), I(0), I(0), I(2)}; o1 = {I(1), I(1), I(1), I(3)}; break;
+        case FMT_LUMINANCE_ALPHA_DELTA: {
+            int32_t l0 = I(0), l1 = I(1), a0 = I(2), a1 = I(3);
+            l0 |= (l1 & 0x80) << 1; a0 |= (a1 & 0x80) << 1;
+            l1 &= 0x7F; a1 &= 0x7F;
+            if (l1 & 0x40) l1 -= 0x80;
+            if (a1 & 0x40) a1 -= 0x80;
+            l0 >>= 1; l1 >>= 1; a0 >>= 1; a1 >>= 1;
+            l1 = min(max(l0 + l1, 0), 255); a1 = min(max(a0 + a1, 0), 255);
+            o0 = {l0, l0, l0, a0}; o1 = {l1, l1, l1, a1}; break;
+        }
+        case FMT_RGB_SCALE: {
+            const int32_t s = I(3);
+            o1 = {I(0), I(1), I(2), 255};
+            o0 = {(I(0) * s) >> 8, (I(1) * s) >> 8, (I(2) * s) >> 8, 255}; break;
+        }
+        case FMT_RGB_SCALE_ALPHA: {
+            const int32_t s = I(3);
+            o1 = {I(0), I(1), I(2), I(5)};
+            o0 = {(I(0) * s) >> 8, (I(1) * s) >> 8, (I(2) * s) >> 8, I(4)}; break;
+        }
+        case FMT_RGB: Packer::rgba_unpack({I(0), I(2), I(4), 0}, {I(1), I(3), I(5), 0}, o0, o1); o0.w = 255; o1.w = 255; break;
+        case FMT_RGB_DELTA: Packer::delta_unpack({I(0), I(2), I(4), 0}, {I(1), I(3), I(5), 0}, o0, o1); o0.w = 255; o1.w = 255; break;
+        case FMT_RGBA: Packer::rgba_unpack({I(0), I(2), I(4), I(6)}, {I(1), I(3), I(5), I(7)}, o0, o1); break;
+        case FMT_RGBA_DELTA: Packer::delta_unpack({I(0), I(2), I(4), I(6)}, {I(1), I(3), I(5), I(7)}, o0, o1); break;
+        default: o0 = {I(0), I(0), I(0), 255}; o1 = {I(1), I(1), I(1), 255}; break;
+    }
+    e0[0] = o0.x * 257; e0[1] = o0.y * 257; e0[2] = o0.z * 257; e0[3] = o0.w * 257;
+    e1[0] = o1.x * 257; e1[1] = o1.y * 257; e1[2] = o1.z * 257; e1[3] = o1.w * 257;
+}
+
+// ------------------------------------------------------------ k_refine
+constexpr int kRefinePBs = 16;
+constexpr int kRefineThreads = kRefinePBs * kNumCand;
+
+// Per-thread candidate state in shared memory.  Plain 4-byte members give the
+// struct an odd word stride (89 words), so a warp's threads hit distinct banks.
+struct CandSmem {
+    float e0[4][4], e1[4][4];
+    int32_t u0[4][4], u1[4][4];
+    uint8_t qw[64];
+    uint8_t packed[32];
+    uint32_t pad;
+};
+__device__ __forceinline__ float4 ld4(const float* p) { return make_float4(p[0], p[1], p[2], p[3]); }
+__device__ __forceinline__ void st4(float* p, float4 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w; }
+
+struct RTabs {
+    const uint8_t* b;
+    const TableLayout* L;
+    __device__ const DevDm& dm(int m) const { return reinterpret_cast<const DevDm*>(b + L->off_dm)[m]; }
+    __device__ const DevBm& bm(int i) const { return reinterpret_cast<const DevBm*>(b + L->off_bm)[i]; }
+    __device__ int tw_count(int m, int t) const { return b[L->off_tw_count + m * L->T + t]; }
+    __device__ int tw_start(int m, int t) const { return reinterpret_cast<const uint16_t*>(b + L->off_tw_start)[m * L->T + t]; }
+    __device__ int wt_count(int m, int w) const { return b[L->off_wt_count + m * 64 + w]; }
+    __device__ int wt_start(int m, int w) const { return reinterpret_cast<const uint16_t*>(b + L->off_wt_start)[m * 64 + w]; }
+    __device__ uint32_t t2w(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_t2w)[i]; }
+    __device__ uint32_t w2t(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_w2t)[i]; }
+    __device__ const uint8_t* part_texels(int P, int e) const { return b + L->off_part_texel + ((size_t)(P - 2) * 1024 + e) * L->T; }
+    __device__ int part_count(int P, int e, int q) const { return b[L->off_part_counts + ((P - 2) * 1024 + e) * 4 + q]; }
+    __device__ uint32_t prev_next(int q, int v) const { return reinterpret_cast<const uint16_t*>(b + L->off_prev_next)[q * 65 + v]; }
+};
+
+__device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const DevDm& d, const uint8_t* qw, int t, bool direct) {
+    if (direct) return (float)qw[t] / 64.0f;
+    const int n = tb.tw_count(dm, t), base = d.tw_base + tb.tw_start(dm, t);
+    float v = 0.0f;
+    for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + ((float)qw[e & 0xFF] / 64.0f) * ((float)(e >> 8) * (1.0f / 16.0f)); }
+    return v;
+}
+
+template <int P>
+__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, const float4* px, const uint8_t* tp,
+                                 CandSmem& cs, Snap* snap) {
+    const RTabs tb{a.tables, &a.L};
+    const int T = a.L.T;
+    const CandInit& ci = rec.c[k];
+    const DevBm bm = tb.bm(ci.bm);
+    const DevDm dmi = tb.dm(bm.dm);
+    const bool direct = dmi.W == T;
+    const float4 cw = chan_w();
+    const float lsw = (cw.x + cw.y) + cw.z;
+    const Packer pk{a.tables + a.L.off_cu2u};
+    float psz[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) psz[q] = P == 1 ? (q == 0 ? (float)T : 0.0f) : (float)tb.part_count(P, rec.entry, q);
+#pragma unroll
+    for (int q = 0; q < 4; q++) { st4(cs.e0[q], rec.ep0[q]); st4(cs.e1[q], rec.ep1[q]); }
+    for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
+    float top_err = ERR_DEFAULT;
+    uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
+    float4 rgbs[4];
+
+    auto final_error = [&]() {
+        float total = 0.0f;
+        for (int t = 0; t < T; t++) {
+            const int p = tp[t];
+            const float w = undec_weight(tb, bm.dm, dmi, cs.qw, t, direct);
+            const int32_t w1 = f2i(rintf(w * 64.0f)), w0 = 64 - w1;
+            const float4 x = px[t];
+            float4 d;
+            d.x = x.x - (float)(((cs.u0[p][0] * w0) + (cs.u1[p][0] * w1) + 32) >> 6);
+            d.y = x.y - (float)(((cs.u0[p][1] * w0) + (cs.u1[p][1] * w1) + 32) >> 6);
+            d.z = x.z - (float)(((cs.u0[p][2] * w0) + (cs.u1[p][2] * w1) + 32) >> 6);
+            d.w = x.w - (float)(((cs.u0[p][3] * w0) + (cs.u1[p][3] * w1) + 32) >> 6);
+            d = vmin(make_float4(fabsf(d.x), fabsf(d.y), fabsf(d.z), fabsf(d.w)), mk(1e15f));
+            total = total + fminf(dot4(d * d, cw), ERR_DEFAULT);
+        }
+        if (total < top_err) {
+            top_err = total;
+            snap->err = total; snap->bm = ci.bm; snap->final_q = (uint8_t)final_q; snap->matched = (uint8_t)matched;
+#pragma unroll
+            for (int q = 0; q < 4; q++) snap->ffmt[q] = (uint8_t)ffmt[q];
+            for (int i = 0; i < 32; i++) snap->packed[i] = cs.packed[i];
+            for (int i = 0; i < 64; i++) snap->qw[i] = cs.qw[i];
+        }
+    };
+
+    for (int it = 0; it < 6; it++) {
+        // ---------------- pass13: least-squares endpoints from the current weights
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            const float ps = psz[q];
+            const float4 rsum = (rec.avg[q] * ps) * cw;
+            const float4 rws = vmax(cw * ps, mk(1e-17f));
+            float4 sv = rsum / rws; sv.w = 0.0f;
+            const float4 sdir = normalize4(sv);
+            float wmin = 1.0f, wmax = 0.0f, ls = 0.0f, ms = 0.0f, rs = 0.0f, smin = 1e10f, smax = 0.0f, sv0 = 0.0f, sv1 = 0.0f;
+            float4 cx = mk(0.0f), cy = mk(0.0f);
+            for (int t = 0; t < T; t++) {
+                if (tp[t] != q) continue;
+                const float4 rgba = px[t];
+                const float w = undec_weight(tb, bm.dm, dmi, cs.qw, t, direct);
+                if (w < wmin) wmin = w;
+                if (w > wmax) wmax = w;
+                const float sc = dot3(rgba, sdir);
+                if (sc < smin) smin = sc;
+                if (sc > smax) smax = sc;
+                const float om = 1.0f - w;
+                ls = ls + om * om; ms = ms + om * w; rs = rs + w * w;
+                const float4 cyc = rgba * w;
+                cy = cy + cyc;
+                cx = cx + (rgba - cyc);
+                sv0 = sv0 + (om * sc) * lsw;
+                sv1 = sv1 + (w * sc) * lsw;
+            }
+            const float4 colx = cx * cw, coly = cy * cw;
+            const float4 lv = mk(ls) * cw, mv = mk(ms) * cw, rv = mk(rs) * cw;
+            const float lx = ls * lsw, my = ms * lsw, rz = rs * lsw;
+            const float scalediv = clampf(smin / fmaxf(smax, 1e-10f), 0.0f, 1.0f);
+            const float4 sds = sdir * smax;
+            rgbs[q] = make_float4(sds.x, sds.y, sds.z, scalediv);
+            if (wmin >= wmax * 0.999f) {
+                const float4 ac = (colx + coly) / vmax(cw * ps, mk(1e-17f));
+                float4 e0 = ld4(cs.e0[q]), e1 = ld4(cs.e1[q]);
+                if (ac.x == ac.x) { e0.x = ac.x; e1.x = ac.x; }
+                if (ac.y == ac.y) { e0.y = ac.y; e1.y = ac.y; }
+                if (ac.z == ac.z) { e0.z = ac.z; e1.z = ac.z; }
+                if (ac.w == ac.w) { e0.w = ac.w; e1.w = ac.w; }
+                st4(cs.e0[q], e0); st4(cs.e1[q], e1);
+                rgbs[q] = make_float4(sds.x, sds.y, sds.z, 1.0f);
+            } else {
+                const float4 det = (lv * rv) - (mv * mv);
+                const float4 rdet = mk(1.0f) / det;
+                const float lsdet = (lx * rz) - (my * my), lsrdet = 1.0f / lsdet;
+                const float4 mss = ((lv * lv) + mk(2.0f) * (mv * mv)) + (rv * rv);
+                const float lsmss = ((lx * lx) + 2.0f * (my * my)) + (rz * rz);
+                const float4 ne0 = ((rv * colx) - (mv * coly)) * rdet;
+                const float4 ne1 = ((lv * coly) - (mv * colx)) * rdet;
+                float4 e0 = ld4(cs.e0[q]), e1 = ld4(cs.e1[q]);
+                if (fabsf(det.x) > (mss.x * 1e-4f) && ne0.x == ne0.x && ne1.x == ne1.x) { e0.x = ne0.x; e1.x = ne1.x; }
+                if (fabsf(det.y) > (mss.y * 1e-4f) && ne0.y == ne0.y && ne1.y == ne1.y) { e0.y = ne0.y; e1.y = ne1.y; }
+                if (fabsf(det.z) > (mss.z * 1e-4f) && ne0.z == ne0.z && ne1.z == ne1.z) { e0.z = ne0.z; e1.z = ne1.z; }
+                if (fabsf(det.w) > (mss.w * 1e-4f) && ne0.w == ne0.w && ne1.w == ne1.w) { e0.w = ne0.w; e1.w = ne1.w; }
+                st4(cs.e0[q], e0); st4(cs.e1[q], e1);
+                const float se0 = ((rz * sv0) - (my * sv1)) * lsrdet;
+                const float se1 = ((lx * sv1) - (my * sv0)) * lsrdet;
+                if ((fabsf(lsdet) > (lsmss * 1e-4f)) && se0 == se0 && se1 == se1 && se0 < se1) {
+                    const float4 sdsm = sdir * se1;
+                    rgbs[q] = make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1);
+                }
+            }
+        }
+        // ---------------- pass14: pack at the trial quant level, then the "mod" level
+        {
+            bool all_same = ci.ql != ci.qlm;
+            uint32_t fn[4] = {0, 0, 0, 0}, vals[8];
+            for (int i = 0; i < 32; i++) cs.packed[i] = 0;
+#pragma unroll
+            for (int q = 0; q < P; q++) {
+                fn[q] = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), rgbs[q], ci.fmt[q], ci.ql, vals);
+#pragma unroll
+                for (int i = 0; i < 8; i++) cs.packed[q * 8 + i] = (uint8_t)vals[i];
+                if (q > 0) all_same = all_same && fn[q] == fn[0];
+            }
+            bool m = false;
+            if (P >= 2 && all_same) {
+                uint32_t fm[4] = {0, 0, 0, 0}, vm[32];
+                bool same_mod = true;
+#pragma unroll
+                for (int q = 0; q < P; q++) {
+                    if (!same_mod) break;
+                    fm[q] = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), rgbs[q], ci.fmt[q], ci.qlm, vals);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) vm[q * 8 + i] = vals[i];
+                    if (q > 0 && fm[q] != fm[0]) same_mod = false;
+                }
+                if (same_mod) {
+                    m = true;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) fn[q] = fm[q];
+                    for (int i = 0; i < 32; i++) cs.packed[i] = i < P * 8 ? (uint8_t)vm[i] : 0;
+                }
+            }
+            matched = m ? 1 : 0;
+            final_q = m ? ci.qlm : ci.ql;
+#pragma unroll
+            for (int q = 0; q < 4; q++) ffmt[q] = fn[q];
+        }
+        // ---------------- pass15
+#pragma unroll
+        for (int q = 0; q < P; q++) unpack_endpoints(ffmt[q], cs.packed + q * 8, cs.u0[q], cs.u1[q]);
+        if (it == 0) final_error();
+        // ---------------- pass16: move each weight one quant step if that lowers the error
+        if (direct) {
+            for (int t = 0; t < T; t++) {
+                const int p = tp[t];
+                const int32_t uqw = cs.qw[t];
+                const uint32_t pn = tb.prev_next(bm.quant, uqw);
+                const int32_t dn = pn & 0xFF, up = (pn >> 8) & 0xFF;
+                const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
+                const float4 offs = make_float4((float)(cs.u1[p][0] - cs.u0[p][0]), (float)(cs.u1[p][1] - cs.u0[p][1]),
+                                                (float)(cs.u1[p][2] - cs.u0[p][2]), (float)(cs.u1[p][3] - cs.u0[p][3])) * (1.0f / 64.0f);
+                const float4 cd = (base + offs * (float)uqw) - px[t];
+                const float4 cdd = cd + offs * (float)(dn - uqw), cdu = cd + offs * (float)(up - uqw);
+                const float eb = dot4(cd * cd, cw), ed = dot4(cdd * cdd, cw), eu = dot4(cdu * cdu, cw);
+                if ((eu < eb) && (eu < ed) && (uqw < 64)) cs.qw[t] = (uint8_t)up;
+                else if ((ed < eb) && (uqw > 0)) cs.qw[t] = (uint8_t)dn;
+            }
+        } else {
+            for (int we = 0; we < dmi.W; we++) {
+                const int32_t uqw = cs.qw[we];
+                const uint32_t pn = tb.prev_next(bm.quant, uqw);
+                const float dn = (float)(pn & 0xFF), up = (float)((pn >> 8) & 0xFF), ub = (float)uqw;
+                const float ddn = dn - ub, dup = up - ub;
+                float4 ebv = mk(0.0f), edv = mk(0.0f), euv = mk(0.0f);
+                const int nt = tb.wt_count(bm.dm, we), wbase = dmi.wt_base + tb.wt_start(bm.dm, we);
+                for (int te = 0; te < nt; te++) {
+                    const int t = tb.w2t(wbase + te) & 0xFF;
+                    const int n = tb.tw_count(bm.dm, t), tbase = dmi.tw_base + tb.tw_start(bm.dm, t);
+                    float wb = 0.0f, twb = 0.0f;
+                    bool found = false;
+                    for (int j = 0; j < n; j++) {
+                        const uint32_t e = tb.t2w(tbase + j);
+                        const float c = (float)(e >> 8) * (1.0f / 16.0f);
+                        wb = wb + (float)cs.qw[e & 0xFF] * c;
+                        if (!found && (int)(e & 0xFF) == we) { twb = c; found = true; }
+                    }
+                    const int p = tp[t];
+                    const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
+                    const float4 offs = make_float4((float)(cs.u1[p][0] - cs.u0[p][0]), (float)(cs.u1[p][1] - cs.u0[p][1]),
+                                                    (float)(cs.u1[p][2] - cs.u0[p][2]), (float)(cs.u1[p][3] - cs.u0[p][3])) * (1.0f / 64.0f);
+                    const float4 cd = (base + offs * wb) - px[t];
+                    const float4 cdd = cd + offs * (ddn * twb), cdu = cd + offs * (dup * twb);
+                    ebv = ebv + cd * cd; edv = edv + cdd * cdd; euv = euv + cdu * cdu;
+                }
+                const float eb = dot4(ebv, cw), ed = dot4(edv, cw), eu = dot4(euv, cw);
+                if ((eu < eb) && (eu < ed) && (uqw < 64)) cs.qw[we] = (uint8_t)up;
+                else if ((ed < eb) && (uqw > 0)) cs.qw[we] = (uint8_t)dn;
+            }
+        }
+        final_error();
+    }
+}
+
+__global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant__ KernelArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int T = a.L.T;
+    CandSmem* cs = reinterpret_cast<CandSmem*>(smem);
+    float4* pxs = reinterpret_cast<float4*>(smem + sizeof(CandSmem) * kRefineThreads);
+    uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefinePBs * T);
+    const int tid = threadIdx.x, pbl = tid / kNumCand, k = tid % kNumCand;
+    const int npb = a.nblocks * kSlotsPerBlock;
+    const int pb = blockIdx.x * kRefinePBs + pbl;
+    const bool live = pb < npb;
+    const PBRec* rec = live ? &a.pbrec[pb] : nullptr;
+    const int P = live ? (int)rec->P : 1;
+    const int ncand = live ? (int)rec->ncand : 0;
+    if (live && ncand > 0) {
+        const int blk = a.block_first + pb / kSlotsPerBlock;
+        const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + rec->entry) * T : nullptr;
+        const int bxi = blk % a.nbx, byi = blk / a.nbx;
+        for (int t = k; t < T; t += kNumCand) {
+            const int x = min(bxi * a.L.bx + t % a.L.bx, a.width - 1), y = min(byi * a.L.by + t / a.L.bx, a.height - 1);
+            const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
+            pxs[pbl * T + t] = make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
+                                           ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
+            tps[pbl * T + t] = P > 1 ? prow[t] : 0;
+        }
+    }
+    __syncthreads();
+    if (!live) return;
+    Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
+    snap->err = ERR_DEFAULT;  // inert slot unless refined below
+    if (k >= ncand) return;
+    const float4* px = pxs + pbl * T;
+    const uint8_t* tp = tps + pbl * T;
+    switch (P) {
+        case 1: refine_candidate<1>(a, *rec, k, px, tp, cs[tid], snap); break;
+        case 2: refine_candidate<2>(a, *rec, k, px, tp, cs[tid], snap); break;
+        case 3: refine_candidate<3>(a, *rec, k, px, tp, cs[tid], snap); break;
+        default: refine_candidate<4>(a, *rec, k, px, tp, cs[tid], snap); break;
+    }
+}
+
+// ------------------------------------------------------------ k_select_pack
+__device__ __forceinline__ void write_bits(uint32_t value, uint32_t count, uint32_t off, uint8_t* p) {
+    uint32_t mask = (1u << count) - 1;
+    value &= mask;
+    p += off >> 3;
+    off &= 7;
+    value <<= off; mask <<= off; mask = ~mask;
+    p[0] &= mask; p[0] |= value;
+    p[1] &= mask >> 8; p[1] |= value >> 8;
+}
+
+__device__ void btq(int q, int& bits, int& trits, int& quints) {
+    int L = c_levels_r[q];
+    trits = quints = 0;
+    if (L % 3 == 0) { trits = 1; L /= 3; } else if (L % 5 == 0) { quints = 1; L /= 5; }
+    bits = 0;
+    while ((1 << bits) < L) bits++;
+}
+__device__ uint32_t ise_bits(uint32_t n, int q) {
+    int b, t, qu; btq(q, b, t, qu);
+    if (t) return (n * (8 + 5 * b) + 4) / 5;
+    if (qu) return (n * (7 + 3 * b) + 2) / 3;
+    return n * b;
+}
+
+// encode_ise (code/physical_compression.cpp:672-826); out has 2 spare bytes.
+__device__ void encode_ise(const TableLayout& L, const uint8_t* tabs, int q, uint32_t n, const uint8_t* in, uint8_t* out, uint32_t off) {
+    int bits, trits, quints; btq(q, bits, trits, quints);
+    const uint32_t mask = (1u << bits) - 1;
+    const uint8_t* tt = tabs + L.off_trits;
+    const uint8_t* qt = tabs + L.off_quints;
+    if (trits) {
+        const uint8_t tb[5] = {2, 2, 1, 2, 1}, ts[5] = {0, 2, 4, 5, 7};
+        for (uint32_t i = 0; i < n; i += 5) {
+            uint32_t d[5];
+            for (int e = 0; e < 5; e++) d[e] = i + e < n ? (uint32_t)(in[i + e] >> bits) : 0;
+            const uint32_t T = tt[(((d[4] * 3 + d[3]) * 3 + d[2]) * 3 + d[1]) * 3 + d[0]];
+            for (int e = 0; e < 5 && i + e < n; e++) {
+                const uint32_t pack = (in[i + e] & mask) | (((T >> ts[e]) & ((1u << tb[e]) - 1)) << bits);
+                write_bits(pack, bits + tb[e], off, out);
+                off += bits + tb[e];
+            }
+        }
+    } else if (quints) {
+        const uint8_t qb[3] = {3, 2, 2}, qs[3] = {0, 3, 5};
+        for (uint32_t i = 0; i < n; i += 3) {
+            uint32_t d[3];
+            for (int e = 0; e < 3; e++) d[e] = i + e < n ? (uint32_t)(in[i + e] >> bits) : 0;
+            const uint32_t Q = qt[(d[2] * 5 + d[1]) * 5 + d[0]];
+            for (int e = 0; e < 3 && i + e < n; e++) {
+                const uint32_t pack = (in[i + e] & mask) | (((Q >> qs[e]) & ((1u << qb[e]) - 1)) << bits);
+                write_bits(pack, bits + qb[e], off, out);
+                off += bits + qb[e];
+            }
+        }
+    } else {
+        for (uint32_t i = 0; i < n; i++) { write_bits(in[i], bits, off, out); off += bits; }
+    }
+}
+
+__device__ __forceinline__ int bitrev8(int p) {
+    p = ((p & 0x0F) << 4) | ((p >> 4) & 0x0F);
+    p = ((p & 0x33) << 2) | ((p >> 2) & 0x33);
+    p = ((p & 0x55) << 1) | ((p >> 1) & 0x55);
+    return p;
+}
+
+__global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ KernelArgs a) {
+    const int lb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lb >= a.nblocks) return;
+    const int blk = a.block_first + lb;
+    float best = 1e30f;
+    int win_slot = -1, win_k = 0;
+    for (int s = 0; s < kSlotsPerBlock; s++) {
+        const PBRec& r = a.pbrec[(size_t)lb * kSlotsPerBlock + s];
+        const int n = r.ncand;
+        for (int k = 0; k < n; k++) {
+            const float e = a.snaps[((size_t)lb * kSlotsPerBlock + s) * kNumCand + k].err;
+            if (e < best) { best = e; win_slot = s; win_k = k; }
+        }
+    }
+    uint8_t blockbytes[18];
+    uint32_t sym[8 + 4 + 32];  // header words of the SymbolicBlock record
+    for (int i = 0; i < 18; i++) blockbytes[i] = 0;
+    for (int i = 0; i < 44; i++) sym[i] = 0;
+    const Snap* sn = nullptr;
+    const PBRec* rec = nullptr;
+    if (win_slot >= 0) {
+        rec = &a.pbrec[(size_t)lb * kSlotsPerBlock + win_slot];
+        sn = &a.snaps[((size_t)lb * kSlotsPerBlock + win_slot) * kNumCand + win_k];
+        const DevBm bm = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[sn->bm];
+        const DevDm dm = reinterpret_cast<const DevDm*>(a.tables + a.L.off_dm)[bm.dm];
+        const uint32_t pc = rec->P, q = bm.quant;
+        sym[0] = __float_as_uint(best); sym[1] = bm.mode_index; sym[2] = pc; sym[3] = rec->seed;
+        sym[4] = sn->matched; sym[5] = sn->final_q;
+        for (int i = 0; i < 4; i++) sym[8 + i] = sn->ffmt[i];
+        for (int i = 0; i < 32; i++) sym[12 + i] = sn->packed[i];
+        // weights: requantise 0..64 to the ISE alphabet, scramble, encode, bit-reverse
+        const uint8_t* wscr = a.tables + a.L.off_wscr + q * 32;
+        const float levels = (float)c_levels_r[q];
+        uint8_t wv[64], wbuf[18];
+        for (int i = 0; i < 18; i++) wbuf[i] = 0;
+        for (int i = 0; i < dm.W; i++) {
+            const float uqw = (float)sn->qw[i];
+            const float qw = (uqw / 64.0f) * (levels - 1.0f);
+            wv[i] = wscr[(int)(qw + 0.5f)];
+        }
+        const uint32_t wbits = ise_bits(dm.W, (int)q);
+        encode_ise(a.L, a.tables, (int)q, dm.W, wv, wbuf, 0);
+        for (int i = 0; i < 16; i++) blockbytes[i] = (uint8_t)bitrev8(wbuf[15 - i]);
+        write_bits(bm.mode_index, 11, 0, blockbytes);
+        write_bits(pc - 1, 2, 11, blockbytes);
+        if (pc > 1) {
+            write_bits(rec->seed, 6, 13, blockbytes);
+            write_bits(rec->seed >> 6, 4, 19, blockbytes);
+            if (sn->matched) {
+                write_bits((uint32_t)sn->ffmt[0] << 2, 6, 23, blockbytes);
+            } else {
+                int low = 4;
+                for (uint32_t i = 0; i < pc; i++) low = min((int)(sn->ffmt[i] >> 2), low);
+                if (low == 3) low = 2;
+                int et = low + 1, bp = 2;
+                for (uint32_t i = 0; i < pc; i++) { et |= ((int)(sn->ffmt[i] >> 2) - low) << bp; bp++; }
+                for (uint32_t i = 0; i < pc; i++) { et |= (int)(sn->ffmt[i] & 3) << bp; bp += 2; }
+                const int hs = 3 * (int)pc - 4;
+                write_bits(et & 0x3F, 6, 23, blockbytes);
+                write_bits((uint32_t)et >> 6, hs, 128 - wbits - hs, blockbytes);
+            }
+        } else {
+            write_bits(sn->ffmt[0], 4, 13, blockbytes);
+        }
+        const uint8_t* cscr = a.tables + a.L.off_cscr + (sn->final_q - 4) * 256;
+        uint8_t vals[32];
+        int nv = 0;
+        for (uint32_t i = 0; i < pc; i++) {
+            const int n = 2 * (sn->ffmt[i] >> 2) + 2;
+            for (int j = 0; j < n; j++) vals[nv + j] = cscr[sn->packed[i * 8 + j]];
+            nv += n;
+        }
+        encode_ise(a.L, a.tables, sn->final_q, nv, vals, blockbytes, pc == 1 ? 17 : 29);
+    }
+    uint4 o;
+    o.x = blockbytes[0] | (blockbytes[1] << 8) | (blockbytes[2] << 16) | ((uint32_t)blockbytes[3] << 24);
+    o.y = blockbytes[4] | (blockbytes[5] << 8) | (blockbytes[6] << 16) | ((uint32_t)blockbytes[7] << 24);
+    o.z = blockbytes[8] | (blockbytes[9] << 8) | (blockbytes[10] << 16) | ((uint32_t)blockbytes[11] << 24);
+    o.w = blockbytes[12] | (blockbytes[13] << 8) | (blockbytes[14] << 16) | ((uint32_t)blockbytes[15] << 24);
+    reinterpret_cast<uint4*>(a.out_blocks)[blk] = o;
+    if (a.symbolic) {
+        uint32_t* s = a.symbolic + (size_t)blk * 108;
+        if (win_slot < 0) sym[0] = __float_as_uint(1e30f);
+        for (int i = 0; i < 44; i++) s[i] = sym[i];
+        for (int i = 0; i < 64; i++) s[44 + i] = sn ? sn->qw[i] : 0;
+    }
+}
+
+}  // namespace
+
+size_t refine_smem_bytes(const TableLayout& L) {
+    return sizeof(CandSmem) * kRefineThreads + (size_t)kRefinePBs * L.T * 16 + (size_t)kRefinePBs * L.T;
+}
+
+cudaError_t configure_search_kernels(const TableLayout& L);
+
+cudaError_t configure_kernels(const TableLayout& L) {
+    cudaError_t e = configure_search_kernels(L);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)refine_smem_bytes(L));
+}
+
+cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
+    const int npb = a.nblocks * kSlotsPerBlock;
+    k_refine<<<(npb + kRefinePBs - 1) / kRefinePBs, kRefineThreads, refine_smem_bytes(a.L), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select_pack(const KernelArgs& a, cudaStream_t s) {
+    k_select_pack<<<(a.nblocks + 127) / 128, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace astcb200

@@ -1,0 +1,889 @@
+// Partition search and front-end kernels of the ASTC encoder (sm_100a).
+//
+//   k_partition_search  passes 001-007 (shaders/pass001..pass007): k-means over
+//                       the block's texels, coverage mismatch against every
+//                       selected partitioning, the reference's bitonic ordering,
+//                       error estimate of 128 candidates, pick of 4.
+//                       One warp per (block, partition count).
+//   k_front             passes 01-12 (shaders/pass01..pass12) for one
+//                       partitioned block per CTA: ideal endpoints, per
+//                       decimation-mode weight solving, per block-mode weight
+//                       quantisation error, colour-format search, top-8 pick.
+//
+// Sums whose order the reference leaves to float atomics are taken in ascending
+// texel / weight order by a single thread, so results are bit-identical to the
+// CPU oracle (oracle/astc_oracle.cpp), which fixes the same order.
+#include "device_math.cuh"
+#include "kernels.h"
+
+namespace astcb200 {
+
+using namespace dev;
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr float ERR_DEFAULT = 1e37f;
+__constant__ int c_levels[21] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256};
+__constant__ int c_steps_for_quant[12] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32};
+__constant__ int c_free_bits[4] = {111, 97, 94, 91};  // pass07:5
+
+enum { FMT_LUMINANCE = 0, FMT_LUMINANCE_ALPHA = 4, FMT_RGB_SCALE = 6, FMT_RGB = 8, FMT_RGB_SCALE_ALPHA = 10, FMT_RGBA = 12 };
+
+struct Tabs {
+    const uint8_t* b;
+    const TableLayout* L;
+    __device__ const DevDm& dm(int m) const { return reinterpret_cast<const DevDm*>(b + L->off_dm)[m]; }
+    __device__ const DevBm& bm(int i) const { return reinterpret_cast<const DevBm*>(b + L->off_bm)[i]; }
+    __device__ int tw_count(int m, int t) const { return b[L->off_tw_count + m * L->T + t]; }
+    __device__ int tw_start(int m, int t) const { return reinterpret_cast<const uint16_t*>(b + L->off_tw_start)[m * L->T + t]; }
+    __device__ int wt_count(int m, int w) const { return b[L->off_wt_count + m * 64 + w]; }
+    __device__ int wt_start(int m, int w) const { return reinterpret_cast<const uint16_t*>(b + L->off_wt_start)[m * 64 + w]; }
+    __device__ uint32_t t2w(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_t2w)[i]; }
+    __device__ uint32_t w2t(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_w2t)[i]; }
+    __device__ const uint8_t* part_texels(int P, int e) const { return b + L->off_part_texel + ((size_t)(P - 2) * 1024 + e) * L->T; }
+    __device__ int part_count(int P, int e, int q) const { return b[L->off_part_counts + ((P - 2) * 1024 + e) * 4 + q]; }
+    __device__ uint32_t part_seed(int P, int e) const { return reinterpret_cast<const uint32_t*>(b + L->off_part_info)[(P - 2) * 1024 + e]; }
+    __device__ uint64_t cov(int P, int e, int q) const { return reinterpret_cast<const uint64_t*>(b + L->off_cov)[((size_t)(P - 2) * 1024 + e) * 4 + q]; }
+    __device__ float sin_t(int i) const { return reinterpret_cast<const float*>(b + L->off_sin)[i]; }
+    __device__ float cos_t(int i) const { return reinterpret_cast<const float*>(b + L->off_cos)[i]; }
+    __device__ int q2u(int i) const { return b[L->off_q2u + i]; }
+    __device__ int q2u_start(int q) const { return b[L->off_q2u_start + q]; }
+    __device__ int qmt(int row, int bits) const { return reinterpret_cast<const int8_t*>(b + L->off_qmt)[row * 128 + bits]; }
+    __device__ float bqe(int i) const { return reinterpret_cast<const float*>(b + L->off_bqe)[i]; }
+};
+
+// Texel t of block blk, edge-clamped, as (v / 255) * 65536 (compression_pipeline.cpp:32-46).
+__device__ __forceinline__ float4 load_texel(const KernelArgs& a, int blk, int t) {
+    const int bx = a.L.bx, by = a.L.by;
+    const int bxi = blk % a.nbx, byi = blk / a.nbx;
+    const int x = min(bxi * bx + t % bx, a.width - 1);
+    const int y = min(byi * by + t / bx, a.height - 1);
+    const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
+    return make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
+                       ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
+}
+
+__device__ __forceinline__ float dist_sq(float4 a, float4 b) {
+    const float4 d = a - b;
+    return dot4(d * d, chan_w());
+}
+
+// ============================================================ passes 001-007
+constexpr int kSearchWarps = 4;
+constexpr int kSearchWarpBytes = 144 * 16 + 1024 * 8 + 128 * 4 * 2 + 160;
+
+template <int P>
+__device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, int lane) {
+    const Tabs tb{a.tables, &a.L};
+    const int T = a.L.T;
+    float4* px = reinterpret_cast<float4*>(ws);
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(ws + 144 * 16);
+    float* eu = reinterpret_cast<float*>(ws + 144 * 16 + 1024 * 8);
+    float* es = eu + 128;
+    uint8_t* asg = reinterpret_cast<uint8_t*>(es + 128);
+    for (int t = lane; t < T; t += 32) px[t] = load_texel(a, blk, t);
+    __syncwarp();
+
+    // pass001: farthest-point initial centres; ties pick the highest texel index
+    float4 c[P];
+    c[0] = px[145897 % T];
+    float dist[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) { const int t = lane + 32 * j; dist[j] = t < T ? dist_sq(c[0], px[t]) : 0.0f; }
+#pragma unroll
+    for (int pp = 1; pp < P; pp++) {
+        uint32_t mx = 0;
+#pragma unroll
+        for (int j = 0; j < 5; j++) if (lane + 32 * j < T) mx = max(mx, fbits(dist[j]));
+        mx = __reduce_max_sync(FULL, mx);
+        int idx = -1;
+#pragma unroll
+        for (int j = 0; j < 5; j++) if (lane + 32 * j < T && fbits(dist[j]) == mx) idx = lane + 32 * j;
+        idx = __reduce_max_sync(FULL, idx);
+        c[pp] = px[idx];
+        if (pp < P - 1) {
+#pragma unroll
+            for (int j = 0; j < 5; j++) { const int t = lane + 32 * j; if (t < T) dist[j] = fminf(dist[j], dist_sq(c[pp], px[t])); }
+        }
+    }
+    // passes 002/003, four iterations
+    uint32_t as[5];
+    for (int it = 0; it < 4; it++) {
+#pragma unroll
+        for (int j = 0; j < 5; j++) {
+            const int t = lane + 32 * j;
+            as[j] = 0;
+            if (t < T) {
+                float best = 1e30f;
+#pragma unroll
+                for (int q = 0; q < P; q++) { const float d = dist_sq(px[t], c[q]); if (d < best) { best = d; as[j] = q; } }
+            }
+        }
+        bool problem = false;
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            int n = 0;
+#pragma unroll
+            for (int j = 0; j < 5; j++) n += __popc(__ballot_sync(FULL, lane + 32 * j < T && as[j] == (uint32_t)q));
+            if (n == 0) problem = true;
+        }
+        if (problem && lane < P) as[0] = lane;
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            uint32_t n = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                const int t = lane + 32 * j;
+                if (t < T && as[j] == (uint32_t)q) {
+                    n++; s0 += f2u(px[t].x); s1 += f2u(px[t].y); s2 += f2u(px[t].z); s3 += f2u(px[t].w);
+                }
+            }
+            n = __reduce_add_sync(FULL, n);
+            s0 = __reduce_add_sync(FULL, s0); s1 = __reduce_add_sync(FULL, s1);
+            s2 = __reduce_add_sync(FULL, s2); s3 = __reduce_add_sync(FULL, s3);
+            if (n > 0) {
+                const float fc = (float)n;
+                c[q] = make_float4((float)s0 / fc, (float)s1 / fc, (float)s2 / fc, (float)s3 / fc);
+            } else {
+                c[q] = mk(0.0f);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 5; j++) { const int t = lane + 32 * j; if (t < T) asg[t] = (uint8_t)as[j]; }
+    __syncwarp();
+    // pass004: k-means bitmaps over the 64 k-means texels, mismatch per partitioning
+    uint64_t km[P];
+    {
+        const int k0 = asg[a.L.kmeans[lane]], k1 = asg[a.L.kmeans[lane + 32]];
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            const uint32_t lo = __ballot_sync(FULL, k0 == q), hi = __ballot_sync(FULL, k1 == q);
+            km[q] = (uint64_t)lo | ((uint64_t)hi << 32);
+        }
+    }
+    const uint32_t sel = a.L.count_selected[P - 1];
+    for (int i = lane; i < 1024; i += 32) {
+        uint32_t m = 0xFFFFFFFFu;
+        if ((uint32_t)i < sel) {
+            uint32_t p[P][P];
+#pragma unroll
+            for (int x = 0; x < P; x++)
+#pragma unroll
+                for (int y = 0; y < P; y++) p[x][y] = __popcll(km[x] ^ tb.cov(P, i, y));
+            if (P == 2) {
+                m = min(p[0][0] + p[1][1], p[0][1] + p[1][0]) / 2;
+            } else if (P == 3) {
+                const uint32_t v0 = min(p[1][1] + p[2][2], p[1][2] + p[2][1]) + p[0][0];
+                const uint32_t v1 = min(p[1][0] + p[2][2], p[1][2] + p[2][0]) + p[0][1];
+                const uint32_t v2 = min(p[1][0] + p[2][1], p[1][1] + p[2][0]) + p[0][2];
+                m = min(v0, min(v1, v2)) / 2;
+            } else {
+                const uint32_t mx23 = min(p[2][2] + p[3][3], p[2][3] + p[3][2]);
+                const uint32_t mx13 = min(p[2][1] + p[3][3], p[2][3] + p[3][1]);
+                const uint32_t mx12 = min(p[2][1] + p[3][2], p[2][2] + p[3][1]);
+                const uint32_t mx03 = min(p[2][0] + p[3][3], p[2][3] + p[3][0]);
+                const uint32_t mx02 = min(p[2][0] + p[3][2], p[2][2] + p[3][0]);
+                const uint32_t mx01 = min(p[2][1] + p[3][0], p[2][0] + p[3][1]);
+                const uint32_t v0 = p[0][0] + min(p[1][1] + mx23, min(p[1][2] + mx13, p[1][3] + mx12));
+                const uint32_t v1 = p[0][1] + min(p[1][0] + mx23, min(p[1][2] + mx03, p[1][3] + mx02));
+                const uint32_t v2 = p[0][2] + min(p[1][1] + mx03, min(p[1][0] + mx13, p[1][3] + mx01));
+                const uint32_t v3 = p[0][3] + min(p[1][1] + mx02, min(p[1][2] + mx01, p[1][0] + mx12));
+                m = min(v0, min(v1, min(v2, v3))) / 2;
+            }
+        }
+        key[i] = ((unsigned long long)m << 32) | (uint32_t)i;
+    }
+    __syncwarp();
+    // pass005: the reference's bitonic network run by 256 invocations (a partial sort)
+    for (unsigned k = 2; k <= 1024; k <<= 1)
+        for (unsigned j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const unsigned l = lane + 32 * r, partner = l ^ j;
+                if (partner > l) {
+                    const bool asc = (l & k) == 0;
+                    const unsigned long long x = key[l], y = key[partner];
+                    if ((x > y) == asc) { key[l] = y; key[partner] = x; }
+                }
+            }
+            __syncwarp();
+        }
+    // pass006: error estimate of the first 128 ordered partitionings.  The
+    // shader keeps avg/dir in per-invocation arrays, so texel t only sees its
+    // own partition's average/direction when t < P and its partition is t.
+    float wie = T <= 20 ? 0.03f : T <= 31 ? 0.04f : T <= 41 ? 0.05f : 0.055f;
+    wie = wie * wie;
+    const float4 cw = chan_w();
+    for (int r = 0; r < 4; r++) {
+        const int cand = lane + 32 * r;
+        const int e = (int)(uint32_t)key[cand];
+        const uint8_t* row = tb.part_texels(P, e);
+        uint32_t cnt[P], sm[P][4];
+#pragma unroll
+        for (int q = 0; q < P; q++) { cnt[q] = 0; sm[q][0] = sm[q][1] = sm[q][2] = sm[q][3] = 0; }
+        for (int t = 0; t < T; t++) {
+            const int p = row[t];
+            const float4 x = px[t];
+            const uint32_t u0 = f2u(x.x), u1 = f2u(x.y), u2 = f2u(x.z), u3 = f2u(x.w);
+#pragma unroll
+            for (int q = 0; q < P; q++) if (p == q) { cnt[q]++; sm[q][0] += u0; sm[q][1] += u1; sm[q][2] += u2; sm[q][3] += u3; }
+        }
+        float4 tavg[P], tdir[P];
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            const float fc = (float)cnt[q];
+            tavg[q] = fc > 0.0f ? make_float4((float)sm[q][0] / fc, (float)sm[q][1] / fc, (float)sm[q][2] / fc, (float)sm[q][3] / fc) : mk(0.0f);
+        }
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            uint32_t ax[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) ax[u][0] = ax[u][1] = ax[u][2] = ax[u][3] = 0;
+            for (int t = 0; t < T; t++) {
+                if (row[t] != q) continue;
+                const float4 av = (t == q) ? tavg[q] : mk(0.0f);
+                const float4 d = px[t] - av;
+                const uint32_t d0 = (uint32_t)f2i(d.x), d1 = (uint32_t)f2i(d.y), d2 = (uint32_t)f2i(d.z), d3 = (uint32_t)f2i(d.w);
+                if (d.x > 0.0f) { ax[0][0] += d0; ax[0][1] += d1; ax[0][2] += d2; ax[0][3] += d3; }
+                if (d.y > 0.0f) { ax[1][0] += d0; ax[1][1] += d1; ax[1][2] += d2; ax[1][3] += d3; }
+                if (d.z > 0.0f) { ax[2][0] += d0; ax[2][1] += d1; ax[2][2] += d2; ax[2][3] += d3; }
+                if (d.w > 0.0f) { ax[3][0] += d0; ax[3][1] += d1; ax[3][2] += d2; ax[3][3] += d3; }
+            }
+            float4 s[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) s[u] = make_float4((float)(int32_t)ax[u][0], (float)(int32_t)ax[u][1], (float)(int32_t)ax[u][2], (float)(int32_t)ax[u][3]);
+            float4 best = s[0];
+            float mp = dot4(s[0], s[0]);
+#pragma unroll
+            for (int u = 1; u < 4; u++) { const float pr = dot4(s[u], s[u]); if (pr > mp) { mp = pr; best = s[u]; } }
+            tdir[q] = normalize4(best);
+        }
+        uint32_t usum = 0, ssum = 0;
+        int32_t lmin[P], lmax[P];
+#pragma unroll
+        for (int q = 0; q < P; q++) { lmin[q] = 2147483647; lmax[q] = -2147483647; }
+        for (int t = 0; t < T; t++) {
+            const int p = row[t];
+            float4 av = mk(0.0f), ud = mk(0.0f);
+            if (t < P && p == t) {
+#pragma unroll
+                for (int q = 0; q < P; q++) if (q == t) { av = tavg[q]; ud = tdir[q]; }
+            }
+            const float4 x = px[t];
+            const float up = dot4(x, ud);
+            const float4 uproj = av + ud * dot4(x - av, ud);
+            const float4 udiff = x - uproj;
+            const float ud2 = dot4(udiff * udiff, cw);
+            const float4 sd = normalize4(av);
+            const float4 sproj = sd * dot4(x, sd);
+            const float4 sdiff = x - sproj;
+            const float sd2 = dot4(sdiff * sdiff, cw);
+            usum += f2u(ud2);
+            ssum += f2u(sd2);
+            const int32_t upi = f2i(up * 4096.0f);
+#pragma unroll
+            for (int q = 0; q < P; q++) if (p == q) { lmin[q] = min(lmin[q], upi); lmax[q] = max(lmax[q], upi); }
+        }
+        float tu = (float)usum, ts = (float)ssum;
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+            const float mn = (float)lmin[q] / 4096.0f, mxv = (float)lmax[q] / 4096.0f;
+            const float ll = fmaxf(mxv - mn, 1e-7f);
+            const float ew = (float)tb.part_count(P, e, q) * wie;
+            tu = tu + ew * (ll * ll);
+            const float4 a0 = q == 0 ? tavg[0] : mk(0.0f);
+            ts = ts + ew * dot4(a0, a0);
+        }
+        eu[cand] = tu;
+        es[cand] = ts;
+    }
+    __syncwarp();
+    // pass007: best 4 by each error, interleaved and deduplicated; the rank is
+    // used as the table entry (REF-BUG-4, pass007:93,156)
+    if (lane == 0) {
+        uint32_t bui[4] = {0, 0, 0, 0}, bsi[4] = {0, 0, 0, 0};
+        float bue[4] = {1e30f, 1e30f, 1e30f, 1e30f}, bse[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+        for (int i = 0; i < 128; i++) {
+            const float u = eu[i], s = es[i];
+            if (u < bue[3]) {
+                bue[3] = u; bui[3] = i;
+                for (int j = 3; j > 0; j--)
+                    if (bue[j] < bue[j - 1]) { float te = bue[j]; bue[j] = bue[j - 1]; bue[j - 1] = te; uint32_t ti = bui[j]; bui[j] = bui[j - 1]; bui[j - 1] = ti; }
+            }
+            if (s < bse[3]) {
+                bse[3] = s; bsi[3] = i;
+                for (int j = 3; j > 0; j--)
+                    if (bse[j] < bse[j - 1]) { float te = bse[j]; bse[j] = bse[j - 1]; bse[j - 1] = te; uint32_t ti = bsi[j]; bsi[j] = bsi[j - 1]; bsi[j - 1] = ti; }
+            }
+        }
+        uint32_t fin[4] = {0, 0, 0, 0};
+        int emitted = 0;
+        for (int i = 0; i < 8 && emitted < 4; i++) {
+            const uint32_t idx = (i & 1) ? bsi[i >> 1] : bui[i >> 1];
+            bool seen = false;
+            for (int j = 0; j < emitted; j++) seen |= fin[j] == idx;
+            if (!seen) fin[emitted++] = idx;
+        }
+        uint16_t* out = a.picks[lb].v + (P - 2) * 5;
+        for (int i = 0; i < 4; i++) out[i] = (uint16_t)fin[i];
+        out[4] = (uint16_t)emitted;
+    }
+}
+
+__global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __grid_constant__ KernelArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int item = blockIdx.x * kSearchWarps + warp;
+    if (item >= a.nblocks * 3) return;
+    const int lb = item / 3, P = item % 3 + 2;
+    uint8_t* ws = smem + warp * kSearchWarpBytes;
+    if (P == 2) search_one<2>(a, a.block_first + lb, lb, ws, lane);
+    else if (P == 3) search_one<3>(a, a.block_first + lb, lb, ws, lane);
+    else search_one<4>(a, a.block_first + lb, lb, ws, lane);
+}
+
+// ============================================================ passes 01-12
+constexpr int kFrontThreads = 64;
+
+struct FrontLayout {
+    int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, total;
+};
+constexpr int kScratchPerWarp = 144 * 4 + 64 * 4 + 16 * 4 + 16 * 20;
+
+struct FrontMisc {
+    float4 avg[4], dir[4], ep0[4], ep1[4];
+    float mn[4], mx[4], lsq[4];
+    float min_cutoff;
+    uint32_t is_const, gray, calpha;
+    float ece_rgb_scale[4], ece_lum[4], ece_alpha_drop[4];
+    uint32_t ece_can_offset[4], ece_can_bc[4];
+    float cerr[4][21][4];
+    uint8_t cfmt[4][21][4];
+    float combo_err[21][13];
+    uint8_t combo_fmt[21][13][4];
+    int top[kNumCand];
+    int ncand;
+};
+
+__host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
+__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm) {
+    FrontLayout f;
+    int o = 0;
+    f.px = take16(o, T * 16);
+    f.w = take16(o, T * 4);
+    f.wes = take16(o, T * 4);
+    f.tp = take16(o, T);
+    f.dec = take16(o, ndm * 64 * 4);
+    f.lo = take16(o, ndm * 8 * 4);
+    f.hi = take16(o, ndm * 8 * 4);
+    f.scratch = take16(o, 2 * kScratchPerWarp);
+    f.bm_err = take16(o, nbm * 4);
+    f.bm_bits = take16(o, nbm * 4);
+    f.ccr_tot = take16(o, nbm * 4);
+    f.ccr_q = take16(o, nbm * 2);
+    f.ccr_fmt = take16(o, nbm * 4);
+    f.qf = take16(o, 64 * kFrontThreads * 4);
+    f.misc = take16(o, (int)sizeof(FrontMisc));
+    f.total = o;
+    return f;
+}
+
+// Quantised weight w of block mode bmi given the dm's ideal decimated weights
+// (pass06 range rules + pass07:230-275).  Returns the unquantised value on the
+// 0..64 scale and writes the rescaled float weight.
+struct BmQuant {
+    float low, scale, slb, rscale, qlm1;
+    int q2u_start, quant;
+};
+__device__ __forceinline__ BmQuant bm_quant_setup(const Tabs& tb, const DevBm& bm, const float* lo, const float* hi, float min_cutoff) {
+    float low = lo[bm.quant < 8 ? bm.quant : 0], high = hi[bm.quant < 8 ? bm.quant : 0];
+    if (bm.quant >= 8) { low = 0.0f; high = 0.0f; }  // pass05 never writes slots 8..12 (REF-BUG-5 buffer read as 0)
+    if (high > 1.02f * min_cutoff) high = 1.0f;
+    if (high <= low) { low = 0.0f; high = 1.0f; }
+    BmQuant r;
+    r.qlm1 = (float)(c_levels[bm.quant] - 1);
+    float rscale = high - low;
+    r.scale = 1.0f / rscale;
+    r.slb = low * r.scale;
+    r.rscale = rscale / 64.0f;
+    r.low = low;
+    r.q2u_start = tb.q2u_start(bm.quant);
+    r.quant = bm.quant;
+    return r;
+}
+__device__ __forceinline__ int bm_quant_weight(const Tabs& tb, const BmQuant& s, float ideal, float* qf) {
+    const float ix = clampf(ideal * s.scale - s.slb, 0.0f, 1.0f);
+    const float ix1 = ix * s.qlm1;
+    const uint32_t wl = f2u(ix1), wh = min(wl + 1, f2u(s.qlm1));
+    const int li = tb.q2u(s.q2u_start + wl), hi = tb.q2u(s.q2u_start + wh);
+    const bool uh = ((float)li + (float)hi) < (128.0f * ix);
+    const int v = uh ? hi : li;
+    *qf = (float)v * s.rscale + s.low;
+    return v;
+}
+
+template <int P>
+__device__ void front_body(const KernelArgs& a, int lb, int slot_in_block, uint32_t entry, uint8_t* sm) {
+    const Tabs tb{a.tables, &a.L};
+    const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int blk = a.block_first + lb;
+    const FrontLayout fl = front_layout(T, ndm, nbm);
+    float4* px = reinterpret_cast<float4*>(sm + fl.px);
+    float* iw = reinterpret_cast<float*>(sm + fl.w);
+    float* wes = reinterpret_cast<float*>(sm + fl.wes);
+    uint8_t* tp = sm + fl.tp;
+    float* dec = reinterpret_cast<float*>(sm + fl.dec);
+    float* lov = reinterpret_cast<float*>(sm + fl.lo);
+    float* hiv = reinterpret_cast<float*>(sm + fl.hi);
+    float* bm_err = reinterpret_cast<float*>(sm + fl.bm_err);
+    int* bm_bits = reinterpret_cast<int*>(sm + fl.bm_bits);
+    float* ccr_tot = reinterpret_cast<float*>(sm + fl.ccr_tot);
+    uint8_t* ccr_q = sm + fl.ccr_q;
+    uint8_t* ccr_fmt = sm + fl.ccr_fmt;
+    float* qfs = reinterpret_cast<float*>(sm + fl.qf);
+    FrontMisc& M = *reinterpret_cast<FrontMisc*>(sm + fl.misc);
+    const float4 cw = chan_w();
+
+    const uint8_t* prow = P > 1 ? tb.part_texels(P, entry) : nullptr;
+    for (int t = tid; t < T; t += kFrontThreads) {
+        px[t] = load_texel(a, blk, t);
+        tp[t] = P > 1 ? prow[t] : 0;
+    }
+    __syncthreads();
+    {
+        bool gray = true, same_a = true;
+        for (int t = tid; t < T; t += kFrontThreads) {
+            gray = gray && px[t].x == px[t].y && px[t].x == px[t].z;
+            same_a = same_a && px[t].w == px[0].w;
+        }
+        gray = __syncthreads_and(gray);
+        same_a = __syncthreads_and(same_a);
+        if (tid == 0) { M.gray = gray; M.calpha = same_a; }
+    }
+    // ---------------- pass01: per-partition average, direction, projections
+    if (tid < 4) {
+        const int p = tid;
+        float4 sum = mk(0.0f);
+        float cnt = 0.0f;
+        for (int t = 0; t < T; t++) if (tp[t] == p) { sum = sum + px[t]; cnt = cnt + 1.0f; }
+        const float4 avg = cnt > 0.0f ? sum / mk(cnt) : mk(0.0f);
+        float4 d = mk(0.0f);
+        for (int t = 0; t < T; t++) if (tp[t] == p) { const float4 pd = vmax(px[t] - avg, mk(0.0f)); d = d + pd * pd; }
+        d = normalize4(d);
+        float mn = 1e10f, mx = -1e10f;
+        for (int t = 0; t < T; t++) if (tp[t] == p) { const float pr = dot4(px[t] - avg, d); mn = fminf(mn, pr); mx = fmaxf(mx, pr); }
+        if (mn >= mx) { mn = 0.0f; mx = 1e-7f; }
+        const float len = mx - mn;
+        M.lsq[p] = len * len;
+        M.mn[p] = mn; M.mx[p] = mx;
+        M.avg[p] = avg; M.dir[p] = d;
+        if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f && d.w == 0.0f) { M.ep0[p] = avg; M.ep1[p] = avg; }
+        else { M.ep0[p] = avg + d * mn; M.ep1[p] = avg + d * mx; }
+    }
+    __syncthreads();
+    const float ew = (((cw.x + cw.y) + cw.z) + cw.w) / 4.0f;
+    for (int t = tid; t < T; t += kFrontThreads) {
+        const int p = tp[t];
+        const float pr = dot4(px[t] - M.avg[p], M.dir[p]);
+        const float span = fmaxf(M.mx[p] - M.mn[p], 1e-6f);
+        iw[t] = clampf((pr - M.mn[p]) / span, 0.0f, 1.0f);
+        wes[t] = M.lsq[p] * ew;
+    }
+    if (tid == 0) {
+        bool ic = true;
+        for (int p = 1; p < 4; p++) ic = ic && M.lsq[p] == M.lsq[0];
+        M.is_const = ic;
+        float4 me = mk(10.0f);
+        for (int p = 0; p < 4; p++) {
+            const float4 ep = (mk(1.0f) - M.ep0[p]) / ((M.ep1[p] - M.ep0[p]) + mk(1e-9f));
+            if (ep.x > 0.5f && ep.x < me.x) me.x = ep.x;
+            if (ep.y > 0.5f && ep.y < me.y) me.y = ep.y;
+            if (ep.z > 0.5f && ep.z < me.z) me.z = ep.z;
+            if (ep.w > 0.5f && ep.w < me.w) me.w = ep.w;
+        }
+        M.min_cutoff = fminf(me.x, fminf(me.y, fminf(me.z, me.w)));
+    }
+    __syncthreads();
+    const bool is_const = M.is_const != 0;
+
+    // ---------------- passes 02-05, one warp per decimation mode
+    {
+        uint8_t* scr = sm + fl.scratch + warp * kScratchPerWarp;
+        float* inf = reinterpret_cast<float*>(scr);
+        uint32_t* smp = reinterpret_cast<uint32_t*>(scr + 144 * 4);
+        float* ang = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4);
+        float* lh = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4 + 16 * 4);  // [16][5]: lowest, span, err, cl, ch
+        for (int m = warp; m < ndm; m += kFrontThreads / 32) {
+            const DevDm dmi = tb.dm(m);
+            const int W = dmi.W;
+            float* dw = dec + m * 64;
+            if (W == T) {
+                for (int w = lane; w < W; w += 32) dw[w] = iw[w];
+            } else {
+                for (int w = lane; w < W; w += 32) {
+                    const int n = tb.wt_count(m, w);
+                    float v = 0.0f;
+                    if (n) {
+                        const int base = dmi.wt_base + tb.wt_start(m, w);
+                        float ws = 0.0f, tc = 1e-10f;
+                        for (int j = 0; j < n; j++) {
+                            const uint32_t e = tb.w2t(base + j);
+                            const int t = e & 0xFF;
+                            const float cwt = ((float)(e >> 8) * (1.0f / 16.0f)) * wes[is_const ? 0 : t];
+                            ws = ws + iw[t] * cwt;
+                            tc = tc + cwt;
+                        }
+                        v = ws / tc;
+                    }
+                    dw[w] = v;
+                }
+                __syncwarp();
+                for (int t = lane; t < T; t += 32) {
+                    const int n = tb.tw_count(m, t), base = dmi.tw_base + tb.tw_start(m, t);
+                    float v = 0.0f;
+                    for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + dw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+                    inf[t] = v;
+                }
+                __syncwarp();
+                for (int w = lane; w < W; w += 32) {
+                    const int n = tb.wt_count(m, w), base = dmi.wt_base + tb.wt_start(m, w);
+                    float e0 = 1e-10f, e1 = 0.0f;
+                    for (int j = 0; j < n; j++) {
+                        const uint32_t e = tb.w2t(base + j);
+                        const int t = e & 0xFF;
+                        const float c = (float)(e >> 8) * (1.0f / 16.0f);
+                        const float sc = wes[is_const ? 0 : t] * c;
+                        e0 = e0 + c * sc;
+                        e1 = e1 + (inf[t] - iw[t]) * sc;
+                    }
+                    dw[w] = dw[w] + clampf((e1 * -16.0f) / e0, -0.25f, 0.25f);
+                }
+            }
+            __syncwarp();
+            // pass03: angular offsets
+            for (int w = lane; w < W; w += 32) smp[w] = f2u(rintf(clampf(dw[w], 0.0f, 1.0f) * (1024.0f - 1.0f)));
+            __syncwarp();
+            if (lane < 16) {
+                float ax = 0.0f, ay = 0.0f;
+                for (int j = 0; j < W; j++) { const int k = smp[j] * 16 + lane; ax = ax + tb.cos_t(k); ay = ay + tb.sin_t(k); }
+                ang[lane] = atan2_search(ay, ax) * (1.0f / (2.0f * 3.14159265358979323846f));
+            }
+            __syncwarp();
+            // pass04: per angular step, rounding error and cut errors
+            const int S = dmi.max_angular_steps;
+            if (lane < S) {
+                float mnw = 3.4e38f, mxw = -3.4e38f;
+                for (int j = 0; j < W; j++) { const float v = dw[j]; if (v < mnw) mnw = v; if (v > mxw) mxw = v; }
+                const float rcp = (float)(lane + 1), off = ang[lane];
+                const float minidx = rintf(mnw * rcp - off), maxidx = rintf(mxw * rcp - off);
+                float ev = 0.0f, cl = 0.0f, ch = 0.0f;
+                for (int j = 0; j < W; j++) {
+                    const float sv = dw[j] * rcp - off, r = rintf(sv), d = sv - r;
+                    ev = ev + d * d;
+                    cl = cl + (r == minidx ? 1.0f - (2.0f * d) : 0.0f);
+                    ch = ch + (r == maxidx ? 1.0f + (2.0f * d) : 0.0f);
+                }
+                const int span = min(max(f2i((maxidx - minidx) + 1.0f), 2), (int)dmi.max_quant_steps + 3);
+                const float ss = 1.0f / rcp, esc = ss * ss;
+                float* o = lh + lane * 5;
+                o[0] = minidx; o[1] = __int_as_float(span); o[2] = ev * esc; o[3] = cl * esc; o[4] = ch * esc;
+            }
+            __syncwarp();
+            // pass05: best angular step per weight span, low/high value per quant level
+            if (lane == 0) {
+                float be[36], bi[36], bc[36];
+                const int nb = min((int)dmi.max_quant_steps + 4, 36);
+                for (int i = 0; i < nb; i++) { be[i] = 1e37f; bi[i] = -1.0f; bc[i] = 0.0f; }
+                for (int i = 0; i < S; i++) {
+                    const float* o = lh + i * 5;
+                    const int s = __float_as_int(o[1]);
+                    const float e = o[2], cl = o[3], ch = o[4];
+                    const float ecl = e + cl, ech = e + ch, eclh = (e + cl) + ch;
+                    const float fi = (float)i;
+                    if (e < be[s]) { be[s] = e; bi[s] = fi; bc[s] = 0.0f; }
+                    if (ecl < be[s - 1]) { be[s - 1] = ecl; bi[s - 1] = fi; bc[s - 1] = 1.0f; }
+                    if (ech < be[s - 1]) { be[s - 1] = ech; bi[s - 1] = fi; bc[s - 1] = 0.0f; }
+                    if (eclh < be[s - 2]) { be[s - 2] = eclh; bi[s - 2] = fi; bc[s - 2] = 1.0f; }
+                }
+                for (int q = 0; q < 8; q++) { lov[m * 8 + q] = 0.0f; hiv[m * 8 + q] = 0.0f; }
+                for (int q = 0; q <= dmi.max_quant_level; q++) {
+                    const int qs = c_steps_for_quant[q];
+                    const int bsi = max(f2i(bi[qs]), 0);
+                    const float lwi = lh[bsi * 5] + bc[qs];
+                    const float hwi = (lwi + (float)qs) - 1.0f;
+                    const float step = 1.0f / (1.0f + (float)bsi);
+                    const float off = ang[bsi];
+                    lov[m * 8 + q] = (off + lwi) * step;
+                    hiv[m * 8 + q] = (off + hwi) * step;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+
+    // ---------------- pass07: weight quantisation error per block mode
+    for (int i = tid; i < nbm; i += kFrontThreads) {
+        const DevBm bm = tb.bm(i);
+        const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+        if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
+        const DevDm dmi = tb.dm(bm.dm);
+        const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
+        const float* dw = dec + bm.dm * 64;
+        for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
+        float err = 0.0f;
+        for (int t = 0; t < T; t++) {
+            const int n = tb.tw_count(bm.dm, t), base = dmi.tw_base + tb.tw_start(bm.dm, t);
+            float v = 0.0f;
+            for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+            const float d = v - iw[t];
+            err = err + (d * d) * wes[is_const ? 0 : t];
+        }
+        bm_err[i] = err;
+        bm_bits[i] = bc;
+    }
+    // ---------------- pass08: encoding-choice errors per partition
+    if (tid < P) {
+        const int p = tid;
+        const float4 pavg = M.avg[p];
+        float4 sx = mk(0.0f), sy = mk(0.0f), sz = mk(0.0f);
+        for (int t = 0; t < T; t++) {
+            if (tp[t] != p) continue;
+            float4 d = px[t] - pavg;
+            d.w = 0.0f;
+            if (d.x > 0.0f) sx = sx + d;
+            if (d.y > 0.0f) sy = sy + d;
+            if (d.z > 0.0f) sz = sz + d;
+        }
+        const float pxx = dot4(sx, sx), pyy = dot4(sy, sy), pzz = dot4(sz, sz);
+        float4 bv = sx; float bs = pxx;
+        if (pyy > bs) { bv = sy; bs = pyy; }
+        if (pzz > bs) { bv = sz; bs = pzz; }
+        float4 avg = pavg; avg.w = 0.0f;
+        const float4 ub = normalize4(bv), ua = avg - ub * dot4(avg, ub);
+        const float4 sb = normalize4(avg);
+        const float4 lb = normalize4(make_float4(1.0f, 1.0f, 1.0f, 0.0f)), la = avg - lb * dot4(avg, lb);
+        float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f, acc4 = 0.0f;
+        for (int t = 0; t < T; t++) {
+            if (tp[t] != p) continue;
+            float4 rgb = px[t]; rgb.w = 0.0f;
+            const float ad = px[t].w - 65536.0f;
+            acc0 = acc0 + (ad * ad) * cw.w;
+            const float4 du = (ua + ub * dot3(rgb, ub)) - rgb;
+            acc1 = acc1 + dot3(du * du, cw);
+            const float4 ds = sb * dot3(rgb, sb) - rgb;
+            acc2 = acc2 + dot3(ds * ds, cw);
+            const float4 dl = (la + lb * dot3(rgb, lb)) - rgb;
+            acc3 = acc3 + dot3(dl * dl, cw);
+            const float4 dn = lb * dot3(rgb, lb) - rgb;
+            acc4 = acc4 + dot3(dn * dn, cw);
+        }
+        const float4 e0 = M.ep0[p], e1 = M.ep1[p];
+        const float lim = 0.12f * 65536.0f;
+        M.ece_can_offset[p] = fabsf(e1.x - e0.x) < lim && fabsf(e1.y - e0.y) < lim && fabsf(e1.z - e0.z) < lim;
+        M.ece_can_bc[p] = (M.gray && M.calpha) ? 0 : 1;
+        M.ece_rgb_scale[p] = (acc2 - acc1) * 0.7f;
+        M.ece_lum[p] = (acc4 - acc1) * 3.0f;
+        M.ece_alpha_drop[p] = acc0 * 3.0f;
+        // pass09: colour error per quant level and integer count
+        const float ps = (float)(P == 1 ? T : tb.part_count(P, entry, p));
+        const float4 e0h = vmax(e0 - mk(65535.0f), mk(0.0f)), e1h = vmax(e1 - mk(65535.0f), mk(0.0f));
+        const float4 e0l = vmin(e0, mk(0.0f)), e1l = vmin(e1, mk(0.0f));
+        const float4 sre = ((e0l * e0l + e1l * e1l) + e0h * e0h) + e1h * e1h;
+        const float rre = (dot3(sre, cw) * 0.5f) * ps;
+        const float are = ((sre.w * cw.w) * 0.5f) * ps;
+        const float brgb = ((cw.x + cw.y) + cw.z) * ps, ba = cw.w * ps;
+        const bool cbc = M.ece_can_bc[p] == 1, coe = M.ece_can_offset[p] == 1;
+        const float bcrgba = cbc ? 0.625f : 1.0f, oergba = coe ? 0.5f : 1.0f, bcrgb = cbc ? 0.5f : 1.0f, oergb = coe ? 0.25f : 1.0f;
+        const float rgbs_e = M.ece_rgb_scale[p], lum_e = M.ece_lum[p], ad_e = M.ece_alpha_drop[p];
+        for (int q = 0; q < 4; q++) {
+            for (int j = 0; j < 4; j++) M.cerr[p][q][j] = ERR_DEFAULT;
+            M.cfmt[p][q][0] = FMT_LUMINANCE; M.cfmt[p][q][1] = FMT_RGB_SCALE; M.cfmt[p][q][2] = FMT_RGB; M.cfmt[p][q][3] = FMT_RGBA;
+        }
+        for (int i = 0; i < 17; i++) {
+            const int q = i + 4;
+            const float orgba = q >= 19 ? 1.0f : oergba, orgb = q >= 19 ? 1.0f : oergb;
+            const float bq = tb.bqe(i);
+            const float qrgb = brgb * bq, qrgba = (brgb + ba) * bq;
+            M.cerr[p][q][3] = (((qrgba * bcrgba) * orgba) + rre) + are; M.cfmt[p][q][3] = FMT_RGBA;
+            const float full = (((qrgb * bcrgb) * orgb) + rre) + ad_e;
+            const float rgbsa = ((qrgba + rgbs_e) + rre) + are;
+            if (rgbsa < full) { M.cerr[p][q][2] = rgbsa; M.cfmt[p][q][2] = FMT_RGB_SCALE_ALPHA; }
+            else { M.cerr[p][q][2] = full; M.cfmt[p][q][2] = FMT_RGB; }
+            const float lrgbs = ((qrgb + rre) + ad_e) + rgbs_e;
+            const float la_e = ((qrgba + rre) + are) + lum_e;
+            if (lrgbs < la_e) { M.cerr[p][q][1] = lrgbs; M.cfmt[p][q][1] = FMT_RGB_SCALE; }
+            else { M.cerr[p][q][1] = la_e; M.cfmt[p][q][1] = FMT_LUMINANCE_ALPHA; }
+            M.cerr[p][q][0] = ((qrgb + rre) + ad_e) + lum_e; M.cfmt[p][q][0] = FMT_LUMINANCE;
+        }
+    }
+    __syncthreads();
+    // ---------------- pass10: best format combination per quant level and integer total
+    if (P > 1 && tid < 17) {
+        const int q = tid + 4;
+        const int NC = P == 2 ? 7 : P == 3 ? 10 : 13;
+        for (int c = 0; c < NC; c++) M.combo_err[q][c] = ERR_DEFAULT;
+        for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+                const int lo2 = min(i, j), hi2 = max(i, j);
+                if (hi2 - lo2 > 1) continue;
+                if (P == 2) {
+                    const float e = fminf(M.cerr[0][q][i] + M.cerr[1][q][j], 1e10f);
+                    if (e < M.combo_err[q][i + j]) {
+                        M.combo_err[q][i + j] = e;
+                        uint8_t* f = M.combo_fmt[q][i + j];
+                        f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = 0; f[3] = 0;
+                    }
+                    continue;
+                }
+                for (int k = 0; k < 4; k++) {
+                    const int lo3 = min(k, lo2), hi3 = max(k, hi2);
+                    if (hi3 - lo3 > 1) continue;
+                    if (P == 3) {
+                        const float e = fminf((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k], 1e10f);
+                        if (e < M.combo_err[q][i + j + k]) {
+                            M.combo_err[q][i + j + k] = e;
+                            uint8_t* f = M.combo_fmt[q][i + j + k];
+                            f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = M.cfmt[2][q][k]; f[3] = 0;
+                        }
+                        continue;
+                    }
+                    for (int l = 0; l < 4; l++) {
+                        const int lo4 = min(l, lo3), hi4 = max(l, hi3);
+                        if (hi4 - lo4 > 1) continue;
+                        const float e = fminf(((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k]) + M.cerr[3][q][l], 1e10f);
+                        if (e < M.combo_err[q][i + j + k + l]) {
+                            M.combo_err[q][i + j + k + l] = e;
+                            uint8_t* f = M.combo_fmt[q][i + j + k + l];
+                            f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = M.cfmt[2][q][k]; f[3] = M.cfmt[3][q][l];
+                        }
+                    }
+                }
+            }
+    }
+    __syncthreads();
+    // ---------------- pass11: best colour combination per block mode
+    for (int i = tid; i < nbm; i += kFrontThreads) {
+        const float werr = bm_err[i];
+        uint8_t* fm = ccr_fmt + i * 4;
+        if (werr >= ERR_DEFAULT) { ccr_tot[i] = ERR_DEFAULT; ccr_q[i * 2] = ccr_q[i * 2 + 1] = 0; fm[0] = fm[1] = fm[2] = fm[3] = 0; continue; }
+        const int bits = bm_bits[i];
+        int best_i = 0;
+        float best_e = ERR_DEFAULT;
+        if (P == 1) {
+            for (int ic = 1; ic <= 4; ic++) {
+                const int ql = tb.qmt(ic, bits);
+                if (ql < 4) continue;
+                const float e = M.cerr[0][ql][ic - 1];
+                if (e < best_e) { best_e = e; best_i = ic; }
+            }
+            const int fql = tb.qmt(best_i, bits);
+            fm[0] = fql >= 4 ? M.cfmt[0][fql][best_i - 1] : FMT_LUMINANCE;
+            fm[1] = fm[2] = fm[3] = 0;
+            ccr_q[i * 2] = ccr_q[i * 2 + 1] = (uint8_t)fql;
+        } else {
+            const int hi = P == 2 ? 8 : 9, modb = P == 2 ? 2 : P == 3 ? 5 : 8;
+            for (int ic = P; ic <= hi; ic++) {
+                const int ql = tb.qmt(ic, bits);
+                if (ql < 4) break;
+                const float e = M.combo_err[ql][ic - P];
+                if (e < best_e) { best_e = e; best_i = ic; }
+            }
+            const int fql = tb.qmt(best_i, bits), fqlm = tb.qmt(best_i, bits + modb);
+            for (int k = 0; k < 4; k++) fm[k] = fql >= 4 ? M.combo_fmt[fql][best_i - P][k] : 0;
+            ccr_q[i * 2] = (uint8_t)fql; ccr_q[i * 2 + 1] = (uint8_t)fqlm;
+        }
+        ccr_tot[i] = best_e + werr;
+    }
+    __syncthreads();
+    // ---------------- pass12: the 8 best trials (first minimum wins ties)
+    if (tid < kNumCand) M.top[tid] = -1;
+    __syncthreads();
+    for (int i = tid; i < nbm; i += kFrontThreads) {
+        const float e = ccr_tot[i];
+        if (!(e < ERR_DEFAULT)) continue;
+        int rank = 0;
+        for (int j = 0; j < nbm && rank < kNumCand; j++) {
+            const float f = ccr_tot[j];
+            if (f < ERR_DEFAULT && (f < e || (f == e && j < i))) rank++;
+        }
+        if (rank < kNumCand) M.top[rank] = i;
+    }
+    __syncthreads();
+    PBRec& rec = a.pbrec[(size_t)lb * kSlotsPerBlock + slot_in_block];
+    if (tid == 0) {
+        int n = 0;
+        while (n < kNumCand && M.top[n] >= 0) n++;
+        M.ncand = n;
+        rec.P = P; rec.entry = entry; rec.ncand = n;
+        rec.seed = P > 1 ? tb.part_seed(P, entry) : 0;
+    }
+    if (tid < 4) { rec.avg[tid] = M.avg[tid]; rec.ep0[tid] = M.ep0[tid]; rec.ep1[tid] = M.ep1[tid]; }
+    __syncthreads();
+    // candidate initial state: the trial's quantised weights (REF-BUG-6: only
+    // floor(W/4)*4 weights are packed by pass07, the rest read as 0)
+    const int ncand = M.ncand;
+    for (int k = tid >> 3; k < ncand; k += kFrontThreads / 8) {
+        const int i = M.top[k];
+        const DevBm bm = tb.bm(i);
+        const DevDm dmi = tb.dm(bm.dm);
+        CandInit& c = rec.c[k];
+        if ((tid & 7) == 0) {
+            c.bm = (uint16_t)i; c.ql = ccr_q[i * 2]; c.qlm = ccr_q[i * 2 + 1];
+            for (int f = 0; f < 4; f++) c.fmt[f] = ccr_fmt[i * 4 + f];
+        }
+        const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
+        const int packed_w = (dmi.W / 4) * 4;
+        for (int w = tid & 7; w < 64; w += 8) {
+            int v = 0;
+            if (w < packed_w) { float qf; v = bm_quant_weight(tb, s, dec[bm.dm * 64 + w], &qf); }
+            c.qw[w] = (uint8_t)v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__ KernelArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int slot = blockIdx.x;
+    const int lb = slot / kSlotsPerBlock, k = slot % kSlotsPerBlock;
+    if (lb >= a.nblocks) return;
+    if (k == 0) { front_body<1>(a, lb, 0, 0, smem); return; }
+    const int P = 2 + (k - 1) / 4, i = (k - 1) % 4;
+    const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
+    if (i >= pk[4]) {
+        if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * kSlotsPerBlock + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
+        return;
+    }
+    const uint32_t entry = pk[i];
+    if (P == 2) front_body<2>(a, lb, k, entry, smem);
+    else if (P == 3) front_body<3>(a, lb, k, entry, smem);
+    else front_body<4>(a, lb, k, entry, smem);
+}
+
+}  // namespace
+
+size_t search_smem_bytes(const TableLayout&) { return (size_t)kSearchWarps * kSearchWarpBytes; }
+size_t front_smem_bytes(const TableLayout& L) { return (size_t)front_layout(L.T, L.ndm, L.nbm).total; }
+
+cudaError_t configure_search_kernels(const TableLayout& L) {
+    cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem_bytes(L));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(L));
+}
+
+cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
+    const int items = a.nblocks * 3;
+    const int grid = (items + kSearchWarps - 1) / kSearchWarps;
+    k_partition_search<<<grid, kSearchWarps * 32, search_smem_bytes(a.L), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
+    k_front<<<a.nblocks * kSlotsPerBlock, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace astcb200

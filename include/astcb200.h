@@ -1,0 +1,95 @@
+/*
+ * astcb200 -- ASTC LDR block-compression search on one NVIDIA B200 (sm_100a).
+ *
+ * A drop-in for the GPU stage of Jure-Z/ASTC_implementation: the reference's
+ * ASTCEncoder facade (code/astc.h:724-733) driven by code/compression_pipeline.cpp
+ * and main.cpp, plus its .astc writer (code/astc_store.h:8-16).  Plain C types
+ * only; every call returns an astcb200_status code and no exception crosses
+ * this boundary.  One context per host thread; each context owns one CUDA
+ * stream and its device buffers.
+ */
+#ifndef ASTCB200_H
+#define ASTCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum astcb200_status {
+    ASTCB200_OK = 0,
+    ASTCB200_INVALID_FOOTPRINT = 1, /* not one of the 14 2D sizes of main.cpp:127-128 */
+    ASTCB200_BAD_ARG = 2,           /* null pointer, zero size, buffer too small */
+    ASTCB200_OOM = 3,               /* device or host allocation failed */
+    ASTCB200_CUDA_ERROR = 4,        /* a CUDA call failed; see astcb200_last_error */
+    ASTCB200_TIMEOUT = 5,           /* the host wait exceeded astcb200_config.timeout_ms */
+    ASTCB200_NO_IMAGE = 6,          /* astcb200_set_image has not been called */
+    ASTCB200_IO_ERROR = 7           /* astcb200_store_image could not write the file */
+} astcb200_status;
+
+typedef struct astcb200_ctx astcb200_ctx;
+
+typedef struct astcb200_config {
+    uint32_t struct_size;  /* sizeof(astcb200_config); 0 selects all defaults */
+    uint32_t chunk_blocks; /* blocks searched per launch sequence; 0 = 65536 */
+    uint32_t timeout_ms;   /* bound on each host wait for the device; 0 = no bound */
+    uint32_t reserved;
+} astcb200_config;
+
+typedef struct astcb200_stats {
+    double ms_wall;       /* host time of the call */
+    double ms_device;     /* device time of the search kernels (CUDA events) */
+    uint64_t blocks;      /* blocks encoded */
+    uint64_t h2d_bytes;   /* host-to-device bytes copied by the call */
+    uint64_t d2h_bytes;   /* device-to-host bytes copied by the call */
+    uint32_t launches;    /* kernels launched by the call */
+    uint32_t reserved;
+} astcb200_stats;
+
+/* Replaces ASTCEncoder::ASTCEncoder(device) + init() (compression_pipeline.cpp:200-233). */
+int astcb200_create(astcb200_ctx** out, int device_ordinal, const astcb200_config* cfg);
+/* Replaces ASTCEncoder::~ASTCEncoder (compression_pipeline.cpp:537). */
+int astcb200_destroy(astcb200_ctx* ctx);
+
+/* Replaces ASTCEncoder::secondaryInit(textureWidth, textureHeight, blockXDim, blockYDim)
+ * (compression_pipeline.cpp:263-321): builds the footprint's tables on the device. */
+int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8_t block_x, uint8_t block_y);
+/* ASTCEncoder::blocksX / blocksY (astc.h:736-737). */
+int astcb200_blocks(const astcb200_ctx* ctx, uint32_t* blocks_x, uint32_t* blocks_y);
+
+/* Replaces ASTCEncoder::encode(imageData, dataOut, dataLen) (compression_pipeline.cpp:323-535):
+ * rgba8 is width*height*4 bytes in host memory; out_blocks receives blocks_x*blocks_y*16
+ * bytes of physical ASTC blocks in raster order (out_len must be at least that). */
+int astcb200_encode(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks, size_t out_len,
+                    astcb200_stats* stats);
+
+/* Same search with both buffers already in device memory of the context's GPU; work is
+ * queued on cuda_stream (a cudaStream_t, or NULL for the context's stream) and the call
+ * returns without waiting.  d_rgba8 must be 4-byte aligned, d_out_blocks 16-byte aligned. */
+int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d_out_blocks, void* cuda_stream);
+
+/* Debug / parity hook: returns the chosen SymbolicBlock of every block in the reference
+ * layout (astc.h:639-655, 108 u32 per block) instead of physical blocks. */
+int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* symbolic, size_t symbolic_words);
+
+/* Replaces store_image(block_x, block_y, dim_x, dim_y, data, data_len, filename)
+ * (astc_store.cpp:18-62): 16-byte .astc header then the blocks. */
+int astcb200_store_image(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
+                         const uint8_t* data, size_t data_len, const char* filename);
+
+/* ASTC LDR decoder (no reference counterpart: the reference has none).  Decodes
+ * blocks_x*blocks_y blocks of an image of dim_x*dim_y texels into rgba8_out
+ * (dim_x*dim_y*4 bytes, UNORM8 with round-to-nearest from the 16-bit result). */
+int astcb200_decode(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
+                    const uint8_t* blocks, size_t blocks_len, uint8_t* rgba8_out);
+
+const char* astcb200_status_string(int status);
+const char* astcb200_last_error(const astcb200_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ASTCB200_H */
