@@ -38,7 +38,7 @@ class ASTCError(RuntimeError):
 
 class _Config(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("chunk_blocks", ctypes.c_uint32),
-                ("timeout_ms", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("timeout_ms", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
 
 
 class Stats(ctypes.Structure):
@@ -67,6 +67,8 @@ def load_library():
         "astcb200_encode_symbolic": (I32, [P, P, P, SZ]),
         "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
         "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
+        "astcb200_stage_times": (I32, [P, P, P]),
+        "astcb200_fp32_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double)]),
         "astcb200_status_string": (ctypes.c_char_p, [I32]),
         "astcb200_last_error": (ctypes.c_char_p, [P]),
     }
@@ -95,9 +97,9 @@ def _ptr(a):
 class ASTCEncoder:
     """One encoder context bound to one GPU and one CUDA stream."""
 
-    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0):
+    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False):
         lib = load_library()
-        cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, 0)
+        cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, 1 if stage_timing else 0)
         ctx = ctypes.c_void_p()
         _check(lib.astcb200_create(ctypes.byref(ctx), device, ctypes.byref(cfg)))
         self._ctx = ctx
@@ -154,6 +156,13 @@ class ASTCEncoder:
         _check(lib.astcb200_encode_device(self._ctx, ctypes.c_void_p(d_rgba8), ctypes.c_void_p(d_out_blocks),
                                           ctypes.c_void_p(stream or None)), self._ctx)
 
+    def stage_times(self):
+        """(ms[4], launches[4]) per kernel for the last encode (needs stage_timing=True)."""
+        ms = np.zeros(4, np.float32)
+        n = np.zeros(4, np.uint32)
+        _check(load_library().astcb200_stage_times(self._ctx, _ptr(ms), _ptr(n)), self._ctx)
+        return ms, n
+
     def close(self):
         if getattr(self, "_ctx", None):
             load_library().astcb200_destroy(self._ctx)
@@ -180,6 +189,13 @@ def decode(block_x, block_y, dim_x, dim_y, blocks):
     out = np.empty((dim_y, dim_x, 4), np.uint8)
     _check(lib.astcb200_decode(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, _ptr(out)))
     return out
+
+
+def fp32_peak_tflops(device=0):
+    """FP32 FMA throughput of the device in TFLOP/s (dependent-FMA microbenchmark)."""
+    t = ctypes.c_double()
+    _check(load_library().astcb200_fp32_peak(device, ctypes.byref(t)))
+    return t.value
 
 
 def psnr(a, b):

@@ -39,6 +39,9 @@ struct astcb200_ctx {
     uint32_t* d_sym = nullptr;
     size_t sym_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> stage_ev;  // 5 per chunk: before the first kernel and after each
+    int stage_chunks = 0;               // chunks recorded by the last encode
+    uint32_t stage_n[4] = {0, 0, 0, 0};
     std::string err;
 };
 
@@ -93,13 +96,32 @@ int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t
     a.picks = ctx->d_picks; a.pbrec = ctx->d_pbrec; a.snaps = ctx->d_snaps;
     a.out_blocks = d_out; a.symbolic = d_sym;
     uint32_t n = 0;
-    for (uint32_t first = 0; first < ctx->nblocks; first += ctx->chunk) {
+    const bool timing = (ctx->cfg.flags & ASTCB200_FLAG_STAGE_TIMING) != 0;
+    const int nchunks = (int)((ctx->nblocks + ctx->chunk - 1) / ctx->chunk);
+    if (timing) {
+        while ((int)ctx->stage_ev.size() < 5 * nchunks) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e), "cudaEventCreate");
+            ctx->stage_ev.push_back(e);
+        }
+        ctx->stage_chunks = nchunks;
+    }
+    for (int k = 0; k < 4; k++) ctx->stage_n[k] = 0;
+    int c = 0;
+    for (uint32_t first = 0; first < ctx->nblocks; first += ctx->chunk, c++) {
         a.block_first = (int)first;
         a.nblocks = (int)std::min<uint32_t>(ctx->chunk, ctx->nblocks - first);
+        cudaEvent_t* ev = timing ? &ctx->stage_ev[5 * c] : nullptr;
+        if (timing) CK(cudaEventRecord(ev[0], s), "stage event");
         CK(launch_partition_search(a, s), "k_partition_search");
+        if (timing) CK(cudaEventRecord(ev[1], s), "stage event");
         CK(launch_front(a, s), "k_front");
+        if (timing) CK(cudaEventRecord(ev[2], s), "stage event");
         CK(launch_refine(a, s), "k_refine");
+        if (timing) CK(cudaEventRecord(ev[3], s), "stage event");
         CK(launch_select_pack(a, s), "k_select_pack");
+        if (timing) CK(cudaEventRecord(ev[4], s), "stage event");
+        for (int k = 0; k < 4; k++) ctx->stage_n[k]++;
         n += 4;
     }
     if (launches) *launches = n;
@@ -154,6 +176,7 @@ int astcb200_destroy(astcb200_ctx* ctx) {
     cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ASTCB200_OK;
@@ -248,6 +271,20 @@ int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* 
     if (!ctx->have_image) return ASTCB200_NO_IMAGE;
     if (words < (size_t)ctx->nblocks * 108) return ASTCB200_BAD_ARG;
     return encode_host(ctx, rgba8, nullptr, symbolic, nullptr);
+}
+
+int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* n4) {
+    if (!ctx || !ms4) return ASTCB200_BAD_ARG;
+    for (int k = 0; k < 4; k++) { ms4[k] = 0.0f; if (n4) n4[k] = ctx->stage_n[k]; }
+    if (ctx->stage_chunks == 0) return ASTCB200_OK;
+    CK(cudaEventSynchronize(ctx->stage_ev[5 * ctx->stage_chunks - 1]), "stage event");
+    for (int c = 0; c < ctx->stage_chunks; c++)
+        for (int k = 0; k < 4; k++) {
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ctx->stage_ev[5 * c + k], ctx->stage_ev[5 * c + k + 1]), "cudaEventElapsedTime");
+            ms4[k] += ms;
+        }
+    return ASTCB200_OK;
 }
 
 // astc_store.cpp:18-62: magic 0x5CA1AB13, block dims, 24-bit image dims, then the blocks.

@@ -1,0 +1,287 @@
+"""Throughput benchmark of the ASTC full search on B200.
+
+Workload (one "step"): one 2048x2048 RGBA8 synthetic texture (generator of
+astc_implementation_b200/synth.py, seeds 1-4 in rotation; rank r of a multi-GPU
+run uses seeds 1+4r .. 4+4r) encoded twice, at 4x4 and at 6x6, by the full
+search.  The metric is Mtexel/s over both encodes.
+
+  value       device-resident input and output, CUDA events on the launching
+              stream around exactly K steps, max over ranks; the L2 is flushed
+              (512 MiB memset) before every step inside the timed region.
+  e2e         the same steps through the public host API (ASTCEncoder.encode:
+              host RGBA8 in, host blocks out, copies inside the timed region).
+  roofline    the dominant kernel's modelled FP32 operations (flop_model.py)
+              over its CUDA-event time, against this GPU's FP32 FMA peak
+              measured by astcb200_fp32_peak.
+  cpu_baseline the CPU oracle (a restatement of the reference's search) on a
+              bounded sample of the same workload, all host threads, rank 0.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+SIZE = 2048
+FOOTPRINTS = [(4, 4), (6, 6)]
+METRIC = "Mtexel/s on 1 B200 (4x4, 6x6): pruned vs full search at ≤0.1 dB PSNR loss"
+
+
+def texels_per_step():
+    return SIZE * SIZE * len(FOOTPRINTS)
+
+
+def blocks_of(bx, by):
+    return ((SIZE + bx - 1) // bx) * ((SIZE + by - 1) // by)
+
+
+def rank_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------- CPU oracle (baseline only)
+def oracle_lib():
+    path = os.path.join(REPO, "oracle", "liboracle.so")
+    if not os.path.exists(path):
+        subprocess.check_call([os.path.join(REPO, "oracle", "build_oracle.sh")])
+    return ctypes.CDLL(path)
+
+
+def cpu_sample_rate(img, sample_side, reps=1):
+    """Oracle Mtexel/s on the top-left sample_side^2 crop at both footprints, all threads."""
+    lib = oracle_lib()
+    crop = np.ascontiguousarray(img[:sample_side, :sample_side])
+    texels, secs = 0, 0.0
+    for _ in range(reps):
+        for bx, by in FOOTPRINTS:
+            n = ((sample_side + bx - 1) // bx) * ((sample_side + by - 1) // by)
+            out = np.zeros(n * 16, np.uint8)
+            t0 = time.perf_counter()
+            rc = lib.orc_encode(ctypes.c_void_p(crop.ctypes.data), sample_side, sample_side, bx, by, 0,
+                                ctypes.c_void_p(out.ctypes.data), None)
+            secs += time.perf_counter() - t0
+            assert rc == 0
+            texels += sample_side * sample_side
+    return texels / secs / 1e6, secs
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    from astc_implementation_b200 import synth
+    img = synth.make_texture(SIZE, SIZE, 1)
+    side = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_sample_rate(img, min(side, 64))
+    rates, secs = [], 0.0
+    for _ in range(args.steps):
+        r, s = cpu_sample_rate(img, side)
+        rates.append(r)
+        secs += s
+    value = float(np.mean(rates))
+    cores = os.cpu_count()
+    sample = "%dx%d crop of the 2048x2048 seed-1 texture at 4x4 and 6x6 per step" % (side, side)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mtexel/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000.0 * secs / max(args.steps, 1), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "2048x2048 RGBA8 synthetic, full search at 4x4 and 6x6 (CPU sample)",
+                   "method": "full search", "sample": sample},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mtexel/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "Mtexel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's search runs only through WebGPU/Dawn, which cannot run on this box; "
+                "this arm times the CPU restatement of its passes (oracle/astc_oracle.cpp) with OpenMP",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- B200 arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline crop")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import astc_implementation_b200 as ab
+    from astc_implementation_b200 import flop_model, synth
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    seeds = [1 + 4 * rank + i for i in range(4)]
+    imgs = [synth.make_texture(SIZE, SIZE, s) for s in seeds]
+    d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
+    stream = torch.cuda.current_stream()
+    encs, outs = [], []
+    for bx, by in FOOTPRINTS:
+        e = ab.ASTCEncoder(device=local, stage_timing=True)
+        e.init()
+        e.secondaryInit(SIZE, SIZE, bx, by)
+        encs.append(e)
+        outs.append(torch.empty(e.numBlocks * 16, dtype=torch.uint8, device="cuda"))
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    stage_ms = np.zeros((len(FOOTPRINTS), 4))
+    stage_n = np.zeros((len(FOOTPRINTS), 4))
+
+    def step(i, record):
+        flush.fill_(i & 0xFF)
+        for k, e in enumerate(encs):
+            e.encode_device(d_imgs[i % 4].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
+            if record:
+                ms, n = e.stage_times()
+                stage_ms[k] += ms
+                stage_n[k] += n
+
+    for i in range(args.warmup):
+        step(i, False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for i in range(args.steps):
+        step(i, True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    texels = texels_per_step() * args.steps * world
+    value = texels / (ms / 1000.0) / 1e6
+    launches = int(stage_n.sum())
+
+    # e2e through the public host API
+    host_steps = max(1, min(args.steps, 3))
+    t_e2e = time.perf_counter()
+    for i in range(host_steps):
+        for e in encs:
+            e.encode(imgs[i % 4])
+    t_e2e = time.perf_counter() - t_e2e
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = texels_per_step() * host_steps * world / t_e2e / 1e6
+    h2d = SIZE * SIZE * 4 * len(FOOTPRINTS)
+    d2h = sum(blocks_of(bx, by) * 16 for bx, by in FOOTPRINTS)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel
+    lib = ab.load_library()
+    names = ["k_partition_search", "k_front", "k_refine", "k_select_pack"]
+    model_keys = ["search", "front", "refine", None]
+    models = [flop_model.per_block(lib, bx, by) for bx, by in FOOTPRINTS]
+    tot_ms = stage_ms.sum(axis=0)
+    dom = int(np.argmax(tot_ms))
+    dom_flops = sum(models[k][model_keys[dom]] * blocks_of(*FOOTPRINTS[k]) for k in range(len(FOOTPRINTS))) * args.steps \
+        if model_keys[dom] else 0.0
+    dom_launches = int(stage_n[:, dom].sum())
+    avg_launch_ms = tot_ms[dom] / max(dom_launches, 1)
+    achieved = dom_flops / dom_launches / (avg_launch_ms / 1000.0) / 1e12 if dom_launches else 0.0
+    peak = ab.fp32_peak_tflops(local)
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(names[dom])
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample)
+        cpu = {"value": round(rate, 4), "unit": "Mtexel/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": "%dx%d crop of the seed-1 texture at 4x4 and 6x6 (%.1f s of CPU time)" % (args.cpu_sample, args.cpu_sample, secs)}
+    total_model = sum(models[k]["total"] * blocks_of(*FOOTPRINTS[k]) for k in range(len(FOOTPRINTS))) * args.steps * world
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mtexel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "2048x2048 RGBA8 synthetic texture (seeds 1-4 per rank), full search at 4x4 and 6x6 per step",
+                   "method": "full search (plain, no learned proposal)", "image": [SIZE, SIZE],
+                   "footprints": ["4x4", "6x6"], "l2": "512 MiB memset before every step, inside the timed region",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "per_footprint_ms": {"%dx%d" % fp: round(float(stage_ms[k].sum() / args.steps), 3) for k, fp in enumerate(FOOTPRINTS)},
+        "stage_ms_per_step": {names[i]: round(float(tot_ms[i] / args.steps), 3) for i in range(4)},
+        "model_tflops_whole_step": round(total_model / (ms / 1000.0) / 1e12, 3),
+        "roofline": {"kernel": names[dom], "bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak else None, "traffic": traffic,
+                     "peak_source": "FP32 FMA microbenchmark on this GPU in this run (an FMA counts 2 ops); "
+                                    "MEASURED_PEAKS.json has no FP32 figure"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e, 3), "unit": "Mtexel/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    for e in encs:
+        e.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

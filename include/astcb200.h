@@ -35,8 +35,12 @@ typedef struct astcb200_config {
     uint32_t struct_size;  /* sizeof(astcb200_config); 0 selects all defaults */
     uint32_t chunk_blocks; /* blocks searched per launch sequence; 0 = 65536 */
     uint32_t timeout_ms;   /* bound on each host wait for the device; 0 = no bound */
-    uint32_t reserved;
+    uint32_t flags;        /* ASTCB200_FLAG_* */
 } astcb200_config;
+
+/* Record CUDA events around every kernel launch (on the launching stream) so that
+ * astcb200_stage_times reports per-kernel device time. */
+#define ASTCB200_FLAG_STAGE_TIMING 1u
 
 typedef struct astcb200_stats {
     double ms_wall;       /* host time of the call */
@@ -84,6 +88,15 @@ int astcb200_store_image(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uin
  * (dim_x*dim_y*4 bytes, UNORM8 with round-to-nearest from the 16-bit result). */
 int astcb200_decode(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
                     const uint8_t* blocks, size_t blocks_len, uint8_t* rgba8_out);
+
+/* Device milliseconds spent in each of the four kernels (partition search, front,
+ * refine, select/pack) by the last encode call, summed over chunks; needs
+ * ASTCB200_FLAG_STAGE_TIMING.  launches[4] receives the launch counts (optional). */
+int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* launches4);
+
+/* Measures the device's FP32 throughput with a dependent-FMA-chain kernel (diagnostic
+ * used by bench.py for the roofline denominator): TFLOP/s counting an FMA as 2 flops. */
+int astcb200_fp32_peak(int device_ordinal, double* tflops);
 
 const char* astcb200_status_string(int status);
 const char* astcb200_last_error(const astcb200_ctx* ctx);
