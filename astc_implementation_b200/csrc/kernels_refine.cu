@@ -182,7 +182,7 @@ struct Packer {
         return true;
     }
     // pack_color_endpoints_helper (pass14:917-1224)
-    __device__ uint32_t pack(float4 color0, float4 color1, float4 rgbs, uint32_t fmt, uint32_t q, uint32_t* out) const {
+    __device__ __noinline__ uint32_t pack(float4 color0, float4 color1, float4 rgbs, uint32_t fmt, uint32_t q, uint32_t* out) const {
         const float4 c0 = vmin(vmax(color0, mk(0.0f)), mk(65535.0f)) / mk(257.0f);
         const float4 c1 = vmin(vmax(color1, mk(0.0f)), mk(65535.0f)) / mk(257.0f);
         float best = ERR_DEFAULT;
@@ -246,7 +246,7 @@ struct Packer {
 };
 
 // pass15: decode packed endpoints of one partition, scaled by 257.
-__device__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, int32_t* e0, int32_t* e1) {
+__device__ __noinline__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, int32_t* e0, int32_t* e1) {
     I4 o0, o1;
     auto I = [&](int k) { return (int32_t)v[k]; };
     switch (fmt) {
@@ -292,10 +292,11 @@ constexpr int kRefineThreads = kRefinePBs * kNumCand;
 // Per-thread candidate state in shared memory.  Plain 4-byte members give the
 // struct an odd word stride (89 words), so a warp's threads hit distinct banks.
 struct CandSmem {
-    float e0[4][4], e1[4][4];
+    float e0[4][4], e1[4][4], rgbs[4][4];
     int32_t u0[4][4], u1[4][4];
     uint8_t qw[64];
     uint8_t packed[32];
+    uint8_t packed_mod[32];
     uint32_t pad;
 };
 __device__ __forceinline__ float4 ld4(const float* p) { return make_float4(p[0], p[1], p[2], p[3]); }
@@ -325,8 +326,7 @@ __device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const Dev
     return v;
 }
 
-template <int P>
-__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, const float4* px, const uint8_t* tp,
+__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const float4* px, const uint8_t* tp,
                                  CandSmem& cs, Snap* snap) {
     const RTabs tb{a.tables, &a.L};
     const int T = a.L.T;
@@ -337,15 +337,11 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
     const float4 cw = chan_w();
     const float lsw = (cw.x + cw.y) + cw.z;
     const Packer pk{a.tables + a.L.off_cu2u};
-    float psz[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) psz[q] = P == 1 ? (q == 0 ? (float)T : 0.0f) : (float)tb.part_count(P, rec.entry, q);
 #pragma unroll
     for (int q = 0; q < 4; q++) { st4(cs.e0[q], rec.ep0[q]); st4(cs.e1[q], rec.ep1[q]); }
     for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
     float top_err = ERR_DEFAULT;
     uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
-    float4 rgbs[4];
 
     auto final_error = [&]() {
         float total = 0.0f;
@@ -374,9 +370,9 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
 
     for (int it = 0; it < 6; it++) {
         // ---------------- pass13: least-squares endpoints from the current weights
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < P; q++) {
-            const float ps = psz[q];
+            const float ps = P == 1 ? (float)T : (float)tb.part_count(P, rec.entry, q);
             const float4 rsum = (rec.avg[q] * ps) * cw;
             const float4 rws = vmax(cw * ps, mk(1e-17f));
             float4 sv = rsum / rws; sv.w = 0.0f;
@@ -405,7 +401,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
             const float lx = ls * lsw, my = ms * lsw, rz = rs * lsw;
             const float scalediv = clampf(smin / fmaxf(smax, 1e-10f), 0.0f, 1.0f);
             const float4 sds = sdir * smax;
-            rgbs[q] = make_float4(sds.x, sds.y, sds.z, scalediv);
+            st4(cs.rgbs[q], make_float4(sds.x, sds.y, sds.z, scalediv));
             if (wmin >= wmax * 0.999f) {
                 const float4 ac = (colx + coly) / vmax(cw * ps, mk(1e-17f));
                 float4 e0 = ld4(cs.e0[q]), e1 = ld4(cs.e1[q]);
@@ -414,7 +410,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
                 if (ac.z == ac.z) { e0.z = ac.z; e1.z = ac.z; }
                 if (ac.w == ac.w) { e0.w = ac.w; e1.w = ac.w; }
                 st4(cs.e0[q], e0); st4(cs.e1[q], e1);
-                rgbs[q] = make_float4(sds.x, sds.y, sds.z, 1.0f);
+                st4(cs.rgbs[q], make_float4(sds.x, sds.y, sds.z, 1.0f));
             } else {
                 const float4 det = (lv * rv) - (mv * mv);
                 const float4 rdet = mk(1.0f) / det;
@@ -433,7 +429,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
                 const float se1 = ((lx * sv1) - (my * sv0)) * lsrdet;
                 if ((fabsf(lsdet) > (lsmss * 1e-4f)) && se0 == se0 && se1 == se1 && se0 < se1) {
                     const float4 sdsm = sdir * se1;
-                    rgbs[q] = make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1);
+                    st4(cs.rgbs[q], make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1));
                 }
             }
         }
@@ -442,30 +438,32 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
             bool all_same = ci.ql != ci.qlm;
             uint32_t fn[4] = {0, 0, 0, 0}, vals[8];
             for (int i = 0; i < 32; i++) cs.packed[i] = 0;
-#pragma unroll
+#pragma unroll 1
             for (int q = 0; q < P; q++) {
-                fn[q] = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), rgbs[q], ci.fmt[q], ci.ql, vals);
+                const uint32_t f = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), ld4(cs.rgbs[q]), ci.fmt[q], ci.ql, vals);
+                fn[0] = q == 0 ? f : fn[0]; fn[1] = q == 1 ? f : fn[1]; fn[2] = q == 2 ? f : fn[2]; fn[3] = q == 3 ? f : fn[3];
 #pragma unroll
                 for (int i = 0; i < 8; i++) cs.packed[q * 8 + i] = (uint8_t)vals[i];
-                if (q > 0) all_same = all_same && fn[q] == fn[0];
+                if (q > 0) all_same = all_same && f == fn[0];
             }
             bool m = false;
             if (P >= 2 && all_same) {
-                uint32_t fm[4] = {0, 0, 0, 0}, vm[32];
+                uint32_t fm[4] = {0, 0, 0, 0};
+                uint8_t* vm = cs.packed_mod;
                 bool same_mod = true;
-#pragma unroll
+#pragma unroll 1
                 for (int q = 0; q < P; q++) {
-                    if (!same_mod) break;
-                    fm[q] = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), rgbs[q], ci.fmt[q], ci.qlm, vals);
+                    const uint32_t f = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), ld4(cs.rgbs[q]), ci.fmt[q], ci.qlm, vals);
+                    fm[0] = q == 0 ? f : fm[0]; fm[1] = q == 1 ? f : fm[1]; fm[2] = q == 2 ? f : fm[2]; fm[3] = q == 3 ? f : fm[3];
 #pragma unroll
-                    for (int i = 0; i < 8; i++) vm[q * 8 + i] = vals[i];
-                    if (q > 0 && fm[q] != fm[0]) same_mod = false;
+                    for (int i = 0; i < 8; i++) vm[q * 8 + i] = (uint8_t)vals[i];
+                    if (q > 0 && f != fm[0]) { same_mod = false; break; }
                 }
                 if (same_mod) {
                     m = true;
 #pragma unroll
                     for (int q = 0; q < 4; q++) fn[q] = fm[q];
-                    for (int i = 0; i < 32; i++) cs.packed[i] = i < P * 8 ? (uint8_t)vm[i] : 0;
+                    for (int i = 0; i < 32; i++) cs.packed[i] = i < P * 8 ? vm[i] : 0;
                 }
             }
             matched = m ? 1 : 0;
@@ -474,7 +472,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, int k, c
             for (int q = 0; q < 4; q++) ffmt[q] = fn[q];
         }
         // ---------------- pass15
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < P; q++) unpack_endpoints(ffmt[q], cs.packed + q * 8, cs.u0[q], cs.u1[q]);
         if (it == 0) final_error();
         // ---------------- pass16: move each weight one quant step if that lowers the error
@@ -536,14 +534,18 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     float4* pxs = reinterpret_cast<float4*>(smem + sizeof(CandSmem) * kRefineThreads);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefinePBs * T);
     const int tid = threadIdx.x, pbl = tid / kNumCand, k = tid % kNumCand;
+    // slot-major order: consecutive CTAs hold partitioned blocks of the same slot
+    // (hence the same partition count), so co-resident warps run the same code
     const int npb = a.nblocks * kSlotsPerBlock;
-    const int pb = blockIdx.x * kRefinePBs + pbl;
-    const bool live = pb < npb;
+    const int li = blockIdx.x * kRefinePBs + pbl;
+    const bool live = li < npb;
+    const int slot = live ? li / a.nblocks : 0, lb = live ? li % a.nblocks : 0;
+    const int pb = lb * kSlotsPerBlock + slot;
     const PBRec* rec = live ? &a.pbrec[pb] : nullptr;
     const int P = live ? (int)rec->P : 1;
     const int ncand = live ? (int)rec->ncand : 0;
     if (live && ncand > 0) {
-        const int blk = a.block_first + pb / kSlotsPerBlock;
+        const int blk = a.block_first + lb;
         const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + rec->entry) * T : nullptr;
         const int bxi = blk % a.nbx, byi = blk / a.nbx;
         for (int t = k; t < T; t += kNumCand) {
@@ -559,14 +561,7 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
     snap->err = ERR_DEFAULT;  // inert slot unless refined below
     if (k >= ncand) return;
-    const float4* px = pxs + pbl * T;
-    const uint8_t* tp = tps + pbl * T;
-    switch (P) {
-        case 1: refine_candidate<1>(a, *rec, k, px, tp, cs[tid], snap); break;
-        case 2: refine_candidate<2>(a, *rec, k, px, tp, cs[tid], snap); break;
-        case 3: refine_candidate<3>(a, *rec, k, px, tp, cs[tid], snap); break;
-        default: refine_candidate<4>(a, *rec, k, px, tp, cs[tid], snap); break;
-    }
+    refine_candidate(a, *rec, P, k, pxs + pbl * T, tps + pbl * T, cs[tid], snap);
 }
 
 // ------------------------------------------------------------ k_select_pack

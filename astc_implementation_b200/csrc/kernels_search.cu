@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int item = blockIdx.x * kSearchWarps + warp;
     if (item >= a.nblocks * 3) return;
-    const int lb = item / 3, P = item % 3 + 2;
+    const int lb = item % a.nblocks, P = item / a.nblocks + 2;  // P-major: a CTA's warps share P
     uint8_t* ws = smem + warp * kSearchWarpBytes;
     if (P == 2) search_one<2>(a, a.block_first + lb, lb, ws, lane);
     else if (P == 3) search_one<3>(a, a.block_first + lb, lb, ws, lane);
@@ -424,8 +424,7 @@ __device__ __forceinline__ int bm_quant_weight(const Tabs& tb, const BmQuant& s,
     return v;
 }
 
-template <int P>
-__device__ void front_body(const KernelArgs& a, int lb, int slot_in_block, uint32_t entry, uint8_t* sm) {
+__device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in_block, uint32_t entry, uint8_t* sm) {
     const Tabs tb{a.tables, &a.L};
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -847,20 +846,18 @@ __device__ void front_body(const KernelArgs& a, int lb, int slot_in_block, uint3
 
 __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const int slot = blockIdx.x;
-    const int lb = slot / kSlotsPerBlock, k = slot % kSlotsPerBlock;
-    if (lb >= a.nblocks) return;
-    if (k == 0) { front_body<1>(a, lb, 0, 0, smem); return; }
+    // slot-major order so that co-resident CTAs work on the same partition count
+    const int li = blockIdx.x;
+    if (li >= a.nblocks * kSlotsPerBlock) return;
+    const int k = li / a.nblocks, lb = li % a.nblocks;
+    if (k == 0) { front_body(a, 1, lb, 0, 0, smem); return; }
     const int P = 2 + (k - 1) / 4, i = (k - 1) % 4;
     const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
     if (i >= pk[4]) {
         if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * kSlotsPerBlock + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
         return;
     }
-    const uint32_t entry = pk[i];
-    if (P == 2) front_body<2>(a, lb, k, entry, smem);
-    else if (P == 3) front_body<3>(a, lb, k, entry, smem);
-    else front_body<4>(a, lb, k, entry, smem);
+    front_body(a, P, lb, k, pk[i], smem);
 }
 
 }  // namespace
