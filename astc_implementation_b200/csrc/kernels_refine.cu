@@ -313,21 +313,29 @@ struct RTabs {
     __device__ int wt_start(int m, int w) const { return reinterpret_cast<const uint16_t*>(b + L->off_wt_start)[m * 64 + w]; }
     __device__ uint32_t t2w(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_t2w)[i]; }
     __device__ uint32_t w2t(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_w2t)[i]; }
-    __device__ const uint8_t* part_texels(int P, int e) const { return b + L->off_part_texel + ((size_t)(P - 2) * 1024 + e) * L->T; }
+    __device__ uint64_t tw4(int m, int t) const { return reinterpret_cast<const uint64_t*>(b + L->off_tw4)[m * L->T + t]; }
     __device__ int part_count(int P, int e, int q) const { return b[L->off_part_counts + ((P - 2) * 1024 + e) * 4 + q]; }
     __device__ uint32_t prev_next(int q, int v) const { return reinterpret_cast<const uint16_t*>(b + L->off_prev_next)[q * 65 + v]; }
 };
 
-__device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const DevDm& d, const uint8_t* qw, int t, bool direct) {
+// Infilled weight of texel t from the 0..64 weights (pass13:165-184, pass17:127-146).
+// Padding entries of the dense list add qw[0]/64 * 0 = +0, which never changes v.
+__device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const uint8_t* qw, int t, bool direct) {
     if (direct) return (float)qw[t] / 64.0f;
-    const int n = tb.tw_count(dm, t), base = d.tw_base + tb.tw_start(dm, t);
+    const uint64_t e4 = tb.tw4(dm, t);
     float v = 0.0f;
-    for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + ((float)qw[e & 0xFF] / 64.0f) * ((float)(e >> 8) * (1.0f / 16.0f)); }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
+        v = v + ((float)qw[e & 0xFF] / 64.0f) * ((float)(e >> 8) * (1.0f / 16.0f));
+    }
     return v;
 }
 
+constexpr int kUwCacheTexels = 36;  // footprints up to 6x6 keep each thread's infilled weights in shared memory
+
 __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const float4* px, const uint8_t* tp,
-                                 CandSmem& cs, Snap* snap) {
+                                 CandSmem& cs, float* uwc, Snap* snap) {
     const RTabs tb{a.tables, &a.L};
     const int T = a.L.T;
     const CandInit& ci = rec.c[k];
@@ -342,12 +350,17 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
     float top_err = ERR_DEFAULT;
     uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
+    // uwc (when non-null) caches this thread's infilled weights, stride kRefineThreads
+    auto fill_uw = [&]() {
+        if (uwc) for (int t = 0; t < T; t++) uwc[t * kRefineThreads] = undec_weight(tb, bm.dm, cs.qw, t, direct);
+    };
+    auto UW = [&](int t) { return uwc ? uwc[t * kRefineThreads] : undec_weight(tb, bm.dm, cs.qw, t, direct); };
 
     auto final_error = [&]() {
         float total = 0.0f;
         for (int t = 0; t < T; t++) {
             const int p = tp[t];
-            const float w = undec_weight(tb, bm.dm, dmi, cs.qw, t, direct);
+            const float w = UW(t);
             const int32_t w1 = f2i(rintf(w * 64.0f)), w0 = 64 - w1;
             const float4 x = px[t];
             float4 d;
@@ -369,6 +382,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     };
 
     for (int it = 0; it < 6; it++) {
+        fill_uw();
         // ---------------- pass13: least-squares endpoints from the current weights
 #pragma unroll 1
         for (int q = 0; q < P; q++) {
@@ -382,7 +396,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             for (int t = 0; t < T; t++) {
                 if (tp[t] != q) continue;
                 const float4 rgba = px[t];
-                const float w = undec_weight(tb, bm.dm, dmi, cs.qw, t, direct);
+                const float w = UW(t);
                 if (w < wmin) wmin = w;
                 if (w > wmax) wmax = w;
                 const float sc = dot3(rgba, sdir);
@@ -500,15 +514,17 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 float4 ebv = mk(0.0f), edv = mk(0.0f), euv = mk(0.0f);
                 const int nt = tb.wt_count(bm.dm, we), wbase = dmi.wt_base + tb.wt_start(bm.dm, we);
                 for (int te = 0; te < nt; te++) {
-                    const int t = tb.w2t(wbase + te) & 0xFF;
-                    const int n = tb.tw_count(bm.dm, t), tbase = dmi.tw_base + tb.tw_start(bm.dm, t);
-                    float wb = 0.0f, twb = 0.0f;
-                    bool found = false;
-                    for (int j = 0; j < n; j++) {
-                        const uint32_t e = tb.t2w(tbase + j);
-                        const float c = (float)(e >> 8) * (1.0f / 16.0f);
-                        wb = wb + (float)cs.qw[e & 0xFF] * c;
-                        if (!found && (int)(e & 0xFF) == we) { twb = c; found = true; }
+                    // the weight's own contribution to texel t is the w2t entry's
+                    // (each (texel, weight) pair appears once in both maps)
+                    const uint32_t we2 = tb.w2t(wbase + te);
+                    const int t = we2 & 0xFF;
+                    const float twb = (float)(we2 >> 8) * (1.0f / 16.0f);
+                    const uint64_t e4 = tb.tw4(bm.dm, t);
+                    float wb = 0.0f;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
+                        wb = wb + (float)cs.qw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f));
                     }
                     const int p = tp[t];
                     const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
@@ -523,6 +539,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 else if ((ed < eb) && (uqw > 0)) cs.qw[we] = (uint8_t)dn;
             }
         }
+        fill_uw();
         final_error();
     }
 }
@@ -533,35 +550,59 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     CandSmem* cs = reinterpret_cast<CandSmem*>(smem);
     float4* pxs = reinterpret_cast<float4*>(smem + sizeof(CandSmem) * kRefineThreads);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefinePBs * T);
-    const int tid = threadIdx.x, pbl = tid / kNumCand, k = tid % kNumCand;
+    int* keys = reinterpret_cast<int*>(tps + ((kRefinePBs * T + 15) & ~15));
+    float* uwc_all = reinterpret_cast<float*>(keys + kRefineThreads);
+    const int tid = threadIdx.x;
     // slot-major order: consecutive CTAs hold partitioned blocks of the same slot
     // (hence the same partition count), so co-resident warps run the same code
     const int npb = a.nblocks * kSlotsPerBlock;
-    const int li = blockIdx.x * kRefinePBs + pbl;
-    const bool live = li < npb;
-    const int slot = live ? li / a.nblocks : 0, lb = live ? li % a.nblocks : 0;
-    const int pb = lb * kSlotsPerBlock + slot;
-    const PBRec* rec = live ? &a.pbrec[pb] : nullptr;
-    const int P = live ? (int)rec->P : 1;
-    const int ncand = live ? (int)rec->ncand : 0;
-    if (live && ncand > 0) {
-        const int blk = a.block_first + lb;
-        const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + rec->entry) * T : nullptr;
-        const int bxi = blk % a.nbx, byi = blk / a.nbx;
-        for (int t = k; t < T; t += kNumCand) {
-            const int x = min(bxi * a.L.bx + t % a.L.bx, a.width - 1), y = min(byi * a.L.by + t / a.L.bx, a.height - 1);
-            const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
-            pxs[pbl * T + t] = make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
-                                           ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
-            tps[pbl * T + t] = P > 1 ? prow[t] : 0;
+    {
+        const int pbl = tid / kNumCand, k = tid % kNumCand;
+        const int li = blockIdx.x * kRefinePBs + pbl;
+        int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
+        if (li < npb) {
+            const int slot = li / a.nblocks, lb = li % a.nblocks;
+            const PBRec& r = a.pbrec[lb * kSlotsPerBlock + slot];
+            if (k < (int)r.ncand) key = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
+            if (r.ncand > 0) {
+                const int P = r.P, blk = a.block_first + lb;
+                const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
+                const int bxi = blk % a.nbx, byi = blk / a.nbx;
+                for (int t = k; t < T; t += kNumCand) {
+                    const int x = min(bxi * a.L.bx + t % a.L.bx, a.width - 1), y = min(byi * a.L.by + t / a.L.bx, a.height - 1);
+                    const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
+                    pxs[pbl * T + t] = make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
+                                                   ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
+                    tps[pbl * T + t] = P > 1 ? prow[t] : 0;
+                }
+            }
         }
+        keys[tid] = key * kRefineThreads + tid;  // unique keys: decimation mode, then position
     }
     __syncthreads();
-    if (!live) return;
+    // Thread tid takes the candidate of rank tid in decimation-mode order, so a
+    // warp's candidates mostly share loop bounds and table rows.
+    int mine = 0;
+    {
+        const int kk = keys[tid];
+        int rank = 0;
+        for (int j = 0; j < kRefineThreads; j++) rank += keys[j] < kk;
+        __syncthreads();
+        keys[rank] = tid;
+        __syncthreads();
+        mine = keys[tid];
+    }
+    const int pbl = mine / kNumCand, k = mine % kNumCand;
+    const int li = blockIdx.x * kRefinePBs + pbl;
+    if (li >= npb) return;
+    const int slot = li / a.nblocks, lb = li % a.nblocks;
+    const int pb = lb * kSlotsPerBlock + slot;
+    const PBRec& rec = a.pbrec[pb];
     Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
     snap->err = ERR_DEFAULT;  // inert slot unless refined below
-    if (k >= ncand) return;
-    refine_candidate(a, *rec, P, k, pxs + pbl * T, tps + pbl * T, cs[tid], snap);
+    if (k >= (int)rec.ncand) return;
+    float* uwc = T <= kUwCacheTexels ? uwc_all + tid : nullptr;
+    refine_candidate(a, rec, (int)rec.P, k, pxs + pbl * T, tps + pbl * T, cs[tid], uwc, snap);
 }
 
 // ------------------------------------------------------------ k_select_pack
@@ -722,7 +763,8 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
 }  // namespace
 
 size_t refine_smem_bytes(const TableLayout& L) {
-    return sizeof(CandSmem) * kRefineThreads + (size_t)kRefinePBs * L.T * 16 + (size_t)kRefinePBs * L.T;
+    return sizeof(CandSmem) * kRefineThreads + (size_t)kRefinePBs * L.T * 16 + (((size_t)kRefinePBs * L.T + 15) & ~(size_t)15) +
+           kRefineThreads * 4 + (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
 }
 
 cudaError_t configure_search_kernels(const TableLayout& L);

@@ -41,6 +41,8 @@ struct Tabs {
     __device__ int wt_start(int m, int w) const { return reinterpret_cast<const uint16_t*>(b + L->off_wt_start)[m * 64 + w]; }
     __device__ uint32_t t2w(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_t2w)[i]; }
     __device__ uint32_t w2t(int i) const { return reinterpret_cast<const uint16_t*>(b + L->off_w2t)[i]; }
+    __device__ uint64_t tw4(int m, int t) const { return reinterpret_cast<const uint64_t*>(b + L->off_tw4)[m * L->T + t]; }
+    __device__ int bm_order(int j) const { return reinterpret_cast<const uint16_t*>(b + L->off_bm_order)[j]; }
     __device__ const uint8_t* part_texels(int P, int e) const { return b + L->off_part_texel + ((size_t)(P - 2) * 1024 + e) * L->T; }
     __device__ int part_count(int P, int e, int q) const { return b[L->off_part_counts + ((P - 2) * 1024 + e) * 4 + q]; }
     __device__ uint32_t part_seed(int P, int e) const { return reinterpret_cast<const uint32_t*>(b + L->off_part_info)[(P - 2) * 1024 + e]; }
@@ -345,7 +347,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
 }
 
 // ============================================================ passes 01-12
-constexpr int kFrontThreads = 64;
+constexpr int kFrontThreads = 128;
+constexpr int kFrontWarps = kFrontThreads / 32;
 
 struct FrontLayout {
     int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, total;
@@ -368,7 +371,7 @@ struct FrontMisc {
 };
 
 __host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
-__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm) {
+__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w) {
     FrontLayout f;
     int o = 0;
     f.px = take16(o, T * 16);
@@ -378,13 +381,13 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm) {
     f.dec = take16(o, ndm * 64 * 4);
     f.lo = take16(o, ndm * 8 * 4);
     f.hi = take16(o, ndm * 8 * 4);
-    f.scratch = take16(o, 2 * kScratchPerWarp);
+    f.scratch = take16(o, kFrontWarps * kScratchPerWarp);
     f.bm_err = take16(o, nbm * 4);
     f.bm_bits = take16(o, nbm * 4);
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    f.qf = take16(o, 64 * kFrontThreads * 4);
+    f.qf = take16(o, max_w * kFrontThreads * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.total = o;
     return f;
@@ -429,7 +432,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int blk = a.block_first + lb;
-    const FrontLayout fl = front_layout(T, ndm, nbm);
+    const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w);
     float4* px = reinterpret_cast<float4*>(sm + fl.px);
     float* iw = reinterpret_cast<float*>(sm + fl.w);
     float* wes = reinterpret_cast<float*>(sm + fl.wes);
@@ -515,7 +518,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
         uint32_t* smp = reinterpret_cast<uint32_t*>(scr + 144 * 4);
         float* ang = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4);
         float* lh = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4 + 16 * 4);  // [16][5]: lowest, span, err, cl, ch
-        for (int m = warp; m < ndm; m += kFrontThreads / 32) {
+        for (int m = warp; m < ndm; m += kFrontWarps) {
             const DevDm dmi = tb.dm(m);
             const int W = dmi.W;
             float* dw = dec + m * 64;
@@ -541,9 +544,11 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
                 }
                 __syncwarp();
                 for (int t = lane; t < T; t += 32) {
-                    const int n = tb.tw_count(m, t), base = dmi.tw_base + tb.tw_start(m, t);
+                    // the texel's entries in list order; padding entries add dw[0] * 0, which never changes v
+                    const uint64_t e4 = tb.tw4(m, t);
                     float v = 0.0f;
-                    for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + dw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+#pragma unroll
+                    for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + dw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
                     inf[t] = v;
                 }
                 __syncwarp();
@@ -625,7 +630,8 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
     __syncthreads();
 
     // ---------------- pass07: weight quantisation error per block mode
-    for (int i = tid; i < nbm; i += kFrontThreads) {
+    for (int j = tid; j < nbm; j += kFrontThreads) {
+        const int i = tb.bm_order(j);  // neighbouring threads get modes of the same decimation
         const DevBm bm = tb.bm(i);
         const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
         if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
@@ -635,9 +641,10 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
         for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
         float err = 0.0f;
         for (int t = 0; t < T; t++) {
-            const int n = tb.tw_count(bm.dm, t), base = dmi.tw_base + tb.tw_start(bm.dm, t);
+            const uint64_t e4 = tb.tw4(bm.dm, t);
             float v = 0.0f;
-            for (int j = 0; j < n; j++) { const uint32_t e = tb.t2w(base + j); v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+#pragma unroll
+            for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
             const float d = v - iw[t];
             err = err + (d * d) * wes[is_const ? 0 : t];
         }
@@ -863,7 +870,7 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__
 }  // namespace
 
 size_t search_smem_bytes(const TableLayout&) { return (size_t)kSearchWarps * kSearchWarpBytes; }
-size_t front_smem_bytes(const TableLayout& L) { return (size_t)front_layout(L.T, L.ndm, L.nbm).total; }
+size_t front_smem_bytes(const TableLayout& L) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w).total; }
 
 cudaError_t configure_search_kernels(const TableLayout& L) {
     cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem_bytes(L));

@@ -511,6 +511,16 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
             }
         }
     }
+    std::vector<uint64_t> tw4((size_t)ndm * T, 0);
+    for (int m = 0; m < ndm; m++)
+        for (int t = 0; t < T; t++) {
+            uint64_t v = 0;
+            const int n = twc[(size_t)m * T + t], base = dms[m].tw_base + tws[(size_t)m * T + t];
+            for (int j = 0; j < n; j++) v |= (uint64_t)t2w[base + j] << (16 * j);
+            tw4[(size_t)m * T + t] = v;
+        }
+    L.max_w = 0;
+    for (int m = 0; m < ndm; m++) L.max_w = std::max<int>(L.max_w, dms[m].W);
     std::vector<DevBm> bms(L.nbm);
     for (int i = 0; i < L.nbm; i++) {
         const HostTables::Bm& b = h.bms[h.valid_bms[i].first];
@@ -528,6 +538,9 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
             pinfo[k] = p.seed;
             for (int q = 0; q < pc; q++) cov[k * 4 + q] = h.cov[pc][(size_t)e * pc + q];
         }
+    std::vector<uint16_t> order(L.nbm);
+    for (int i = 0; i < L.nbm; i++) order[i] = (uint16_t)i;
+    std::stable_sort(order.begin(), order.end(), [&](uint16_t x, uint16_t y) { return bms[x].dm < bms[y].dm; });
     L.off_dm = put(blob, dms.data(), dms.size());
     L.off_bm = put(blob, bms.data(), bms.size());
     L.off_tw_count = put(blob, twc.data(), twc.size());
@@ -536,6 +549,8 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
     L.off_wt_start = put(blob, wts.data(), wts.size());
     L.off_t2w = put(blob, t2w.data(), t2w.size());
     L.off_w2t = put(blob, w2t.data(), w2t.size());
+    L.off_tw4 = put(blob, tw4.data(), tw4.size());
+    L.off_bm_order = put(blob, order.data(), order.size());
     L.off_part_texel = put(blob, ptex.data(), ptex.size());
     L.off_part_info = put(blob, pinfo.data(), pinfo.size());
     L.off_part_counts = put(blob, pcnt.data(), pcnt.size());

@@ -41,6 +41,7 @@ struct DevBm {
 // Byte offsets of every table inside the device blob; passed to kernels by value.
 struct TableLayout {
     int32_t bx, by, T, ndm, nbm;
+    int32_t max_w;            // largest weight count over the valid decimation modes
     uint32_t count_selected[4];
     uint32_t kmeans[64];
     // footprint tables
@@ -51,6 +52,9 @@ struct TableLayout {
     uint32_t off_wt_count;    // u8 [ndm][64]     texels per weight
     uint32_t off_wt_start;    // u16[ndm][64]     start entry (relative to dm.wt_base)
     uint32_t off_t2w;         // u16 entries: weight index | (contribution*16) << 8
+    uint32_t off_tw4;         // u64[ndm][T]: the texel's (up to 4) entries of t2w, padded with 0
+                              // (weight 0, contribution 0), four u16 in list order
+    uint32_t off_bm_order;    // u16[nbm]: block-mode trial indices sorted by decimation mode
     uint32_t off_w2t;         // u16 entries: texel index  | (contribution*16) << 8
     uint32_t off_part_texel;  // u8 [3][1024][T]  partition of texel (P = 2..4)
     uint32_t off_part_info;   // u32[3][1024]     seed | count0<<10 | ... (see kernels)
