@@ -50,6 +50,24 @@ def rank_info():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def rank_seeds(rank):
+    """Texture seeds of one rank: blocks are independent, so each rank encodes its
+    own textures (weak scaling, no data exchange)."""
+    return [1 + 4 * rank + i for i in range(4)]
+
+
+def job_rate(texels_per_rank, rank_ms, dist=None, device=None):
+    """Whole-job Mtexel/s: all ranks' texels over the slowest rank's time."""
+    world = 1
+    if dist is not None:
+        import torch
+        t = torch.tensor([float(rank_ms)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        rank_ms = float(t.item())
+        world = dist.get_world_size()
+    return texels_per_rank * world / (rank_ms / 1000.0) / 1e6, rank_ms
+
+
 # ---------------------------------------------------------------- CPU oracle (baseline only)
 def oracle_lib():
     path = os.path.join(REPO, "oracle", "liboracle.so")
@@ -164,7 +182,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    seeds = [1 + 4 * rank + i for i in range(4)]
+    seeds = rank_seeds(rank)
     imgs = [synth.make_texture(SIZE, SIZE, s) for s in seeds]
     d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
     stream = torch.cuda.current_stream()
@@ -202,14 +220,9 @@ def main():
     t1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
+    value, ms = job_rate(texels_per_step() * args.steps, t0.elapsed_time(t1), dist, "cuda")
     if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
         dist.barrier()
-    texels = texels_per_step() * args.steps * world
-    value = texels / (ms / 1000.0) / 1e6
     launches = int(stage_n.sum())
 
     # e2e through the public host API
@@ -218,12 +231,7 @@ def main():
     for i in range(host_steps):
         for e in encs:
             e.encode(imgs[i % 4])
-    t_e2e = time.perf_counter() - t_e2e
-    if dist:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = texels_per_step() * host_steps * world / t_e2e / 1e6
+    e2e, _ = job_rate(texels_per_step() * host_steps, 1000.0 * (time.perf_counter() - t_e2e), dist, "cuda")
     h2d = SIZE * SIZE * 4 * len(FOOTPRINTS)
     d2h = sum(blocks_of(bx, by) * 16 for bx, by in FOOTPRINTS)
 
