@@ -27,7 +27,7 @@ _lib = None
 VALID_FOOTPRINTS = [(4, 4), (5, 4), (5, 5), (6, 5), (6, 6), (8, 5), (8, 6), (10, 5), (10, 6),
                     (8, 8), (10, 8), (10, 10), (12, 10), (12, 12)]
 
-OK, INVALID_FOOTPRINT, BAD_ARG, OOM, CUDA_ERROR, TIMEOUT, NO_IMAGE, IO_ERROR = range(8)
+OK, INVALID_FOOTPRINT, BAD_ARG, OOM, CUDA_ERROR, TIMEOUT, NO_IMAGE, IO_ERROR, TOO_LARGE = range(9)
 
 
 class ASTCError(RuntimeError):
@@ -68,6 +68,7 @@ def load_library():
         "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
         "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
         "astcb200_stage_times": (I32, [P, P, P]),
+        "astcb200_encode_noalloc": (I32, [I32, P, U32, U32, ctypes.c_uint8, ctypes.c_uint8, P, P]),
         "astcb200_fp32_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double)]),
         "astcb200_status_string": (ctypes.c_char_p, [I32]),
         "astcb200_last_error": (ctypes.c_char_p, [P]),
@@ -189,6 +190,13 @@ def decode(block_x, block_y, dim_x, dim_y, blocks):
     out = np.empty((dim_y, dim_x, 4), np.uint8)
     _check(lib.astcb200_decode(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, _ptr(out)))
     return out
+
+
+def encode_noalloc(device, d_rgba8, width, height, block_x, block_y, d_out_blocks, stream=0):
+    """Allocation-free encode of at most 2048 blocks between device buffers (queued on
+    `stream`, not waited for); see astcb200_encode_noalloc in include/astcb200.h."""
+    _check(load_library().astcb200_encode_noalloc(device, ctypes.c_void_p(d_rgba8), width, height, block_x, block_y,
+                                                 ctypes.c_void_p(d_out_blocks), ctypes.c_void_p(stream or None)))
 
 
 def fp32_peak_tflops(device=0):

@@ -142,6 +142,7 @@ const char* astcb200_status_string(int s) {
         case ASTCB200_TIMEOUT: return "timeout";
         case ASTCB200_NO_IMAGE: return "no image configured";
         case ASTCB200_IO_ERROR: return "file write failed";
+        case ASTCB200_TOO_LARGE: return "request exceeds the no-allocation scratch (at most 2048 blocks per call)";
         default: return "unknown status";
     }
 }

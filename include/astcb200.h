@@ -26,7 +26,8 @@ typedef enum astcb200_status {
     ASTCB200_CUDA_ERROR = 4,        /* a CUDA call failed; see astcb200_last_error */
     ASTCB200_TIMEOUT = 5,           /* the host wait exceeded astcb200_config.timeout_ms */
     ASTCB200_NO_IMAGE = 6,          /* astcb200_set_image has not been called */
-    ASTCB200_IO_ERROR = 7           /* astcb200_store_image could not write the file */
+    ASTCB200_IO_ERROR = 7,          /* astcb200_store_image could not write the file */
+    ASTCB200_TOO_LARGE = 8          /* the request exceeds astcb200_encode_noalloc's fixed scratch */
 } astcb200_status;
 
 typedef struct astcb200_ctx astcb200_ctx;
@@ -73,6 +74,19 @@ int astcb200_encode(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks
  * queued on cuda_stream (a cudaStream_t, or NULL for the context's stream) and the call
  * returns without waiting.  d_rgba8 must be 4-byte aligned, d_out_blocks 16-byte aligned. */
 int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d_out_blocks, void* cuda_stream);
+
+/* Encode without allocating (no counterpart in the reference).  For callers that cannot
+ * call cudaMalloc -- an engine whose allocator owns the device heap, code running during
+ * another component's graph capture, a plug-in in a process with a fixed allocation
+ * policy.  Inputs and outputs are the caller's device buffers (as for
+ * astcb200_encode_device); every intermediate lives in a 48 MiB file-scope device array
+ * that each GPU loading this library holds until exit.  At most 2048 blocks per call
+ * (ASTCB200_TOO_LARGE beyond).  All calls share that array: calls overlapping on the GPU
+ * race and must be serialised by the caller.  The first call on a device resolves the
+ * array's address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Work is queued on cuda_stream (NULL = the legacy default stream); no wait. */
+int astcb200_encode_noalloc(int device_ordinal, const uint8_t* d_rgba8, uint32_t width, uint32_t height,
+                            uint8_t block_x, uint8_t block_y, uint8_t* d_out_blocks, void* cuda_stream);
 
 /* Debug / parity hook: returns the chosen SymbolicBlock of every block in the reference
  * layout (astc.h:639-655, 108 u32 per block) instead of physical blocks. */

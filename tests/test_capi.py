@@ -1,0 +1,61 @@
+"""C-ABI surface that needs no GPU: symbols, status strings, argument checks."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import _libs
+import astc_implementation_b200 as ab
+
+HEADER = os.path.join(_libs.REPO, "include", "astcb200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(astcb200_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_function():
+    lib = ab.load_library()
+    names = declared_functions()
+    assert len(names) >= 14
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    lib = ab.load_library()
+    for code in range(9):
+        assert lib.astcb200_status_string(code)
+    assert b"2048" in lib.astcb200_status_string(ab.TOO_LARGE)
+
+
+def test_decode_rejects_bad_arguments():
+    lib = ab.load_library()
+    buf = np.zeros(16, np.uint8)
+    out = np.zeros(64, np.uint8)
+    assert lib.astcb200_decode(3, 3, 4, 4, buf.ctypes.data_as(ctypes.c_void_p), 16, out.ctypes.data_as(ctypes.c_void_p)) == ab.BAD_ARG
+    assert lib.astcb200_decode(4, 4, 8, 8, buf.ctypes.data_as(ctypes.c_void_p), 16, out.ctypes.data_as(ctypes.c_void_p)) == ab.BAD_ARG
+
+
+def test_store_image_io_error(tmp_path):
+    with pytest.raises(ab.ASTCError) as e:
+        ab.store_image(4, 4, 4, 4, np.zeros(16, np.uint8), str(tmp_path / "missing" / "x.astc"))
+    assert e.value.status == ab.IO_ERROR
+
+
+def test_noalloc_rejects_before_touching_the_device():
+    lib = ab.load_library()
+    # footprint and size checks come before any CUDA call
+    assert lib.astcb200_encode_noalloc(0, ctypes.c_void_p(16), 64, 64, 3, 3, ctypes.c_void_p(16), None) == ab.INVALID_FOOTPRINT
+    assert lib.astcb200_encode_noalloc(0, ctypes.c_void_p(16), 4096, 4096, 4, 4, ctypes.c_void_p(16), None) == ab.TOO_LARGE
+    assert lib.astcb200_encode_noalloc(0, None, 64, 64, 4, 4, ctypes.c_void_p(16), None) == ab.BAD_ARG
+
+
+def test_flop_model_matches_survey():
+    from astc_implementation_b200 import flop_model
+    lib = ab.load_library()
+    assert abs(flop_model.per_block(lib, 4, 4)["total"] / 1e6 - 4.29) < 0.01
+    assert abs(flop_model.per_block(lib, 6, 6)["total"] / 1e6 - 9.61) < 0.01
