@@ -246,7 +246,7 @@ struct Packer {
 };
 
 // pass15: decode packed endpoints of one partition, scaled by 257.
-__device__ __noinline__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, int32_t* e0, int32_t* e1) {
+__device__ __noinline__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, uint16_t* e0, uint16_t* e1) {
     I4 o0, o1;
     auto I = [&](int k) { return (int32_t)v[k]; };
     switch (fmt) {
@@ -281,26 +281,23 @@ __device__ __noinline__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, in
         case FMT_RGBA_DELTA: Packer::delta_unpack({I(0), I(2), I(4), I(6)}, {I(1), I(3), I(5), I(7)}, o0, o1); break;
         default: o0 = {I(0), I(0), I(0), 255}; o1 = {I(1), I(1), I(1), 255}; break;
     }
-    e0[0] = o0.x * 257; e0[1] = o0.y * 257; e0[2] = o0.z * 257; e0[3] = o0.w * 257;
-    e1[0] = o1.x * 257; e1[1] = o1.y * 257; e1[2] = o1.z * 257; e1[3] = o1.w * 257;
+    e0[0] = (uint16_t)(o0.x * 257); e0[1] = (uint16_t)(o0.y * 257); e0[2] = (uint16_t)(o0.z * 257); e0[3] = (uint16_t)(o0.w * 257);
+    e1[0] = (uint16_t)(o1.x * 257); e1[1] = (uint16_t)(o1.y * 257); e1[2] = (uint16_t)(o1.z * 257); e1[3] = (uint16_t)(o1.w * 257);
 }
 
 // ------------------------------------------------------------ k_refine
 constexpr int kRefinePBs = 16;
 constexpr int kRefineThreads = kRefinePBs * kNumCand;
 
-// Per-thread candidate state in shared memory.  Plain 4-byte members give the
-// struct an odd word stride (89 words), so a warp's threads hit distinct banks.
+// Per-thread candidate state in shared memory (41 words: an odd stride, so a
+// warp's threads hit distinct banks).  Endpoints live in per-thread local arrays.
 struct CandSmem {
-    float e0[4][4], e1[4][4], rgbs[4][4];
-    int32_t u0[4][4], u1[4][4];
+    uint16_t u0[4][4], u1[4][4];  // unpacked endpoints x257 (0..65535)
     uint8_t qw[64];
     uint8_t packed[32];
-    uint8_t packed_mod[32];
     uint32_t pad;
 };
-__device__ __forceinline__ float4 ld4(const float* p) { return make_float4(p[0], p[1], p[2], p[3]); }
-__device__ __forceinline__ void st4(float* p, float4 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w; }
+
 
 struct RTabs {
     const uint8_t* b;
@@ -345,8 +342,10 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     const float4 cw = chan_w();
     const float lsw = (cw.x + cw.y) + cw.z;
     const Packer pk{a.tables + a.L.off_cu2u};
+    float4 ep0[4], ep1[4], rgbs[4];
+    uint8_t packed_mod[32];
 #pragma unroll
-    for (int q = 0; q < 4; q++) { st4(cs.e0[q], rec.ep0[q]); st4(cs.e1[q], rec.ep1[q]); }
+    for (int q = 0; q < 4; q++) { ep0[q] = rec.ep0[q]; ep1[q] = rec.ep1[q]; }
     for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
     float top_err = ERR_DEFAULT;
     uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
@@ -364,10 +363,10 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             const int32_t w1 = f2i(rintf(w * 64.0f)), w0 = 64 - w1;
             const float4 x = px[t];
             float4 d;
-            d.x = x.x - (float)(((cs.u0[p][0] * w0) + (cs.u1[p][0] * w1) + 32) >> 6);
-            d.y = x.y - (float)(((cs.u0[p][1] * w0) + (cs.u1[p][1] * w1) + 32) >> 6);
-            d.z = x.z - (float)(((cs.u0[p][2] * w0) + (cs.u1[p][2] * w1) + 32) >> 6);
-            d.w = x.w - (float)(((cs.u0[p][3] * w0) + (cs.u1[p][3] * w1) + 32) >> 6);
+            d.x = x.x - (float)((((int32_t)cs.u0[p][0] * w0) + ((int32_t)cs.u1[p][0] * w1) + 32) >> 6);
+            d.y = x.y - (float)((((int32_t)cs.u0[p][1] * w0) + ((int32_t)cs.u1[p][1] * w1) + 32) >> 6);
+            d.z = x.z - (float)((((int32_t)cs.u0[p][2] * w0) + ((int32_t)cs.u1[p][2] * w1) + 32) >> 6);
+            d.w = x.w - (float)((((int32_t)cs.u0[p][3] * w0) + ((int32_t)cs.u1[p][3] * w1) + 32) >> 6);
             d = vmin(make_float4(fabsf(d.x), fabsf(d.y), fabsf(d.z), fabsf(d.w)), mk(1e15f));
             total = total + fminf(dot4(d * d, cw), ERR_DEFAULT);
         }
@@ -415,16 +414,16 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             const float lx = ls * lsw, my = ms * lsw, rz = rs * lsw;
             const float scalediv = clampf(smin / fmaxf(smax, 1e-10f), 0.0f, 1.0f);
             const float4 sds = sdir * smax;
-            st4(cs.rgbs[q], make_float4(sds.x, sds.y, sds.z, scalediv));
+            rgbs[q] = make_float4(sds.x, sds.y, sds.z, scalediv);
             if (wmin >= wmax * 0.999f) {
                 const float4 ac = (colx + coly) / vmax(cw * ps, mk(1e-17f));
-                float4 e0 = ld4(cs.e0[q]), e1 = ld4(cs.e1[q]);
+                float4 e0 = ep0[q], e1 = ep1[q];
                 if (ac.x == ac.x) { e0.x = ac.x; e1.x = ac.x; }
                 if (ac.y == ac.y) { e0.y = ac.y; e1.y = ac.y; }
                 if (ac.z == ac.z) { e0.z = ac.z; e1.z = ac.z; }
                 if (ac.w == ac.w) { e0.w = ac.w; e1.w = ac.w; }
-                st4(cs.e0[q], e0); st4(cs.e1[q], e1);
-                st4(cs.rgbs[q], make_float4(sds.x, sds.y, sds.z, 1.0f));
+                ep0[q] = e0; ep1[q] = e1;
+                rgbs[q] = make_float4(sds.x, sds.y, sds.z, 1.0f);
             } else {
                 const float4 det = (lv * rv) - (mv * mv);
                 const float4 rdet = mk(1.0f) / det;
@@ -433,17 +432,17 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 const float lsmss = ((lx * lx) + 2.0f * (my * my)) + (rz * rz);
                 const float4 ne0 = ((rv * colx) - (mv * coly)) * rdet;
                 const float4 ne1 = ((lv * coly) - (mv * colx)) * rdet;
-                float4 e0 = ld4(cs.e0[q]), e1 = ld4(cs.e1[q]);
+                float4 e0 = ep0[q], e1 = ep1[q];
                 if (fabsf(det.x) > (mss.x * 1e-4f) && ne0.x == ne0.x && ne1.x == ne1.x) { e0.x = ne0.x; e1.x = ne1.x; }
                 if (fabsf(det.y) > (mss.y * 1e-4f) && ne0.y == ne0.y && ne1.y == ne1.y) { e0.y = ne0.y; e1.y = ne1.y; }
                 if (fabsf(det.z) > (mss.z * 1e-4f) && ne0.z == ne0.z && ne1.z == ne1.z) { e0.z = ne0.z; e1.z = ne1.z; }
                 if (fabsf(det.w) > (mss.w * 1e-4f) && ne0.w == ne0.w && ne1.w == ne1.w) { e0.w = ne0.w; e1.w = ne1.w; }
-                st4(cs.e0[q], e0); st4(cs.e1[q], e1);
+                ep0[q] = e0; ep1[q] = e1;
                 const float se0 = ((rz * sv0) - (my * sv1)) * lsrdet;
                 const float se1 = ((lx * sv1) - (my * sv0)) * lsrdet;
                 if ((fabsf(lsdet) > (lsmss * 1e-4f)) && se0 == se0 && se1 == se1 && se0 < se1) {
                     const float4 sdsm = sdir * se1;
-                    st4(cs.rgbs[q], make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1));
+                    rgbs[q] = make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1);
                 }
             }
         }
@@ -454,7 +453,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             for (int i = 0; i < 32; i++) cs.packed[i] = 0;
 #pragma unroll 1
             for (int q = 0; q < P; q++) {
-                const uint32_t f = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), ld4(cs.rgbs[q]), ci.fmt[q], ci.ql, vals);
+                const uint32_t f = pk.pack(ep0[q], ep1[q], rgbs[q], ci.fmt[q], ci.ql, vals);
                 fn[0] = q == 0 ? f : fn[0]; fn[1] = q == 1 ? f : fn[1]; fn[2] = q == 2 ? f : fn[2]; fn[3] = q == 3 ? f : fn[3];
 #pragma unroll
                 for (int i = 0; i < 8; i++) cs.packed[q * 8 + i] = (uint8_t)vals[i];
@@ -463,11 +462,11 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             bool m = false;
             if (P >= 2 && all_same) {
                 uint32_t fm[4] = {0, 0, 0, 0};
-                uint8_t* vm = cs.packed_mod;
+                uint8_t* vm = packed_mod;
                 bool same_mod = true;
 #pragma unroll 1
                 for (int q = 0; q < P; q++) {
-                    const uint32_t f = pk.pack(ld4(cs.e0[q]), ld4(cs.e1[q]), ld4(cs.rgbs[q]), ci.fmt[q], ci.qlm, vals);
+                    const uint32_t f = pk.pack(ep0[q], ep1[q], rgbs[q], ci.fmt[q], ci.qlm, vals);
                     fm[0] = q == 0 ? f : fm[0]; fm[1] = q == 1 ? f : fm[1]; fm[2] = q == 2 ? f : fm[2]; fm[3] = q == 3 ? f : fm[3];
 #pragma unroll
                     for (int i = 0; i < 8; i++) vm[q * 8 + i] = (uint8_t)vals[i];
@@ -497,8 +496,8 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 const uint32_t pn = tb.prev_next(bm.quant, uqw);
                 const int32_t dn = pn & 0xFF, up = (pn >> 8) & 0xFF;
                 const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
-                const float4 offs = make_float4((float)(cs.u1[p][0] - cs.u0[p][0]), (float)(cs.u1[p][1] - cs.u0[p][1]),
-                                                (float)(cs.u1[p][2] - cs.u0[p][2]), (float)(cs.u1[p][3] - cs.u0[p][3])) * (1.0f / 64.0f);
+                const float4 offs = make_float4((float)((int32_t)cs.u1[p][0] - (int32_t)cs.u0[p][0]), (float)((int32_t)cs.u1[p][1] - (int32_t)cs.u0[p][1]),
+                                                (float)((int32_t)cs.u1[p][2] - (int32_t)cs.u0[p][2]), (float)((int32_t)cs.u1[p][3] - (int32_t)cs.u0[p][3])) * (1.0f / 64.0f);
                 const float4 cd = (base + offs * (float)uqw) - px[t];
                 const float4 cdd = cd + offs * (float)(dn - uqw), cdu = cd + offs * (float)(up - uqw);
                 const float eb = dot4(cd * cd, cw), ed = dot4(cdd * cdd, cw), eu = dot4(cdu * cdu, cw);
@@ -528,8 +527,8 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                     }
                     const int p = tp[t];
                     const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
-                    const float4 offs = make_float4((float)(cs.u1[p][0] - cs.u0[p][0]), (float)(cs.u1[p][1] - cs.u0[p][1]),
-                                                    (float)(cs.u1[p][2] - cs.u0[p][2]), (float)(cs.u1[p][3] - cs.u0[p][3])) * (1.0f / 64.0f);
+                    const float4 offs = make_float4((float)((int32_t)cs.u1[p][0] - (int32_t)cs.u0[p][0]), (float)((int32_t)cs.u1[p][1] - (int32_t)cs.u0[p][1]),
+                                                    (float)((int32_t)cs.u1[p][2] - (int32_t)cs.u0[p][2]), (float)((int32_t)cs.u1[p][3] - (int32_t)cs.u0[p][3])) * (1.0f / 64.0f);
                     const float4 cd = (base + offs * wb) - px[t];
                     const float4 cdd = cd + offs * (ddn * twb), cdu = cd + offs * (dup * twb);
                     ebv = ebv + cd * cd; edv = edv + cdd * cdd; euv = euv + cdu * cdu;
