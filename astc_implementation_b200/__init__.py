@@ -18,7 +18,8 @@ import os
 
 import numpy as np
 
-__all__ = ["ASTCEncoder", "ASTCError", "store_image", "decode", "load_library", "VALID_FOOTPRINTS"]
+__all__ = ["ASTCEncoder", "ASTCError", "store_image", "decode", "load_library", "VALID_FOOTPRINTS", "Texture",
+           "downsample_device", "mip_dims"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libastcb200.so")
@@ -47,6 +48,20 @@ class Stats(ctypes.Structure):
                 ("launches", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class Texture(ctypes.Structure):
+    """astcb200_texture: one texture of a batch."""
+    _fields_ = [("rgba8", ctypes.c_void_p), ("out_blocks", ctypes.c_void_p), ("out_len", ctypes.c_size_t),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("block_x", ctypes.c_uint8),
+                ("block_y", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("chunk_blocks", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("ms", ctypes.c_double)]
+
+
+FLAG_STAGE_TIMING, FLAG_NO_GRAPH = 1, 2
+
+
 def load_library():
     """Loads libastcb200.so, building it first when it is missing."""
     global _lib
@@ -70,6 +85,11 @@ def load_library():
         "astcb200_stage_times": (I32, [P, P, P]),
         "astcb200_encode_noalloc": (I32, [I32, P, U32, U32, ctypes.c_uint8, ctypes.c_uint8, P, P]),
         "astcb200_fp32_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double)]),
+        "astcb200_encode_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Stats)]),
+        "astcb200_encode_batch_device": (I32, [P, ctypes.POINTER(Texture), U32, P]),
+        "astcb200_autotune_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Tuning), ctypes.POINTER(Tuning),
+                                          U32, ctypes.POINTER(U32)]),
+        "astcb200_downsample_device": (I32, [P, U32, U32, P, P]),
         "astcb200_status_string": (ctypes.c_char_p, [I32]),
         "astcb200_last_error": (ctypes.c_char_p, [P]),
     }
@@ -98,9 +118,10 @@ def _ptr(a):
 class ASTCEncoder:
     """One encoder context bound to one GPU and one CUDA stream."""
 
-    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False):
+    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False, use_graphs=True):
         lib = load_library()
-        cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, 1 if stage_timing else 0)
+        flags = (FLAG_STAGE_TIMING if stage_timing else 0) | (0 if use_graphs else FLAG_NO_GRAPH)
+        cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, flags)
         ctx = ctypes.c_void_p()
         _check(lib.astcb200_create(ctypes.byref(ctx), device, ctypes.byref(cfg)))
         self._ctx = ctx
@@ -157,6 +178,49 @@ class ASTCEncoder:
         _check(lib.astcb200_encode_device(self._ctx, ctypes.c_void_p(d_rgba8), ctypes.c_void_p(d_out_blocks),
                                           ctypes.c_void_p(stream or None)), self._ctx)
 
+    def encode_batch(self, textures):
+        """Encodes [(rgba8 (h, w, 4) uint8, block_x, block_y), ...] as one batch; returns the
+        blocks of each texture (uint8 arrays of blocks*16 bytes) in the same order."""
+        lib = load_library()
+        imgs, outs = [], []
+        arr = (Texture * len(textures))()
+        for i, (img, bx, by) in enumerate(textures):
+            img = np.ascontiguousarray(img, dtype=np.uint8)
+            h, w = img.shape[0], img.shape[1]
+            out = np.empty(((w + bx - 1) // bx) * ((h + by - 1) // by) * 16, np.uint8)
+            imgs.append(img)
+            outs.append(out)
+            arr[i] = Texture(img.ctypes.data, out.ctypes.data, out.size, w, h, bx, by)
+        st = Stats()
+        _check(lib.astcb200_encode_batch(self._ctx, arr, len(textures), ctypes.byref(st)), self._ctx)
+        self.last_stats = st
+        return outs
+
+    @staticmethod
+    def _device_textures(textures):
+        arr = (Texture * len(textures))()
+        for i, (d_img, w, h, bx, by, d_out, out_len) in enumerate(textures):
+            arr[i] = Texture(d_img, d_out, out_len, w, h, bx, by)
+        return arr
+
+    def encode_batch_device(self, textures, stream=0):
+        """Queues a batch of device textures [(d_rgba8, w, h, bx, by, d_out, out_len), ...]
+        (integer device addresses) on `stream`; does not wait."""
+        arr = self._device_textures(textures)
+        _check(load_library().astcb200_encode_batch_device(self._ctx, arr, len(textures), ctypes.c_void_p(stream or None)),
+               self._ctx)
+
+    def autotune_batch(self, textures):
+        """Times the launch configurations on a device batch (as for encode_batch_device) and
+        keeps the fastest for batches of this shape.  Returns (best, tried) as
+        (chunk_blocks, streams, ms) tuples."""
+        arr = self._device_textures(textures)
+        best, tried, n = Tuning(), (Tuning * 32)(), ctypes.c_uint32()
+        _check(load_library().astcb200_autotune_batch(self._ctx, arr, len(textures), ctypes.byref(best), tried, 32,
+                                                      ctypes.byref(n)), self._ctx)
+        return ((best.chunk_blocks, best.streams, best.ms),
+                [(tried[i].chunk_blocks, tried[i].streams, tried[i].ms) for i in range(n.value)])
+
     def stage_times(self):
         """(ms[4], launches[4]) per kernel for the last encode (needs stage_timing=True)."""
         ms = np.zeros(4, np.float32)
@@ -197,6 +261,22 @@ def encode_noalloc(device, d_rgba8, width, height, block_x, block_y, d_out_block
     `stream`, not waited for); see astcb200_encode_noalloc in include/astcb200.h."""
     _check(load_library().astcb200_encode_noalloc(device, ctypes.c_void_p(d_rgba8), width, height, block_x, block_y,
                                                  ctypes.c_void_p(d_out_blocks), ctypes.c_void_p(stream or None)))
+
+
+def downsample_device(d_src, width, height, d_dst, stream=0):
+    """Queues one 2x2 box-filter mip step between device RGBA8 buffers (integer addresses);
+    the result is max(1, width//2) x max(1, height//2)."""
+    _check(load_library().astcb200_downsample_device(ctypes.c_void_p(d_src), width, height, ctypes.c_void_p(d_dst),
+                                                     ctypes.c_void_p(stream or None)))
+
+
+def mip_dims(width, height):
+    """Sizes of the full mip chain of a width x height image, level 0 first, down to 1x1."""
+    dims = [(width, height)]
+    while dims[-1] != (1, 1):
+        w, h = dims[-1]
+        dims.append((max(1, w // 2), max(1, h // 2)))
+    return dims
 
 
 def fp32_peak_tflops(device=0):

@@ -13,71 +13,26 @@
 #include <thread>
 #include <vector>
 
-#include "astcb200.h"
-#include "kernels.h"
-#include "tables.h"
+#include "ctx.h"
 
 using namespace astcb200;
 
-struct astcb200_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    astcb200_config cfg{};
-    uint32_t width = 0, height = 0, bx = 0, by = 0, nbx = 0, nby = 0, nblocks = 0;
-    bool have_image = false;
-    TableLayout L{};
-    int tables_bx = 0, tables_by = 0;
-    uint8_t* d_tables = nullptr;
-    uint32_t chunk = 65536;
-    PartPicks* d_picks = nullptr;
-    PBRec* d_pbrec = nullptr;
-    Snap* d_snaps = nullptr;
-    uint8_t* d_img = nullptr;
-    size_t img_cap = 0;
-    uint8_t* d_out = nullptr;
-    size_t out_cap = 0;
-    uint32_t* d_sym = nullptr;
-    size_t sym_cap = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> stage_ev;  // 5 per chunk: before the first kernel and after each
-    int stage_chunks = 0;               // chunks recorded by the last encode
-    uint32_t stage_n[4] = {0, 0, 0, 0};
-    std::string err;
-};
-
-namespace {
+namespace astcb200 {
 
 int cuda_fail(astcb200_ctx* c, cudaError_t e, const char* what) {
     if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? ASTCB200_OOM : ASTCB200_CUDA_ERROR;
 }
-#define CK(call, what)                                    \
-    do {                                                  \
-        cudaError_t e_ = (call);                          \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
-    } while (0)
 
-template <class T>
-int ensure(astcb200_ctx* ctx, T*& p, size_t& cap, size_t need, const char* what) {
-    if (cap >= need && p) return ASTCB200_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    cudaError_t e = cudaMalloc((void**)&p, need);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
-    cap = need;
-    return ASTCB200_OK;
-}
-
-// Bounded host wait on the context's stream (astcb200_config.timeout_ms).
-int wait_stream(astcb200_ctx* ctx) {
+// Bounded host wait on stream s (astcb200_config.timeout_ms).
+int wait_stream(astcb200_ctx* ctx, cudaStream_t s) {
     if (ctx->cfg.timeout_ms == 0) {
-        CK(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+        CK(cudaStreamSynchronize(s), "cudaStreamSynchronize");
         return ASTCB200_OK;
     }
     const auto t0 = std::chrono::steady_clock::now();
     for (;;) {
-        cudaError_t e = cudaStreamQuery(ctx->stream);
+        cudaError_t e = cudaStreamQuery(s);
         if (e == cudaSuccess) return ASTCB200_OK;
         if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "cudaStreamQuery");
         const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -86,15 +41,49 @@ int wait_stream(astcb200_ctx* ctx) {
     }
 }
 
+// Tables of footprint bx x by on the context's device, built and uploaded on first use.
+int get_tables(astcb200_ctx* ctx, int bx, int by, const FootTables** out) {
+    for (const FootTables* f : ctx->feet)
+        if (f->bx == bx && f->by == by) { *out = f; return ASTCB200_OK; }
+    std::vector<uint8_t> blob;
+    FootTables* f = new FootTables();
+    f->bx = bx; f->by = by;
+    if (!build_tables(bx, by, f->L, blob)) { delete f; return ASTCB200_INVALID_FOOTPRINT; }
+    cudaError_t e = cudaMalloc((void**)&f->d, blob.size());
+    if (e == cudaSuccess) e = cudaMemcpy(f->d, blob.data(), blob.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = configure_kernels(f->L);
+    if (e != cudaSuccess) { cudaFree(f->d); delete f; return cuda_fail(ctx, e, "upload tables"); }
+    ctx->feet.push_back(f);
+    *out = f;
+    return ASTCB200_OK;
+}
+
+int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots) {
+    int rc;
+    if ((rc = ensure_buf(ctx, sc.picks, sc.cap_picks, blocks * sizeof(PartPicks), "cudaMalloc picks"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.pbrec, sc.cap_rec, blocks * slots * sizeof(PBRec), "cudaMalloc records"))) return rc;
+    return ensure_buf(ctx, sc.snaps, sc.cap_snap, blocks * slots * kNumCand * sizeof(Snap), "cudaMalloc snapshots");
+}
+
+void free_scratch(Scratch& sc) {
+    cudaFree(sc.picks); cudaFree(sc.pbrec); cudaFree(sc.snaps);
+    sc = Scratch();
+}
+
+}  // namespace astcb200
+
+namespace {
+
 int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t* d_sym, cudaStream_t s, uint32_t* launches) {
     KernelArgs a;
     std::memset(&a, 0, sizeof(a));
     a.img = d_img;
     a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
-    a.tables = ctx->d_tables;
-    a.L = ctx->L;
-    a.picks = ctx->d_picks; a.pbrec = ctx->d_pbrec; a.snaps = ctx->d_snaps;
+    a.tables = ctx->cur->d;
+    a.L = ctx->cur->L;
+    a.picks = ctx->scratch.picks; a.pbrec = ctx->scratch.pbrec; a.snaps = ctx->scratch.snaps;
     a.out_blocks = d_out; a.symbolic = d_sym;
+    a.slots = kSlotsPerBlock; a.topn = kNumCand;
     uint32_t n = 0;
     const bool timing = (ctx->cfg.flags & ASTCB200_FLAG_STAGE_TIMING) != 0;
     const int nchunks = (int)((ctx->nblocks + ctx->chunk - 1) / ctx->chunk);
@@ -173,7 +162,9 @@ int astcb200_destroy(astcb200_ctx* ctx) {
     if (!ctx) return ASTCB200_BAD_ARG;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->d_tables); cudaFree(ctx->d_picks); cudaFree(ctx->d_pbrec); cudaFree(ctx->d_snaps);
+    release_batches(ctx);
+    free_scratch(ctx->scratch);
+    for (FootTables* f : ctx->feet) { cudaFree(f->d); delete f; }
     cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -189,28 +180,13 @@ int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8
     const uint64_t nbx = (width + block_x - 1) / block_x, nby = (height + block_y - 1) / block_y;
     if (nbx * nby > 0x7FFFFFFFull) return ASTCB200_BAD_ARG;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    if (ctx->tables_bx != block_x || ctx->tables_by != block_y || !ctx->d_tables) {
-        std::vector<uint8_t> blob;
-        TableLayout L;
-        if (!build_tables(block_x, block_y, L, blob)) return ASTCB200_INVALID_FOOTPRINT;
-        if (ctx->d_tables) { cudaFree(ctx->d_tables); ctx->d_tables = nullptr; }
-        CK(cudaMalloc((void**)&ctx->d_tables, blob.size()), "cudaMalloc tables");
-        CK(cudaMemcpy(ctx->d_tables, blob.data(), blob.size(), cudaMemcpyHostToDevice), "upload tables");
-        CK(configure_kernels(L), "configure kernels");
-        ctx->L = L;
-        ctx->tables_bx = block_x; ctx->tables_by = block_y;
-    }
+    const FootTables* ft = nullptr;
+    int rc = get_tables(ctx, block_x, block_y, &ft);
+    if (rc) return rc;
+    ctx->cur = ft;
     ctx->width = width; ctx->height = height; ctx->bx = block_x; ctx->by = block_y;
     ctx->nbx = (uint32_t)nbx; ctx->nby = (uint32_t)nby; ctx->nblocks = (uint32_t)(nbx * nby);
-    const size_t chunk = std::min<size_t>(ctx->chunk, ctx->nblocks);
-    size_t cap_picks = 0, cap_rec = 0, cap_snap = 0;
-    if (ctx->d_picks) { cudaFree(ctx->d_picks); ctx->d_picks = nullptr; }
-    if (ctx->d_pbrec) { cudaFree(ctx->d_pbrec); ctx->d_pbrec = nullptr; }
-    if (ctx->d_snaps) { cudaFree(ctx->d_snaps); ctx->d_snaps = nullptr; }
-    int rc;
-    if ((rc = ensure(ctx, ctx->d_picks, cap_picks, chunk * sizeof(PartPicks), "cudaMalloc picks"))) return rc;
-    if ((rc = ensure(ctx, ctx->d_pbrec, cap_rec, chunk * kSlotsPerBlock * sizeof(PBRec), "cudaMalloc records"))) return rc;
-    if ((rc = ensure(ctx, ctx->d_snaps, cap_snap, chunk * kSlotsPerBlock * kNumCand * sizeof(Snap), "cudaMalloc snapshots"))) return rc;
+    if ((rc = ensure_scratch(ctx, ctx->scratch, std::min<size_t>(ctx->chunk, ctx->nblocks), kSlotsPerBlock))) return rc;
     ctx->have_image = true;
     return ASTCB200_OK;
 }
@@ -236,9 +212,9 @@ static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blo
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const size_t in_bytes = (size_t)ctx->width * ctx->height * 4, out_bytes = (size_t)ctx->nblocks * 16;
     int rc;
-    if ((rc = ensure(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
-    if ((rc = ensure(ctx, ctx->d_out, ctx->out_cap, out_bytes, "cudaMalloc output"))) return rc;
-    if (symbolic && (rc = ensure(ctx, ctx->d_sym, ctx->sym_cap, (size_t)ctx->nblocks * 108 * 4, "cudaMalloc symbolic"))) return rc;
+    if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
+    if ((rc = ensure_buf(ctx, ctx->d_out, ctx->out_cap, out_bytes, "cudaMalloc output"))) return rc;
+    if (symbolic && (rc = ensure_buf(ctx, ctx->d_sym, ctx->sym_cap, (size_t)ctx->nblocks * 108 * 4, "cudaMalloc symbolic"))) return rc;
     CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
     CK(cudaEventRecord(ctx->ev0, ctx->stream), "event");
     uint32_t launches = 0;
@@ -246,7 +222,7 @@ static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blo
     CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
     if (out_blocks) CK(cudaMemcpyAsync(out_blocks, ctx->d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H blocks");
     if (symbolic) CK(cudaMemcpyAsync(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H symbolic");
-    if ((rc = wait_stream(ctx))) return rc;
+    if ((rc = wait_stream(ctx, ctx->stream))) return rc;
     if (stats) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);

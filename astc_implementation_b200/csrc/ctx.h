@@ -1,0 +1,111 @@
+// Encoder context shared by the single-image entry points (capi.cu) and the
+// batched ones (batch.cu).  Host-side only.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "astcb200.h"
+#include "kernels.h"
+#include "tables.h"
+
+namespace astcb200 {
+
+// Tables of one footprint, uploaded once per context.
+struct FootTables {
+    int bx = 0, by = 0;
+    TableLayout L{};
+    uint8_t* d = nullptr;
+};
+
+// Per-chunk intermediates of one launch stream: partition picks, 13
+// partitioned-block records and 104 candidate snapshots per block.
+struct Scratch {
+    PartPicks* picks = nullptr;
+    PBRec* pbrec = nullptr;
+    Snap* snaps = nullptr;
+    size_t cap_picks = 0, cap_rec = 0, cap_snap = 0;
+};
+
+// A batch shape: texture sizes and footprints in call order.
+using BatchShape = std::vector<uint32_t>;
+
+// A captured batch: the graph of one batch shape and launch configuration.
+struct BatchGraph {
+    uint32_t chunk = 0, streams = 0;
+    std::vector<const void*> bufs;  // device buffers baked into the graph
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;
+};
+
+struct BatchTuning {
+    uint32_t chunk = 0, streams = 0;
+};
+
+}  // namespace astcb200
+
+struct astcb200_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    astcb200_config cfg{};
+    uint32_t width = 0, height = 0, bx = 0, by = 0, nbx = 0, nby = 0, nblocks = 0;
+    bool have_image = false;
+    const astcb200::FootTables* cur = nullptr;      // tables of the set_image footprint
+    std::vector<astcb200::FootTables*> feet;        // every footprint used so far
+    uint32_t chunk = 65536;
+    astcb200::Scratch scratch;                      // single-image scratch
+    uint8_t* d_img = nullptr;
+    size_t img_cap = 0;
+    uint8_t* d_out = nullptr;
+    size_t out_cap = 0;
+    uint32_t* d_sym = nullptr;
+    size_t sym_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> stage_ev;  // 5 per chunk: before the first kernel and after each
+    int stage_chunks = 0;               // chunks recorded by the last encode
+    uint32_t stage_n[4] = {0, 0, 0, 0};
+    // batches
+    std::vector<cudaStream_t> branch;                // extra streams of batched launches
+    std::vector<cudaEvent_t> fork_ev, join_ev;
+    std::vector<astcb200::Scratch> bscratch;         // one per batch stream
+    astcb200::TexSeg* d_segs = nullptr;
+    size_t segs_cap = 0;
+    uint8_t* d_bin = nullptr;                        // host-pointer batches: staged inputs
+    size_t bin_cap = 0;
+    uint8_t* d_bout = nullptr;                       // and outputs
+    size_t bout_cap = 0;
+    std::map<astcb200::BatchShape, astcb200::BatchGraph> graphs;
+    std::map<astcb200::BatchShape, astcb200::BatchTuning> tuned;
+    std::string err;
+};
+
+namespace astcb200 {
+
+int cuda_fail(astcb200_ctx* c, cudaError_t e, const char* what);
+int wait_stream(astcb200_ctx* ctx, cudaStream_t s);
+int get_tables(astcb200_ctx* ctx, int bx, int by, const FootTables** out);
+int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots);
+void free_scratch(Scratch& sc);
+void release_batches(astcb200_ctx* ctx);
+
+template <class T>
+int ensure_buf(astcb200_ctx* ctx, T*& p, size_t& cap, size_t need, const char* what) {
+    if (cap >= need && p) return ASTCB200_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)&p, need);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    cap = need;
+    return ASTCB200_OK;
+}
+
+}  // namespace astcb200
+
+#define CK(call, what)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)

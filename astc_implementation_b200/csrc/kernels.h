@@ -10,11 +10,18 @@
 
 namespace astcb200 {
 
-constexpr int kSlotsPerBlock = 13;
+constexpr int kSlotsPerBlock = 13;   // full search: P = 1 plus 4 partitionings for each of P = 2, 3, 4
+constexpr int kMaxProposals = 16;    // proposal search: P = 1 plus up to 16 proposed partitionings
+constexpr int kMaxSlots = 1 + kMaxProposals;
+constexpr int kMaskWords = 4;        // block-mode masks cover up to 256 block modes
 
 // Partitionings picked by the partition search for one block and P = 2..4:
 // picks[(P-2)*5 + i] = table entry (i < 4), picks[(P-2)*5 + 4] = count.
 struct PartPicks { uint16_t v[15]; uint16_t pad; };
+
+// Partitionings proposed for one block (proposal search): v[i] = (P - 2) << 10 | table entry,
+// best first; slot 1 + i of the block searches v[i].
+struct PropPicks { uint16_t n, pad; uint16_t v[kMaxProposals]; };
 
 // Initial state of one refinement candidate (pass12 output).
 struct CandInit {
@@ -42,18 +49,87 @@ struct Snap {
     uint8_t qw[64];
 };
 
-struct KernelArgs {
+// One texture of a batch as the kernels address it.  A batch launch numbers
+// the blocks of all its textures (one footprint) consecutively: texture i owns
+// blocks [block_base, block_base + nbx * nby).
+struct TexSeg {
     const uint8_t* img;       // RGBA8, row-major, device memory
+    uint8_t* out;             // its 16-byte blocks, row-major
+    int width, height, nbx, block_base;
+};
+
+struct KernelArgs {
+    const uint8_t* img;       // RGBA8, row-major, device memory (single image: nsegs == 0)
     int width, height, nbx, nby;
     int block_first, nblocks; // the chunk of blocks handled by this launch sequence
+    const TexSeg* segs;       // batch textures sorted by block_base (nsegs > 0), device memory
+    int nsegs;
     const uint8_t* tables;    // device table blob
     TableLayout L;
     PartPicks* picks;         // [nblocks]
-    PBRec* pbrec;             // [nblocks * 13]
-    Snap* snaps;              // [nblocks * 13 * 8]
+    PBRec* pbrec;             // [nblocks * slots]
+    Snap* snaps;              // [nblocks * slots * 8]
     uint8_t* out_blocks;      // [total blocks * 16], indexed by global block index
     uint32_t* symbolic;       // optional [total blocks * 108]
+    int slots;                // partitioned blocks per block: 13 (full search) or 1 + kMaxProposals
+    int topn;                 // refinement candidates kept per partitioned block (<= 8)
+    // Block lists (proposal search and its full-search fallback): the chunk's
+    // blocks are block_list[block_first + lb] while block_first + lb < *block_count.
+    const int* block_list;
+    const int* block_count;
+    const PropPicks* prop;    // per list position: proposed partitionings (replaces the partition search)
+    const uint64_t* bm_mask;  // per list position and P = 1..4: block modes the front evaluates
 };
+
+// Global index of the chunk's lb-th block, or -1 past the end of a block list.
+__host__ __device__ inline int chunk_block(const KernelArgs& a, int lb) {
+    const int pos = a.block_first + lb;
+    if (!a.block_list) return pos;
+    return pos < *a.block_count ? a.block_list[pos] : -1;
+}
+
+#ifdef __CUDACC__
+// Where block blk's texels come from: the image, its size and the block's
+// top-left texel.
+struct BlockSrc {
+    const uchar4* img;
+    int width, height, x0, y0;
+    int seg;  // batch texture index, -1 for a single image
+};
+
+__device__ __forceinline__ BlockSrc block_src(const KernelArgs& a, int blk) {
+    if (a.nsegs == 0) {
+        const int bxi = blk % a.nbx, byi = blk / a.nbx;
+        return {reinterpret_cast<const uchar4*>(a.img), a.width, a.height, bxi * a.L.bx, byi * a.L.by, -1};
+    }
+    int lo = 0, hi = a.nsegs - 1;  // last texture whose first block is <= blk
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.segs[mid].block_base <= blk) lo = mid; else hi = mid - 1;
+    }
+    const TexSeg& s = a.segs[lo];
+    const int local = blk - s.block_base;
+    const int bxi = local % s.nbx, byi = local / s.nbx;
+    return {reinterpret_cast<const uchar4*>(s.img), s.width, s.height, bxi * a.L.bx, byi * a.L.by, lo};
+}
+
+// Texel t of the block, edge-clamped, as (v / 255) * 65536 (compression_pipeline.cpp:32-46).
+__device__ __forceinline__ float4 src_texel(const BlockSrc& s, int bx, int t) {
+    const int x = min(s.x0 + t % bx, s.width - 1);
+    const int y = min(s.y0 + t / bx, s.height - 1);
+    const uchar4 p = s.img[(size_t)y * s.width + x];
+    return make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
+                       ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
+}
+
+// Destination of block blk's 16 bytes.
+__device__ __forceinline__ uint4* block_dst(const KernelArgs& a, int blk) {
+    if (a.nsegs == 0) return reinterpret_cast<uint4*>(a.out_blocks) + blk;
+    const BlockSrc s = block_src(a, blk);
+    const TexSeg& t = a.segs[s.seg];
+    return reinterpret_cast<uint4*>(t.out) + (blk - t.block_base);
+}
+#endif
 
 // Shared-memory sizes the launches need for one footprint.
 size_t front_smem_bytes(const TableLayout& L);

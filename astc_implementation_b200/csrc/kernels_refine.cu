@@ -11,6 +11,9 @@
 //                  counts (compression_pipeline.cpp:500-519), then the ASTC
 //                  physical block layout (code/physical_compression.cpp:843)
 //                  written straight to the 16-byte output block.
+#include <algorithm>
+#include <mutex>
+
 #include "device_math.cuh"
 #include "kernels.h"
 
@@ -554,24 +557,22 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     const int tid = threadIdx.x;
     // slot-major order: consecutive CTAs hold partitioned blocks of the same slot
     // (hence the same partition count), so co-resident warps run the same code
-    const int npb = a.nblocks * kSlotsPerBlock;
+    const int npb = a.nblocks * a.slots;
     {
         const int pbl = tid / kNumCand, k = tid % kNumCand;
         const int li = blockIdx.x * kRefinePBs + pbl;
         int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
-        if (li < npb) {
+        const int blk = li < npb ? chunk_block(a, li % a.nblocks) : -1;
+        if (blk >= 0) {
             const int slot = li / a.nblocks, lb = li % a.nblocks;
-            const PBRec& r = a.pbrec[lb * kSlotsPerBlock + slot];
+            const PBRec& r = a.pbrec[lb * a.slots + slot];
             if (k < (int)r.ncand) key = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
             if (r.ncand > 0) {
-                const int P = r.P, blk = a.block_first + lb;
+                const int P = r.P;
                 const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
-                const int bxi = blk % a.nbx, byi = blk / a.nbx;
+                const BlockSrc src = block_src(a, blk);
                 for (int t = k; t < T; t += kNumCand) {
-                    const int x = min(bxi * a.L.bx + t % a.L.bx, a.width - 1), y = min(byi * a.L.by + t / a.L.bx, a.height - 1);
-                    const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
-                    pxs[pbl * T + t] = make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
-                                                   ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
+                    pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
                     tps[pbl * T + t] = P > 1 ? prow[t] : 0;
                 }
             }
@@ -595,7 +596,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     const int li = blockIdx.x * kRefinePBs + pbl;
     if (li >= npb) return;
     const int slot = li / a.nblocks, lb = li % a.nblocks;
-    const int pb = lb * kSlotsPerBlock + slot;
+    if (chunk_block(a, lb) < 0) return;
+    const int pb = lb * a.slots + slot;
     const PBRec& rec = a.pbrec[pb];
     Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
     snap->err = ERR_DEFAULT;  // inert slot unless refined below
@@ -674,14 +676,15 @@ __device__ __forceinline__ int bitrev8(int p) {
 __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ KernelArgs a) {
     const int lb = blockIdx.x * blockDim.x + threadIdx.x;
     if (lb >= a.nblocks) return;
-    const int blk = a.block_first + lb;
+    const int blk = chunk_block(a, lb);
+    if (blk < 0) return;
     float best = 1e30f;
     int win_slot = -1, win_k = 0;
-    for (int s = 0; s < kSlotsPerBlock; s++) {
-        const PBRec& r = a.pbrec[(size_t)lb * kSlotsPerBlock + s];
+    for (int s = 0; s < a.slots; s++) {
+        const PBRec& r = a.pbrec[(size_t)lb * a.slots + s];
         const int n = r.ncand;
         for (int k = 0; k < n; k++) {
-            const float e = a.snaps[((size_t)lb * kSlotsPerBlock + s) * kNumCand + k].err;
+            const float e = a.snaps[((size_t)lb * a.slots + s) * kNumCand + k].err;
             if (e < best) { best = e; win_slot = s; win_k = k; }
         }
     }
@@ -692,8 +695,8 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
     const Snap* sn = nullptr;
     const PBRec* rec = nullptr;
     if (win_slot >= 0) {
-        rec = &a.pbrec[(size_t)lb * kSlotsPerBlock + win_slot];
-        sn = &a.snaps[((size_t)lb * kSlotsPerBlock + win_slot) * kNumCand + win_k];
+        rec = &a.pbrec[(size_t)lb * a.slots + win_slot];
+        sn = &a.snaps[((size_t)lb * a.slots + win_slot) * kNumCand + win_k];
         const DevBm bm = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[sn->bm];
         const DevDm dm = reinterpret_cast<const DevDm*>(a.tables + a.L.off_dm)[bm.dm];
         const uint32_t pc = rec->P, q = bm.quant;
@@ -750,7 +753,7 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
     o.y = blockbytes[4] | (blockbytes[5] << 8) | (blockbytes[6] << 16) | ((uint32_t)blockbytes[7] << 24);
     o.z = blockbytes[8] | (blockbytes[9] << 8) | (blockbytes[10] << 16) | ((uint32_t)blockbytes[11] << 24);
     o.w = blockbytes[12] | (blockbytes[13] << 8) | (blockbytes[14] << 16) | ((uint32_t)blockbytes[15] << 24);
-    reinterpret_cast<uint4*>(a.out_blocks)[blk] = o;
+    *block_dst(a, blk) = o;
     if (a.symbolic) {
         uint32_t* s = a.symbolic + (size_t)blk * 108;
         if (win_slot < 0) sym[0] = __float_as_uint(1e30f);
@@ -766,16 +769,31 @@ size_t refine_smem_bytes(const TableLayout& L) {
            kRefineThreads * 4 + (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
 }
 
-cudaError_t configure_search_kernels(const TableLayout& L);
+cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes);
+constexpr int kMaxConfigDevices = 64;
 
+// The dynamic shared-memory limit is a per-function attribute shared by every
+// context and thread of the process; it only ever grows (per device), so
+// launches for different footprints may be queued concurrently.
 cudaError_t configure_kernels(const TableLayout& L) {
-    cudaError_t e = configure_search_kernels(L);
+    static std::mutex mu;
+    static size_t limit[kMaxConfigDevices][3];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)refine_smem_bytes(L));
+    if (dev < 0 || dev >= kMaxConfigDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(mu);
+    size_t* m = limit[dev];
+    const size_t need[3] = {search_smem_bytes(L), front_smem_bytes(L), refine_smem_bytes(L)};
+    if (need[0] <= m[0] && need[1] <= m[1] && need[2] <= m[2]) return cudaSuccess;
+    for (int i = 0; i < 3; i++) m[i] = std::max(m[i], need[i]);
+    e = configure_search_kernels(m[0], m[1]);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m[2]);
 }
 
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
-    const int npb = a.nblocks * kSlotsPerBlock;
+    const int npb = a.nblocks * a.slots;
     k_refine<<<(npb + kRefinePBs - 1) / kRefinePBs, kRefineThreads, refine_smem_bytes(a.L), s>>>(a);
     return cudaGetLastError();
 }

@@ -55,17 +55,6 @@ struct Tabs {
     __device__ float bqe(int i) const { return reinterpret_cast<const float*>(b + L->off_bqe)[i]; }
 };
 
-// Texel t of block blk, edge-clamped, as (v / 255) * 65536 (compression_pipeline.cpp:32-46).
-__device__ __forceinline__ float4 load_texel(const KernelArgs& a, int blk, int t) {
-    const int bx = a.L.bx, by = a.L.by;
-    const int bxi = blk % a.nbx, byi = blk / a.nbx;
-    const int x = min(bxi * bx + t % bx, a.width - 1);
-    const int y = min(byi * by + t / bx, a.height - 1);
-    const uchar4 p = reinterpret_cast<const uchar4*>(a.img)[(size_t)y * a.width + x];
-    return make_float4(((float)p.x / 255.0f) * 65536.0f, ((float)p.y / 255.0f) * 65536.0f,
-                       ((float)p.z / 255.0f) * 65536.0f, ((float)p.w / 255.0f) * 65536.0f);
-}
-
 __device__ __forceinline__ float dist_sq(float4 a, float4 b) {
     const float4 d = a - b;
     return dot4(d * d, chan_w());
@@ -84,7 +73,8 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
     float* eu = reinterpret_cast<float*>(ws + 144 * 16 + 1024 * 8);
     float* es = eu + 128;
     uint8_t* asg = reinterpret_cast<uint8_t*>(es + 128);
-    for (int t = lane; t < T; t += 32) px[t] = load_texel(a, blk, t);
+    const BlockSrc src = block_src(a, blk);
+    for (int t = lane; t < T; t += 32) px[t] = src_texel(src, a.L.bx, t);
     __syncwarp();
 
     // pass001: farthest-point initial centres; ties pick the highest texel index
@@ -341,9 +331,11 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
     if (item >= a.nblocks * 3) return;
     const int lb = item % a.nblocks, P = item / a.nblocks + 2;  // P-major: a CTA's warps share P
     uint8_t* ws = smem + warp * kSearchWarpBytes;
-    if (P == 2) search_one<2>(a, a.block_first + lb, lb, ws, lane);
-    else if (P == 3) search_one<3>(a, a.block_first + lb, lb, ws, lane);
-    else search_one<4>(a, a.block_first + lb, lb, ws, lane);
+    const int blk = chunk_block(a, lb);
+    if (blk < 0) return;
+    if (P == 2) search_one<2>(a, blk, lb, ws, lane);
+    else if (P == 3) search_one<3>(a, blk, lb, ws, lane);
+    else search_one<4>(a, blk, lb, ws, lane);
 }
 
 // ============================================================ passes 01-12
@@ -351,7 +343,7 @@ constexpr int kFrontThreads = 128;
 constexpr int kFrontWarps = kFrontThreads / 32;
 
 struct FrontLayout {
-    int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, total;
+    int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, dml, total;
 };
 constexpr int kScratchPerWarp = 144 * 4 + 64 * 4 + 16 * 4 + 16 * 20;
 
@@ -389,6 +381,7 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.ccr_fmt = take16(o, nbm * 4);
     f.qf = take16(o, max_w * kFrontThreads * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
+    f.dml = take16(o, 16 + ndm * 2);
     f.total = o;
     return f;
 }
@@ -427,11 +420,10 @@ __device__ __forceinline__ int bm_quant_weight(const Tabs& tb, const BmQuant& s,
     return v;
 }
 
-__device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in_block, uint32_t entry, uint8_t* sm) {
+__device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, int slot_in_block, uint32_t entry, uint8_t* sm) {
     const Tabs tb{a.tables, &a.L};
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int blk = a.block_first + lb;
     const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w);
     float4* px = reinterpret_cast<float4*>(sm + fl.px);
     float* iw = reinterpret_cast<float*>(sm + fl.w);
@@ -450,8 +442,9 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
     const float4 cw = chan_w();
 
     const uint8_t* prow = P > 1 ? tb.part_texels(P, entry) : nullptr;
+    const BlockSrc src = block_src(a, blk);
     for (int t = tid; t < T; t += kFrontThreads) {
-        px[t] = load_texel(a, blk, t);
+        px[t] = src_texel(src, a.L.bx, t);
         tp[t] = P > 1 ? prow[t] : 0;
     }
     __syncthreads();
@@ -511,6 +504,29 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
     __syncthreads();
     const bool is_const = M.is_const != 0;
 
+    // Block-mode subset of the proposal search: only its modes and their
+    // decimation modes are evaluated; the others never become candidates.
+    const uint64_t* bmm = a.bm_mask ? a.bm_mask + ((size_t)lb * 4 + (P - 1)) * kMaskWords : nullptr;
+    int ndm_run = ndm;
+    const int16_t* dm_run = nullptr;
+    if (bmm) {
+        uint32_t* flags = reinterpret_cast<uint32_t*>(sm + fl.dml);  // 4 words: one bit per decimation mode
+        int16_t* list = reinterpret_cast<int16_t*>(sm + fl.dml + 16);
+        if (tid < 4) flags[tid] = 0;
+        __syncthreads();
+        for (int i = tid; i < nbm; i += kFrontThreads)
+            if ((bmm[i >> 6] >> (i & 63)) & 1) { const int d = tb.bm(i).dm; atomicOr(&flags[d >> 5], 1u << (d & 31)); }
+        __syncthreads();
+        if (tid == 0) {
+            int n = 0;
+            for (int d = 0; d < ndm; d++) if ((flags[d >> 5] >> (d & 31)) & 1) list[n++] = (int16_t)d;
+            flags[0] = n;  // the flags are no longer needed
+        }
+        __syncthreads();
+        ndm_run = (int)flags[0];
+        dm_run = list;
+    }
+
     // ---------------- passes 02-05, one warp per decimation mode
     {
         uint8_t* scr = sm + fl.scratch + warp * kScratchPerWarp;
@@ -518,7 +534,8 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
         uint32_t* smp = reinterpret_cast<uint32_t*>(scr + 144 * 4);
         float* ang = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4);
         float* lh = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4 + 16 * 4);  // [16][5]: lowest, span, err, cl, ch
-        for (int m = warp; m < ndm; m += kFrontWarps) {
+        for (int mi = warp; mi < ndm_run; mi += kFrontWarps) {
+            const int m = dm_run ? dm_run[mi] : mi;
             const DevDm dmi = tb.dm(m);
             const int W = dmi.W;
             float* dw = dec + m * 64;
@@ -632,6 +649,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
     // ---------------- pass07: weight quantisation error per block mode
     for (int j = tid; j < nbm; j += kFrontThreads) {
         const int i = tb.bm_order(j);  // neighbouring threads get modes of the same decimation
+        if (bmm && !((bmm[i >> 6] >> (i & 63)) & 1)) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
         const DevBm bm = tb.bm(i);
         const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
         if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
@@ -819,10 +837,10 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int slot_in
         if (rank < kNumCand) M.top[rank] = i;
     }
     __syncthreads();
-    PBRec& rec = a.pbrec[(size_t)lb * kSlotsPerBlock + slot_in_block];
+    PBRec& rec = a.pbrec[(size_t)lb * a.slots + slot_in_block];
     if (tid == 0) {
         int n = 0;
-        while (n < kNumCand && M.top[n] >= 0) n++;
+        while (n < a.topn && M.top[n] >= 0) n++;
         M.ncand = n;
         rec.P = P; rec.entry = entry; rec.ncand = n;
         rec.seed = P > 1 ? tb.part_seed(P, entry) : 0;
@@ -855,16 +873,30 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__
     extern __shared__ __align__(16) uint8_t smem[];
     // slot-major order so that co-resident CTAs work on the same partition count
     const int li = blockIdx.x;
-    if (li >= a.nblocks * kSlotsPerBlock) return;
+    if (li >= a.nblocks * a.slots) return;
     const int k = li / a.nblocks, lb = li % a.nblocks;
-    if (k == 0) { front_body(a, 1, lb, 0, 0, smem); return; }
-    const int P = 2 + (k - 1) / 4, i = (k - 1) % 4;
-    const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
-    if (i >= pk[4]) {
-        if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * kSlotsPerBlock + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
+    const int blk = chunk_block(a, lb);
+    if (blk < 0) return;
+    if (k == 0) { front_body(a, 1, lb, blk, 0, 0, smem); return; }
+    int P, entry;
+    bool present;
+    if (a.prop) {
+        const PropPicks& pp = a.prop[lb];
+        present = k - 1 < (int)pp.n;
+        const int v = present ? pp.v[k - 1] : 0;
+        P = 2 + (v >> 10); entry = v & 1023;
+    } else {
+        P = 2 + (k - 1) / 4;
+        const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
+        const int i = (k - 1) % 4;
+        present = i < pk[4];
+        entry = present ? pk[i] : 0;
+    }
+    if (!present) {
+        if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * a.slots + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
         return;
     }
-    front_body(a, P, lb, k, pk[i], smem);
+    front_body(a, P, lb, blk, k, entry, smem);
 }
 
 }  // namespace
@@ -872,10 +904,10 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__
 size_t search_smem_bytes(const TableLayout&) { return (size_t)kSearchWarps * kSearchWarpBytes; }
 size_t front_smem_bytes(const TableLayout& L) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w).total; }
 
-cudaError_t configure_search_kernels(const TableLayout& L) {
-    cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_smem_bytes(L));
+cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(L));
+    return cudaFuncSetAttribute(k_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
 }
 
 cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
@@ -886,7 +918,7 @@ cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
-    k_front<<<a.nblocks * kSlotsPerBlock, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
+    k_front<<<a.nblocks * a.slots, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
     return cudaGetLastError();
 }
 

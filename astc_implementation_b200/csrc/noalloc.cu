@@ -97,6 +97,8 @@ extern "C" int astcb200_encode_noalloc(int device, const uint8_t* d_rgba8, uint3
     a.snaps = reinterpret_cast<Snap*>(base + off);
     a.out_blocks = d_out_blocks;
     a.symbolic = nullptr;
+    a.slots = kSlotsPerBlock;
+    a.topn = kNumCand;
     // Every record the kernels read is written earlier in the same call (absent
     // partitioned blocks get ncand = 0, unrefined candidates err = 1e37), so the
     // previous call's contents need no clearing.

@@ -17,6 +17,8 @@ search.  The metric is Mtexel/s over both encodes.
               bounded sample of the same workload, all host threads, rank 0.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                [--size S] [--footprints 4x4,6x6]      smaller cases (profiling)
+                [--workload batch]                      64 mixed textures, batched vs per-texture
 """
 import argparse
 import ctypes
@@ -157,8 +159,96 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- batched workload
+def batch_textures(count=64, seed=3):
+    """64 textures with log-uniform sides in 64..2048 (independently per axis, so
+    non-square and with edges that are not multiples of the block size), footprints
+    4x4 / 6x6 / 8x8 uniformly, generator seeds 1000+i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        w, h = (int(round(np.exp(rng.uniform(np.log(64), np.log(2048))))) for _ in range(2))
+        bx = int(rng.choice([4, 6, 8]))
+        out.append((w, h, bx, bx, 1000 + i))
+    return out
+
+
+def run_batch(args):
+    """Batched encoder (one graph-captured launch sequence per footprint queue, autotuned)
+    against per-texture launches of the same textures, both device-resident."""
+    import torch
+    import astc_implementation_b200 as ab
+    from astc_implementation_b200 import synth
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    spec = batch_textures()
+    imgs = [synth.make_texture(w, h, seed) for w, h, _, _, seed in spec]
+    d_in = [torch.from_numpy(im.reshape(-1)).cuda() for im in imgs]
+    nblk = [((w + bx - 1) // bx) * ((h + by - 1) // by) for w, h, bx, by, _ in spec]
+    d_out = [torch.empty(n * 16, dtype=torch.uint8, device="cuda") for n in nblk]
+    desc = [(d_in[i].data_ptr(), w, h, bx, by, d_out[i].data_ptr(), nblk[i] * 16) for i, (w, h, bx, by, _) in enumerate(spec)]
+    texels = sum(w * h for w, h, _, _, _ in spec)
+    # a created stream: handle 0 (the legacy default stream) would select the encoder's own stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    enc = ab.ASTCEncoder(device=local)
+    best, tried = enc.autotune_batch(desc)
+
+    def timed(fn):
+        for i in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            fn()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / args.steps
+
+    ms_batch = timed(lambda: enc.encode_batch_device(desc, stream.cuda_stream))
+    per = {}
+    for fp in sorted({(bx, by) for _, _, bx, by, _ in spec}):
+        per[fp] = ab.ASTCEncoder(device=local)
+
+    def per_texture():
+        for i, (w, h, bx, by, _) in enumerate(spec):
+            e = per[(bx, by)]
+            e.secondaryInit(w, h, bx, by)
+            e.encode_device(d_in[i].data_ptr(), d_out[i].data_ptr(), stream.cuda_stream)
+
+    ms_single = timed(per_texture)
+    clocks = ClockSampler(local)
+    ms_batch2 = timed(lambda: enc.encode_batch_device(desc, stream.cuda_stream))
+    clk = clocks.stop()
+    ms_batch = min(ms_batch, ms_batch2)
+    value = texels / (ms_batch / 1000.0) / 1e6
+    line = {
+        "metric": "Mtexel/s, batched full search (64 mixed textures)", "value": round(value, 3), "unit": "Mtexel/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "64 textures, log-uniform sides 64-2048 per axis, footprints 4x4/6x6/8x8 uniform, seeds 1000-1063",
+                   "texels": texels, "blocks": int(sum(nblk)), "l2": "512 MiB memset before every step, inside the timed region"},
+        "per_texture_launches": {"value": round(texels / (ms_single / 1000.0) / 1e6, 3), "ms_per_step": round(ms_single, 3)},
+        "speedup_vs_per_texture": round(ms_single / ms_batch, 3),
+        "autotune": {"best": {"chunk_blocks": best[0], "streams": best[1], "ms": round(best[2], 3)},
+                     "tried": [{"chunk_blocks": c, "streams": s_, "ms": round(m, 3)} for c, s_, m in tried]},
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    enc.close()
+    for e in per.values():
+        e.close()
+    return 0
+
+
 # ---------------------------------------------------------------- B200 arm
 def main():
+    global SIZE, FOOTPRINTS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -166,9 +256,16 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline crop")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=SIZE, help="texture side (default: the 2048x2048 workload)")
+    ap.add_argument("--footprints", default="4x4,6x6")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch"])
     args = ap.parse_args()
+    SIZE = args.size
+    FOOTPRINTS = [tuple(int(v) for v in f.split("x")) for f in args.footprints.split(",")]
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
 
     import torch
     import astc_implementation_b200 as ab
@@ -185,7 +282,9 @@ def main():
     seeds = rank_seeds(rank)
     imgs = [synth.make_texture(SIZE, SIZE, s) for s in seeds]
     d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
-    stream = torch.cuda.current_stream()
+    # a created stream: handle 0 (the legacy default stream) would select the encoder's own stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     encs, outs = [], []
     for bx, by in FOOTPRINTS:
         e = ab.ASTCEncoder(device=local, stage_timing=True)
@@ -256,7 +355,10 @@ def main():
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(names[dom])
+        per_block = json.load(open(tpath)).get(names[dom], {}).get("dram_bytes_per_block")
+        if per_block:  # measured DRAM bytes per block (ncu) x blocks per launch
+            blocks = sum(blocks_of(*fp) for fp in FOOTPRINTS) * args.steps
+            traffic = round(per_block * blocks / max(dom_launches, 1))
     cpu = None
     if not args.no_cpu_baseline:
         rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample)
@@ -267,9 +369,10 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": "Mtexel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "2048x2048 RGBA8 synthetic texture (seeds 1-4 per rank), full search at 4x4 and 6x6 per step",
+        "config": {"workload": "%dx%d RGBA8 synthetic texture (seeds 1-4 per rank), full search at %s per step"
+                               % (SIZE, SIZE, " and ".join("%dx%d" % f for f in FOOTPRINTS)),
                    "method": "full search (plain, no learned proposal)", "image": [SIZE, SIZE],
-                   "footprints": ["4x4", "6x6"], "l2": "512 MiB memset before every step, inside the timed region",
+                   "footprints": ["%dx%d" % f for f in FOOTPRINTS], "l2": "512 MiB memset before every step, inside the timed region",
                    "parallelism": "replicas" if world > 1 else "single"},
         "per_footprint_ms": {"%dx%d" % fp: round(float(stage_ms[k].sum() / args.steps), 3) for k, fp in enumerate(FOOTPRINTS)},
         "stage_ms_per_step": {names[i]: round(float(tot_ms[i] / args.steps), 3) for i in range(4)},

@@ -42,6 +42,8 @@ typedef struct astcb200_config {
 /* Record CUDA events around every kernel launch (on the launching stream) so that
  * astcb200_stage_times reports per-kernel device time. */
 #define ASTCB200_FLAG_STAGE_TIMING 1u
+/* Batched encodes launch their kernels directly instead of replaying a captured CUDA graph. */
+#define ASTCB200_FLAG_NO_GRAPH 2u
 
 typedef struct astcb200_stats {
     double ms_wall;       /* host time of the call */
@@ -87,6 +89,52 @@ int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d
  * Work is queued on cuda_stream (NULL = the legacy default stream); no wait. */
 int astcb200_encode_noalloc(int device_ordinal, const uint8_t* d_rgba8, uint32_t width, uint32_t height,
                             uint8_t block_x, uint8_t block_y, uint8_t* d_out_blocks, void* cuda_stream);
+
+/* One texture of a batch (no reference counterpart: the reference encodes one image per
+ * ASTCEncoder::encode call).  out_blocks receives ceil(width/block_x)*ceil(height/block_y)*16
+ * bytes of physical blocks in raster order; out_len must be at least that. */
+typedef struct astcb200_texture {
+    const uint8_t* rgba8;  /* width*height*4 bytes, rows of width texels */
+    uint8_t* out_blocks;
+    size_t out_len;
+    uint32_t width, height;
+    uint8_t block_x, block_y; /* any of the 14 footprints; a batch may mix them */
+    uint8_t reserved[6];
+} astcb200_texture;
+
+/* Encodes n textures of any sizes and footprints as one batch: the blocks of all textures
+ * with the same footprint form one work queue searched by one launch sequence per chunk, the
+ * footprints' queues run on concurrent streams, and the whole sequence is captured once per
+ * batch shape (sizes and footprints) into a CUDA graph that later calls replay.  Host
+ * pointers; blocks until the blocks are in out_blocks.  Each texture gets exactly the blocks
+ * astcb200_encode gives it alone. */
+int astcb200_encode_batch(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n, astcb200_stats* stats);
+
+/* Same with rgba8 and out_blocks in device memory of the context's GPU (rgba8 4-byte
+ * aligned, out_blocks 16-byte aligned); queued on cuda_stream (NULL = the context's
+ * stream), no wait.  The textures array itself is host memory and is consumed before the
+ * call returns. */
+int astcb200_encode_batch_device(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n, void* cuda_stream);
+
+/* Launch configuration of a batch shape, chosen by astcb200_autotune_batch. */
+typedef struct astcb200_tuning {
+    uint32_t chunk_blocks; /* blocks per launch sequence within one footprint's queue */
+    uint32_t streams;      /* concurrent streams the footprints' queues are spread over */
+    double ms;             /* device time of one batch with this configuration */
+} astcb200_tuning;
+
+/* Times every candidate configuration (chunk_blocks x streams) on this batch (device
+ * pointers, as for astcb200_encode_batch_device; the outputs are written), keeps the
+ * fastest for later batches of the same shape and returns it in best.  Candidates tried
+ * are written to tried[0..*n_tried) when tried is not NULL (capacity max_tried).  Blocks. */
+int astcb200_autotune_batch(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n,
+                            astcb200_tuning* best, astcb200_tuning* tried, uint32_t max_tried, uint32_t* n_tried);
+
+/* Box-filters a device RGBA8 image to the next mip level: dst is max(1, width/2) x
+ * max(1, height/2) texels, each the rounded mean (sum + 2) / 4 of the 2x2 source texels at
+ * (2x, 2y)..(2x+1, 2y+1), source coordinates clamped to the image.  Queued on cuda_stream;
+ * no wait.  (No reference counterpart: the reference encodes the image it is given.) */
+int astcb200_downsample_device(const uint8_t* d_src, uint32_t width, uint32_t height, uint8_t* d_dst, void* cuda_stream);
 
 /* Debug / parity hook: returns the chosen SymbolicBlock of every block in the reference
  * layout (astc.h:639-655, 108 u32 per block) instead of physical blocks. */
