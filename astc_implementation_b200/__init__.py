@@ -62,6 +62,19 @@ class Tuning(ctypes.Structure):
 FLAG_STAGE_TIMING, FLAG_NO_GRAPH = 1, 2
 
 
+class ProposalNet(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("block_x", ctypes.c_uint8), ("block_y", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8 * 2), ("inputs", ctypes.c_uint32), ("hidden", ctypes.c_uint32),
+                ("outputs", ctypes.c_uint32), ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p),
+                ("b2", ctypes.c_void_p), ("w3", ctypes.c_void_p), ("b3", ctypes.c_void_p)]
+
+
+class Pruning(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("enable", ctypes.c_uint32), ("max_partitionings", ctypes.c_uint32),
+                ("block_modes", ctypes.c_uint32), ("refine_candidates", ctypes.c_uint32), ("coverage", ctypes.c_float),
+                ("threshold", ctypes.c_float)]
+
+
 def load_library():
     """Loads libastcb200.so, building it first when it is missing."""
     global _lib
@@ -90,6 +103,17 @@ def load_library():
         "astcb200_autotune_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Tuning), ctypes.POINTER(Tuning),
                                           U32, ctypes.POINTER(U32)]),
         "astcb200_downsample_device": (I32, [P, U32, U32, P, P]),
+        "astcb200_proposal_layout": (I32, [ctypes.c_uint8, ctypes.c_uint8] + [ctypes.POINTER(U32)] * 6 + [P]),
+        "astcb200_set_proposal_net": (I32, [P, ctypes.POINTER(ProposalNet)]),
+        "astcb200_set_pruning": (I32, [P, ctypes.POINTER(Pruning)]),
+        "astcb200_pruning_stats": (I32, [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+        "astcb200_proposal_logits": (I32, [P, P, P, SZ]),
+        "astcb200_train_gemm": (I32, [P, P, P, I32, I32, I32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                      P, I32, I32, P]),
+        "astcb200_train_xent": (I32, [P, U32, P, P, U32, U32, U32, P, P, P, P]),
+        "astcb200_train_relu_backward": (I32, [P, P, SZ, P]),
+        "astcb200_train_colsum": (I32, [P, P, U32, U32, P]),
+        "astcb200_train_adam": (I32, [P, P, P, P, SZ, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, U32, P]),
         "astcb200_status_string": (ctypes.c_char_p, [I32]),
         "astcb200_last_error": (ctypes.c_char_p, [P]),
     }
@@ -220,6 +244,34 @@ class ASTCEncoder:
                                                       ctypes.byref(n)), self._ctx)
         return ((best.chunk_blocks, best.streams, best.ms),
                 [(tried[i].chunk_blocks, tried[i].streams, tried[i].ms) for i in range(n.value)])
+
+    def set_proposal_net(self, w, block_x=None, block_y=None):
+        """Loads a trained proposal network (dict of FP32 w1, b1, w2, b2, w3, b3) for a footprint."""
+        bx, by = (block_x, block_y) if block_x else w["footprint"]
+        arrs = {k: np.ascontiguousarray(w[k], dtype=np.float32) for k in ("w1", "b1", "w2", "b2", "w3", "b3")}
+        net = ProposalNet(ctypes.sizeof(ProposalNet), bx, by, (ctypes.c_uint8 * 2)(), arrs["w1"].shape[1], arrs["w1"].shape[0],
+                          arrs["w3"].shape[0], *[arrs[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")])
+        _check(load_library().astcb200_set_proposal_net(self._ctx, ctypes.byref(net)), self._ctx)
+
+    def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=4, coverage=0.95,
+                    threshold=0.5):
+        """Proposal-search settings for later encodes of footprints with a network."""
+        cfg = Pruning(ctypes.sizeof(Pruning), 1 if enable else 0, max_partitionings, block_modes, refine_candidates,
+                      coverage, threshold)
+        _check(load_library().astcb200_set_pruning(self._ctx, ctypes.byref(cfg)), self._ctx)
+
+    def pruning_stats(self):
+        """(proposal-search blocks, full-search blocks) of the last encode."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load_library().astcb200_pruning_stats(self._ctx, ctypes.byref(a), ctypes.byref(b)), self._ctx)
+        return a.value, b.value
+
+    def proposal_logits(self, imageData, outputs):
+        """The proposal network's logits (numBlocks, outputs) for an image (test hook)."""
+        img = self._image(imageData)
+        z = np.empty((self.numBlocks, outputs), np.float32)
+        _check(load_library().astcb200_proposal_logits(self._ctx, _ptr(img), _ptr(z), z.size), self._ctx)
+        return z
 
     def stage_times(self):
         """(ms[4], launches[4]) per kernel for the last encode (needs stage_timing=True)."""

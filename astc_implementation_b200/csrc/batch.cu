@@ -117,18 +117,26 @@ int prepare(astcb200_ctx* ctx, const Plan& p, uint32_t chunk, uint32_t streams) 
     }
     if (ctx->bscratch.size() < streams) ctx->bscratch.resize(streams);
     const size_t need = std::min<size_t>(chunk, p.max_group_blocks);
-    for (uint32_t i = 0; i < streams; i++) {
-        int rc = ensure_scratch(ctx, ctx->bscratch[i], need, kSlotsPerBlock);
-        if (rc) return rc;
-    }
+    for (uint32_t i = 0; i < streams; i++)
+        for (const Group& g : p.groups) {  // sized for the largest need over the footprints
+            int rc = ensure_chunk_scratch(ctx, ctx->bscratch[i], need, g.ft);
+            if (rc) return rc;
+        }
+    size_t units = 0;
+    for (const Group& g : p.groups) units += (g.nblocks + chunk - 1) / chunk;
+    int rc = begin_routes(ctx, units);
+    if (rc) return rc;
     return ensure_buf(ctx, ctx->d_segs, ctx->segs_cap, p.segs.size() * sizeof(TexSeg), "cudaMalloc batch descriptors");
 }
 
 // Device buffers a launch sequence with `streams` streams bakes in.
 std::vector<const void*> baked_buffers(const astcb200_ctx* ctx, uint32_t streams) {
-    std::vector<const void*> v{ctx->d_segs};
+    std::vector<const void*> v{ctx->d_segs, ctx->d_counts, ctx->d_mlp_error};
     for (uint32_t i = 0; i < streams; i++) {
-        v.push_back(ctx->bscratch[i].picks); v.push_back(ctx->bscratch[i].pbrec); v.push_back(ctx->bscratch[i].snaps);
+        const Scratch& sc = ctx->bscratch[i];
+        for (const void* q : {(const void*)sc.picks, (const void*)sc.pbrec, (const void*)sc.snaps, (const void*)sc.logits,
+                              (const void*)sc.lists, (const void*)sc.prop, (const void*)sc.masks})
+            v.push_back(q);
     }
     return v;
 }
@@ -143,25 +151,18 @@ int enqueue(astcb200_ctx* ctx, const Plan& p, cudaStream_t s, uint32_t chunk, ui
         for (uint32_t i = 1; i < streams; i++) CK(cudaStreamWaitEvent(st[i], ctx->fork_ev[0], 0), "fork wait");
     }
     uint32_t unit = 0, n = 0;
+    ctx->counts_used = 0;
     for (const Group& g : p.groups) {
         for (uint32_t first = 0; first < g.nblocks; first += chunk, unit++) {
             const uint32_t k = unit % streams;
-            const Scratch& sc = ctx->bscratch[k];
             KernelArgs a;
             std::memset(&a, 0, sizeof(a));
             a.segs = ctx->d_segs + g.first_seg;
             a.nsegs = (int)g.nsegs;
-            a.tables = g.ft->d;
-            a.L = g.ft->L;
-            a.picks = sc.picks; a.pbrec = sc.pbrec; a.snaps = sc.snaps;
-            a.slots = kSlotsPerBlock; a.topn = kNumCand;
             a.block_first = (int)first;
             a.nblocks = (int)std::min<uint32_t>(chunk, g.nblocks - first);
-            CK(launch_partition_search(a, st[k]), "k_partition_search");
-            CK(launch_front(a, st[k]), "k_front");
-            CK(launch_refine(a, st[k]), "k_refine");
-            CK(launch_select_pack(a, st[k]), "k_select_pack");
-            n += 4;
+            int rc = enqueue_chunk(ctx, a, g.ft, ctx->bscratch[k], st[k], nullptr, nullptr, &n);
+            if (rc) return rc;
         }
     }
     if (streams > 1) {
@@ -209,12 +210,14 @@ int launch_plan(astcb200_ctx* ctx, Plan& p, cudaStream_t s, const BatchTuning& t
         cudaError_t e = cudaStreamEndCapture(s, &g);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+        bg.routes = ctx->counts_used;
         e = cudaGraphInstantiate(&bg.exec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
         it = ctx->graphs.emplace(p.shape, bg).first;
     }
     CK(cudaGraphLaunch(it->second.exec, s), "cudaGraphLaunch");
+    ctx->counts_used = it->second.routes;
     if (launches) *launches = it->second.launches;
     return ASTCB200_OK;
 }

@@ -67,6 +67,7 @@ int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots) {
 
 void free_scratch(Scratch& sc) {
     cudaFree(sc.picks); cudaFree(sc.pbrec); cudaFree(sc.snaps);
+    cudaFree(sc.logits); cudaFree(sc.lists); cudaFree(sc.prop); cudaFree(sc.masks);
     sc = Scratch();
 }
 
@@ -79,39 +80,30 @@ int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t
     std::memset(&a, 0, sizeof(a));
     a.img = d_img;
     a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
-    a.tables = ctx->cur->d;
-    a.L = ctx->cur->L;
-    a.picks = ctx->scratch.picks; a.pbrec = ctx->scratch.pbrec; a.snaps = ctx->scratch.snaps;
     a.out_blocks = d_out; a.symbolic = d_sym;
-    a.slots = kSlotsPerBlock; a.topn = kNumCand;
-    uint32_t n = 0;
     const bool timing = (ctx->cfg.flags & ASTCB200_FLAG_STAGE_TIMING) != 0;
     const int nchunks = (int)((ctx->nblocks + ctx->chunk - 1) / ctx->chunk);
+    int rc = ensure_chunk_scratch(ctx, ctx->scratch, std::min<size_t>(ctx->chunk, ctx->nblocks), ctx->cur);
+    if (rc) return rc;
+    if ((rc = begin_routes(ctx, nchunks))) return rc;
+    constexpr int E = kStageIntervals + 1;
     if (timing) {
-        while ((int)ctx->stage_ev.size() < 5 * nchunks) {
+        while ((int)ctx->stage_ev.size() < E * nchunks) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e), "cudaEventCreate");
             ctx->stage_ev.push_back(e);
         }
+        ctx->stage_kind.assign((size_t)kStageIntervals * nchunks, -1);
         ctx->stage_chunks = nchunks;
     }
-    for (int k = 0; k < 4; k++) ctx->stage_n[k] = 0;
+    uint32_t n = 0;
     int c = 0;
     for (uint32_t first = 0; first < ctx->nblocks; first += ctx->chunk, c++) {
         a.block_first = (int)first;
         a.nblocks = (int)std::min<uint32_t>(ctx->chunk, ctx->nblocks - first);
-        cudaEvent_t* ev = timing ? &ctx->stage_ev[5 * c] : nullptr;
-        if (timing) CK(cudaEventRecord(ev[0], s), "stage event");
-        CK(launch_partition_search(a, s), "k_partition_search");
-        if (timing) CK(cudaEventRecord(ev[1], s), "stage event");
-        CK(launch_front(a, s), "k_front");
-        if (timing) CK(cudaEventRecord(ev[2], s), "stage event");
-        CK(launch_refine(a, s), "k_refine");
-        if (timing) CK(cudaEventRecord(ev[3], s), "stage event");
-        CK(launch_select_pack(a, s), "k_select_pack");
-        if (timing) CK(cudaEventRecord(ev[4], s), "stage event");
-        for (int k = 0; k < 4; k++) ctx->stage_n[k]++;
-        n += 4;
+        if ((rc = enqueue_chunk(ctx, a, ctx->cur, ctx->scratch, s, timing ? &ctx->stage_ev[(size_t)E * c] : nullptr,
+                                timing ? &ctx->stage_kind[(size_t)kStageIntervals * c] : nullptr, &n)))
+            return rc;
     }
     if (launches) *launches = n;
     return ASTCB200_OK;
@@ -165,6 +157,8 @@ int astcb200_destroy(astcb200_ctx* ctx) {
     release_batches(ctx);
     free_scratch(ctx->scratch);
     for (FootTables* f : ctx->feet) { cudaFree(f->d); delete f; }
+    for (NetDev* nd : ctx->nets) { cudaFree(nd->mem); delete nd; }
+    cudaFree(ctx->d_counts); cudaFree(ctx->d_mlp_error);
     cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -186,7 +180,6 @@ int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8
     ctx->cur = ft;
     ctx->width = width; ctx->height = height; ctx->bx = block_x; ctx->by = block_y;
     ctx->nbx = (uint32_t)nbx; ctx->nby = (uint32_t)nby; ctx->nblocks = (uint32_t)(nbx * nby);
-    if ((rc = ensure_scratch(ctx, ctx->scratch, std::min<size_t>(ctx->chunk, ctx->nblocks), kSlotsPerBlock))) return rc;
     ctx->have_image = true;
     return ASTCB200_OK;
 }
@@ -252,14 +245,19 @@ int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* 
 
 int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* n4) {
     if (!ctx || !ms4) return ASTCB200_BAD_ARG;
-    for (int k = 0; k < 4; k++) { ms4[k] = 0.0f; if (n4) n4[k] = ctx->stage_n[k]; }
+    for (int k = 0; k < 4; k++) { ms4[k] = 0.0f; if (n4) n4[k] = 0; }
     if (ctx->stage_chunks == 0) return ASTCB200_OK;
-    CK(cudaEventSynchronize(ctx->stage_ev[5 * ctx->stage_chunks - 1]), "stage event");
+    constexpr int E = kStageIntervals + 1;
     for (int c = 0; c < ctx->stage_chunks; c++)
-        for (int k = 0; k < 4; k++) {
+        for (int i = 0; i < kStageIntervals; i++) {
+            const int k = ctx->stage_kind[(size_t)kStageIntervals * c + i];
+            if (k < 0) break;
+            cudaEvent_t e1 = ctx->stage_ev[(size_t)E * c + i + 1];
+            CK(cudaEventSynchronize(e1), "stage event");
             float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, ctx->stage_ev[5 * c + k], ctx->stage_ev[5 * c + k + 1]), "cudaEventElapsedTime");
+            CK(cudaEventElapsedTime(&ms, ctx->stage_ev[(size_t)E * c + i], e1), "cudaEventElapsedTime");
             ms4[k] += ms;
+            if (n4) n4[k]++;
         }
     return ASTCB200_OK;
 }

@@ -9,6 +9,7 @@
 
 #include "astcb200.h"
 #include "kernels.h"
+#include "mlp.h"
 #include "tables.h"
 
 namespace astcb200 {
@@ -27,6 +28,25 @@ struct Scratch {
     PBRec* pbrec = nullptr;
     Snap* snaps = nullptr;
     size_t cap_picks = 0, cap_rec = 0, cap_snap = 0;
+    // proposal search: logits and the routes of one chunk
+    float* logits = nullptr;
+    int* lists = nullptr;          // [2][blocks]: proposal-search blocks, full-search blocks
+    PropPicks* prop = nullptr;
+    uint64_t* masks = nullptr;
+    size_t cap_logits = 0, cap_lists = 0, cap_prop = 0, cap_masks = 0;
+};
+
+// A footprint's proposal network on the device.
+struct NetDev {
+    int bx = 0, by = 0;
+    mlp::Net net{};
+    void* mem = nullptr;  // one allocation holding weights and biases
+};
+
+struct Pruning {
+    bool enable = false;
+    int kmax = 4, kbm = 16, topn = 4;
+    float coverage = 0.95f, threshold = 0.5f;
 };
 
 // A batch shape: texture sizes and footprints in call order.
@@ -38,6 +58,7 @@ struct BatchGraph {
     std::vector<const void*> bufs;  // device buffers baked into the graph
     cudaGraphExec_t exec = nullptr;
     uint32_t launches = 0;
+    uint32_t routes = 0;  // route-counter entries the captured sequence writes
 };
 
 struct BatchTuning {
@@ -63,9 +84,9 @@ struct astcb200_ctx {
     uint32_t* d_sym = nullptr;
     size_t sym_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> stage_ev;  // 5 per chunk: before the first kernel and after each
+    std::vector<cudaEvent_t> stage_ev;  // kStageIntervals + 1 per chunk
+    std::vector<int8_t> stage_kind;     // kStageIntervals per chunk
     int stage_chunks = 0;               // chunks recorded by the last encode
-    uint32_t stage_n[4] = {0, 0, 0, 0};
     // batches
     std::vector<cudaStream_t> branch;                // extra streams of batched launches
     std::vector<cudaEvent_t> fork_ev, join_ev;
@@ -78,6 +99,13 @@ struct astcb200_ctx {
     size_t bout_cap = 0;
     std::map<astcb200::BatchShape, astcb200::BatchGraph> graphs;
     std::map<astcb200::BatchShape, astcb200::BatchTuning> tuned;
+    // learned proposal search
+    std::vector<astcb200::NetDev*> nets;
+    astcb200::Pruning pruning;
+    int* d_counts = nullptr;     // [chunks][2] routed blocks of the last encode
+    size_t counts_cap = 0;
+    uint32_t counts_used = 0;    // chunk entries written by the last encode
+    int* d_mlp_error = nullptr;  // set by an inference CTA that gave up waiting
     std::string err;
 };
 
@@ -87,6 +115,19 @@ int cuda_fail(astcb200_ctx* c, cudaError_t e, const char* what);
 int wait_stream(astcb200_ctx* ctx, cudaStream_t s);
 int get_tables(astcb200_ctx* ctx, int bx, int by, const FootTables** out);
 int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots);
+// Scratch for `blocks` blocks per chunk of footprint ft (proposal buffers when it is pruned).
+int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const FootTables* ft);
+const NetDev* net_for(const astcb200_ctx* ctx, const FootTables* ft);  // null: full search
+// Room for `chunks` route counters; resets the per-call counter index.
+int begin_routes(astcb200_ctx* ctx, size_t chunks);
+// Stage timing: per chunk, an event before the first launch and after each launch
+// (at most kStageIntervals launches), and the stage (0 partition search or network, 1
+// front, 2 refine, 3 select-pack) of each launch, -1 past the last.
+constexpr int kStageIntervals = 9;
+// Queues the search of one chunk (base: addressing, block_first, nblocks) on s; ev and
+// kinds, when not null, receive kStageIntervals + 1 events and the launches' stages.
+int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* ft, Scratch& sc, cudaStream_t s,
+                  cudaEvent_t* ev, int8_t* kinds, uint32_t* launches);
 void free_scratch(Scratch& sc);
 void release_batches(astcb200_ctx* ctx);
 

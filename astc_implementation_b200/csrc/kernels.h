@@ -79,6 +79,8 @@ struct KernelArgs {
     const int* block_count;
     const PropPicks* prop;    // per list position: proposed partitionings (replaces the partition search)
     const uint64_t* bm_mask;  // per list position and P = 1..4: block modes the front evaluates
+    int* reroute_list;        // blocks that end without any candidate are appended here (and
+    int* reroute_count;       // left unwritten) instead of being encoded; null: never
 };
 
 // Global index of the chunk's lb-th block, or -1 past the end of a block list.
@@ -111,6 +113,13 @@ __device__ __forceinline__ BlockSrc block_src(const KernelArgs& a, int blk) {
     const int local = blk - s.block_base;
     const int bxi = local % s.nbx, byi = local / s.nbx;
     return {reinterpret_cast<const uchar4*>(s.img), s.width, s.height, bxi * a.L.bx, byi * a.L.by, lo};
+}
+
+// Texel t of the block, edge-clamped, as stored.
+__device__ __forceinline__ uchar4 src_rgba8(const BlockSrc& s, int bx, int t) {
+    const int x = min(s.x0 + t % bx, s.width - 1);
+    const int y = min(s.y0 + t / bx, s.height - 1);
+    return s.img[(size_t)y * s.width + x];
 }
 
 // Texel t of the block, edge-clamped, as (v / 255) * 65536 (compression_pipeline.cpp:32-46).

@@ -688,6 +688,10 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
             if (e < best) { best = e; win_slot = s; win_k = k; }
         }
     }
+    if (win_slot < 0 && a.reroute_list) {  // proposal search found nothing: hand the block to the full search
+        a.reroute_list[atomicAdd(a.reroute_count, 1)] = blk;
+        return;
+    }
     uint8_t blockbytes[18];
     uint32_t sym[8 + 4 + 32];  // header words of the SymbolicBlock record
     for (int i = 0; i < 18; i++) blockbytes[i] = 0;

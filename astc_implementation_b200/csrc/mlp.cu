@@ -1,0 +1,451 @@
+// Learned proposal: network inference on the tcgen05 tensor cores and the
+// selection of partitionings, block modes and routes from its logits.
+//
+// k_mlp_logits: one CTA of 4 warps per 128 blocks.  The block texels are
+// staged in shared memory as bf16 in the tensor core's K-major core-matrix
+// layout; each layer is a chain of tcgen05.mma (M=128, K=16 per instruction,
+// A and B from shared memory, FP32 accumulators in tensor memory) issued by
+// one thread.  Weights arrive by bulk copies (cp.async.bulk, completion on an
+// mbarrier) already laid out on the host in the same core-matrix order.  The
+// two hidden layers' epilogues (bias, ReLU, bf16) read the accumulators with
+// tcgen05.ld and write the next layer's A operand in place; layer 3 runs in
+// 128-column chunks with double-buffered weights and accumulators, so the
+// epilogue of chunk j (bias, FP32 logits to global memory) overlaps the MMAs
+// of chunk j+1 and the copy of chunk j+2.  Every wait on an mbarrier is
+// bounded; a CTA that gives up sets *error_flag, waits (bounded) for its own
+// copies and MMAs in flight, frees its tensor memory and returns.
+//
+// k_select: one warp per block turns the logits into the proposal search's
+// inputs: a softmax over the partition classes, the best partitionings (in
+// probability order, until the proposed mass reaches the coverage), the best
+// block modes of each partition count as bit masks, and the route: blocks
+// whose best-kmax mass is below the threshold take the full search.
+#include <cuda_bf16.h>
+
+#include "mlp.h"
+
+namespace astcb200 {
+namespace mlp {
+namespace {
+
+constexpr uint32_t kOffA = 0;                 // 64 KB: X, then H1, then H2 (128 rows x up to 256 bf16)
+constexpr uint32_t kOffW = 65536;             // 128 KB: W1 | W2 | two W3 chunks of 64 KB
+constexpr uint32_t kOffBar = 65536 + 131072;  // mbarriers and flags
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kWaitLimit = 1u << 24;     // polls of an mbarrier before a CTA gives up
+constexpr uint32_t kCopyPiece = 32768;        // bytes per bulk copy instruction
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// One thread: expect `bytes` on bar and copy them in pieces.
+__device__ void load_weights(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    mbar_expect_tx(bar, bytes);
+    for (uint32_t o = 0; o < bytes; o += kCopyPiece)
+        bulk_load(static_cast<uint8_t*>(dst) + o, static_cast<const uint8_t*>(src) + o, min(kCopyPiece, bytes - o), bar);
+}
+
+__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: no swizzle, K-major core matrices; lbo =
+// bytes between K-adjacent core matrices, sbo = bytes between M/N-adjacent
+// ones; descriptor version 1 (bits 46-47), base offset 0.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: bf16 A and B (K-major), FP32 accumulator.
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+static_assert(instr_desc(128, 256) == 0x08400490u, "instruction descriptor layout");
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 32 consecutive FP32 columns of the calling thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t bf16_bits(float f) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f));
+}
+__device__ __forceinline__ uint4 pack8(const float* v) {
+    return make_uint4(bf16_bits(v[0]) | (bf16_bits(v[1]) << 16), bf16_bits(v[2]) | (bf16_bits(v[3]) << 16),
+                      bf16_bits(v[4]) | (bf16_bits(v[5]) << 16), bf16_bits(v[6]) | (bf16_bits(v[7]) << 16));
+}
+
+// Hidden-layer epilogue: accumulator columns [col0, col0+256) of this thread's
+// row -> bias, ReLU, bf16 -> the A operand (128 rows x 256) for the next layer.
+__device__ void hidden_epilogue(uint32_t tmem_row, uint32_t col0, const float* __restrict__ bias, uint8_t* sA, int m) {
+    for (int c = 0; c < 256; c += 32) {
+        float v[32];
+        tmem_load32(tmem_row + col0 + c, v);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            float h[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) h[i] = fmaxf(v[q * 8 + i] + __ldg(bias + c + q * 8 + i), 0.0f);
+            *reinterpret_cast<uint4*>(sA + core_index(m, c + q * 8, kTileRows) * 2) = pack8(h);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTileRows, 1)
+    k_mlp_logits(const __grid_constant__ KernelArgs a, const __grid_constant__ Net net, float* __restrict__ logits, int* error_flag) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = sm + kOffA;
+    uint8_t* sW = sm + kOffW;
+    uint64_t* bw = reinterpret_cast<uint64_t*>(sm + kOffBar);       // [2] weight buffers
+    uint64_t* bm = bw + 2;                                           // [3] MMA completion: layers 1-2, layer-3 buffers
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bw + 5);
+    int* abort_flag = reinterpret_cast<int*>(bw + 6);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int m = tid;  // this thread's row (block) in the tile and tensor-memory lane
+    const int lb = blockIdx.x * kTileRows + m;
+    const Shape& S = net.s;
+    const int nchunks = S.nout / kChunkN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 5; i++) mbar_init(&bw[i], 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+
+    // thread 0's bookkeeping of weight copies and MMA commits in flight
+    uint32_t w_issued[2] = {0, 0}, w_done[2] = {0, 0};
+    uint32_t m_issued[3] = {0, 0, 0}, m_done[3] = {0, 0, 0};  // only the waits of all threads advance m_done
+    bool ok = true, failed = false;  // failed: the same in every thread (set only at uniform exits)
+
+    if (tid == 0) { load_weights(sW, net.w1, 256u * S.k0p * 2, &bw[0]); w_issued[0]++; }
+
+    // stage the block's texels (RGBA8 / 255 -> bf16), zero rows past the chunk
+    {
+        const int blk = lb < a.nblocks ? chunk_block(a, lb) : -1;
+        const int T = a.L.T;
+        BlockSrc src{};
+        if (blk >= 0) src = block_src(a, blk);
+        for (int j = 0; j < S.k0p / 8; j++) {
+            float v[8];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int t = 2 * j + h;
+                uchar4 p = make_uchar4(0, 0, 0, 0);
+                if (blk >= 0 && t < T) p = src_rgba8(src, a.L.bx, t);
+                v[4 * h + 0] = (float)p.x / 255.0f; v[4 * h + 1] = (float)p.y / 255.0f;
+                v[4 * h + 2] = (float)p.z / 255.0f; v[4 * h + 3] = (float)p.w / 255.0f;
+            }
+            *reinterpret_cast<uint4*>(sA + core_index(m, 8 * j, kTileRows) * 2) = pack8(v);
+        }
+    }
+    async_proxy_fence();
+    tc_before();
+    __syncthreads();
+
+    const uint32_t a_base = smem_u32(sA), w_base = smem_u32(sW);
+    constexpr uint32_t kLboA = (kTileRows / 8) * 128, kLboW256 = (256 / 8) * 128, kLboW128 = (kChunkN / 8) * 128;
+
+    // ---- layer 1: X (128 x k0p) . W1^T -> tensor memory columns [0, 256)
+    if (tid == 0) {
+        tc_after();
+        if (!mbar_wait(&bw[0], (w_done[0]++) & 1)) *abort_flag = 1;
+        else {
+            for (int kk = 0; kk < S.k0p / 16; kk++)
+                mma_bf16(tmem, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128), smem_desc(w_base + kk * 2 * kLboW256, kLboW256, 128),
+                         instr_desc(128, 256), kk > 0);
+            mma_commit(&bm[0]);
+            m_issued[0]++;
+        }
+    }
+    __syncthreads();
+    if (*abort_flag) { failed = true; goto cleanup; }
+    ok = mbar_wait(&bm[0], m_done[0] & 1);
+    m_done[0]++;
+    if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
+    tc_after();
+    if (tid == 0) { load_weights(sW, net.w2, 256u * 256u * 2, &bw[0]); w_issued[0]++; }
+    hidden_epilogue(tmem_row, 0, net.b1, sA, m);
+    async_proxy_fence();
+    tc_before();
+    __syncthreads();
+
+    // ---- layer 2: H1 (128 x 256) . W2^T -> columns [256, 512)
+    if (tid == 0) {
+        tc_after();
+        if (!mbar_wait(&bw[0], (w_done[0]++) & 1)) *abort_flag = 1;
+        else {
+            for (int kk = 0; kk < 16; kk++)
+                mma_bf16(tmem + 256, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
+                         smem_desc(w_base + kk * 2 * kLboW256, kLboW256, 128), instr_desc(128, 256), kk > 0);
+            mma_commit(&bm[0]);
+            m_issued[0]++;
+        }
+    }
+    __syncthreads();
+    if (*abort_flag) { failed = true; goto cleanup; }
+    ok = mbar_wait(&bm[0], m_done[0] & 1);
+    m_done[0]++;
+    if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
+    tc_after();
+    if (tid == 0) {
+        for (int j = 0; j < 2 && j < nchunks; j++) {
+            load_weights(sW + j * 65536, net.w3 + (size_t)j * kChunkN * 256, kChunkN * 256 * 2, &bw[j]);
+            w_issued[j]++;
+        }
+    }
+    hidden_epilogue(tmem_row, 256, net.b2, sA, m);
+    async_proxy_fence();
+    tc_before();
+    __syncthreads();
+
+    // ---- layer 3: H2 (128 x 256) . W3^T in chunks of 128 columns, accumulators
+    // alternating between tensor-memory columns [0, 128) and [128, 256)
+    for (int j = 0; j < nchunks; j++) {
+        const int b = j & 1;
+        if (tid == 0) {
+            tc_after();
+            for (int jj = (j == 0 ? 0 : j + 1); jj <= j + 1 && jj < nchunks; jj++) {
+                const int bb = jj & 1;
+                if (!mbar_wait(&bw[bb], (w_done[bb]++) & 1)) { *abort_flag = 1; break; }
+                for (int kk = 0; kk < 16; kk++)
+                    mma_bf16(tmem + bb * kChunkN, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
+                             smem_desc(w_base + bb * 65536 + kk * 2 * kLboW128, kLboW128, 128), instr_desc(128, kChunkN), kk > 0);
+                mma_commit(&bm[1 + bb]);
+                m_issued[1 + bb]++;
+            }
+        }
+        __syncthreads();
+        if (*abort_flag) { failed = true; goto cleanup; }
+        ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1);
+        m_done[1 + b]++;
+        if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
+        tc_after();
+        if (tid == 0 && j + 2 < nchunks) {
+            load_weights(sW + b * 65536, net.w3 + (size_t)(j + 2) * kChunkN * 256, kChunkN * 256 * 2, &bw[b]);
+            w_issued[b]++;
+        }
+        const bool store = lb < a.nblocks;
+        float* out = logits + (size_t)lb * S.nout + j * kChunkN;
+        const float* bias = net.b3 + j * kChunkN;
+        for (int c = 0; c < kChunkN; c += 32) {
+            float v[32];
+            tmem_load32(tmem_row + b * kChunkN + c, v);
+            if (store) {
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    reinterpret_cast<float4*>(out + c)[q] = make_float4(v[4 * q] + __ldg(bias + c + 4 * q), v[4 * q + 1] + __ldg(bias + c + 4 * q + 1),
+                                                                        v[4 * q + 2] + __ldg(bias + c + 4 * q + 2), v[4 * q + 3] + __ldg(bias + c + 4 * q + 3));
+            }
+        }
+        tc_before();
+        __syncthreads();
+    }
+
+cleanup:
+    __syncthreads();
+    if (failed) {
+        // give up: record it, then let our own copies and MMAs drain (bounded) before the
+        // shared and tensor memory are released
+        if (tid == 0) {
+            atomicExch(error_flag, 1);
+            for (int b = 0; b < 2; b++)
+                while (w_done[b] < w_issued[b]) { mbar_wait(&bw[b], w_done[b] & 1); w_done[b]++; }
+            for (int b = 0; b < 3; b++)
+                for (uint32_t i = m_done[b]; i < m_issued[b]; i++) mbar_wait(&bm[b], i & 1);
+        }
+        __syncthreads();
+    }
+    tc_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// ------------------------------------------------------------ selection
+
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+// Warp argmax of (value, index) pairs: larger value, then smaller index.
+__device__ __forceinline__ void warp_argmax(float& v, int& i) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, i, o);
+        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+    }
+}
+// (value, index) strictly after (pv, pi) in the order value desc, index asc.
+__device__ __forceinline__ bool after(float v, int i, float pv, int pi) { return v < pv || (v == pv && i > pi); }
+
+__device__ __forceinline__ bool part_valid(int c, const Select& sel) {
+    return c == kClassP1 || (c < kPartClasses && (c & 1023) < sel.sel[c >> 10]);
+}
+
+__global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelArgs a, const __grid_constant__ Shape S,
+                                                 const float* __restrict__ logits, const __grid_constant__ Select sel,
+                                                 const __grid_constant__ Routes r) {
+    const int lane = threadIdx.x & 31;
+    const int lb = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (lb >= a.nblocks) return;
+    const int blk = chunk_block(a, lb);
+    if (blk < 0) return;
+    const float* z = logits + (size_t)lb * S.nout;
+    // softmax over the partition classes
+    float mx = -3.0e38f;
+    for (int c = lane; c <= kClassP1; c += 32)
+        if (part_valid(c, sel)) mx = fmaxf(mx, z[c]);
+    mx = warp_max(mx);
+    float se = 0.0f;
+    for (int c = lane; c <= kClassP1; c += 32)
+        if (part_valid(c, sel)) se += __expf(z[c] - mx);
+    se = warp_sum(se);
+    const float p1 = __expf(z[kClassP1] - mx) / se;
+    // the kmax best partitionings
+    uint16_t picks[kMaxProposals];
+    float mass[kMaxProposals];
+    float pv = 3.0e38f;
+    int pi = -1, n = 0;
+    float acc = p1;
+    for (int k = 0; k < sel.kmax; k++) {
+        float bv = -3.0e38f;
+        int bi = 0x7FFFFFFF;
+        for (int c = lane; c < kPartClasses; c += 32) {
+            if ((c & 1023) >= sel.sel[c >> 10]) continue;
+            const float v = z[c];
+            if (after(v, c, pv, pi) && (v > bv || (v == bv && c < bi))) { bv = v; bi = c; }
+        }
+        warp_argmax(bv, bi);
+        if (bi == 0x7FFFFFFF) break;
+        picks[n] = (uint16_t)(((bi >> 10) << 10) | (bi & 1023));
+        acc += __expf(bv - mx) / se;
+        mass[n] = acc;
+        n++;
+        pv = bv; pi = bi;
+    }
+    const bool confident = acc >= sel.threshold;
+    if (r.confidence && lane == 0) r.confidence[lb] = acc;
+    int pos = 0;
+    if (lane == 0) pos = atomicAdd(&r.counts[confident ? 0 : 1], 1);
+    pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+    if (!confident) {
+        if (lane == 0) r.full[pos] = blk;
+        return;
+    }
+    // propose the shortest best-first prefix whose mass reaches the coverage
+    int used = n;
+    for (int k = 0; k < n; k++)
+        if (mass[k] >= sel.coverage) { used = k + 1; break; }
+    if (p1 >= sel.coverage) used = 0;
+    if (lane == 0) {
+        r.pruned[pos] = blk;
+        PropPicks& pp = r.prop[pos];
+        pp.n = (uint16_t)used;
+        for (int k = 0; k < kMaxProposals; k++) pp.v[k] = k < used ? picks[k] : 0;
+    }
+    // block-mode masks: the kbm best modes of each partition count's head
+    uint64_t* mk = r.masks + (size_t)pos * 4 * kMaskWords;
+    for (int p = 0; p < 4; p++) {
+        const float* h = z + kHeadBase + p * S.nbm_pad;
+        uint32_t bits[kMaskWords * 2] = {};
+        float qv = 3.0e38f;
+        int qi = -1;
+        for (int k = 0; k < sel.kbm && k < S.nbm; k++) {
+            float bv = -3.0e38f;
+            int bi = 0x7FFFFFFF;
+            for (int c = lane; c < S.nbm; c += 32) {
+                const float v = h[c];
+                if (after(v, c, qv, qi) && (v > bv || (v == bv && c < bi))) { bv = v; bi = c; }
+            }
+            warp_argmax(bv, bi);
+            if (bi == 0x7FFFFFFF) break;
+            bits[bi >> 5] |= 1u << (bi & 31);
+            qv = bv; qi = bi;
+        }
+        if (lane < kMaskWords) mk[p * kMaskWords + lane] = (uint64_t)bits[2 * lane] | ((uint64_t)bits[2 * lane + 1] << 32);
+    }
+}
+
+}  // namespace
+
+cudaError_t configure_mlp() {
+    return cudaFuncSetAttribute(k_mlp_logits, cudaFuncAttributeMaxDynamicSharedMemorySize, kMlpSmemBytes);
+}
+
+cudaError_t launch_mlp_logits(const KernelArgs& a, const Net& net, float* logits, int* error_flag, cudaStream_t s) {
+    const int grid = (a.nblocks + kTileRows - 1) / kTileRows;
+    k_mlp_logits<<<grid, kTileRows, kMlpSmemBytes, s>>>(a, net, logits, error_flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select(const KernelArgs& a, const Net& net, const float* logits, const Select& sel, const Routes& r,
+                          cudaStream_t s) {
+    k_select<<<(a.nblocks + 3) / 4, 128, 0, s>>>(a, net.s, logits, sel, r);
+    return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace astcb200

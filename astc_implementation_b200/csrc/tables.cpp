@@ -635,6 +635,15 @@ int astcb200_tables_partitions(int bx, int by, uint32_t* pinfo, uint64_t* cov2, 
     std::memcpy(pidx, h->packed_index, sizeof(h->packed_index));
     return 0;
 }
+// Block mode (11-bit ASTC mode) of every trial block mode, in trial order.
+int astcb200_tables_trial_modes(int bx, int by, uint32_t* n_bm, uint16_t* mode_index) {
+    const HostTables* h = astcb200::host_tables(bx, by);
+    if (!h || !n_bm) return -1;
+    *n_bm = (uint32_t)h->valid_bms.size();
+    if (mode_index)
+        for (size_t i = 0; i < h->valid_bms.size(); i++) mode_index[i] = (uint16_t)h->bms[h->valid_bms[i].first].mode;
+    return 0;
+}
 int astcb200_tables_angular(float* s, float* c) {
     const HostTables* h = astcb200::host_tables(4, 4);
     std::memcpy(s, h->sin_t.data(), 16384 * 4);

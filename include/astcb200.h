@@ -136,6 +136,73 @@ int astcb200_autotune_batch(astcb200_ctx* ctx, const astcb200_texture* textures,
  * no wait.  (No reference counterpart: the reference encodes the image it is given.) */
 int astcb200_downsample_device(const uint8_t* d_src, uint32_t width, uint32_t height, uint8_t* d_dst, void* cuda_stream);
 
+/* ---- Learned proposal search (no reference counterpart) ----
+ * A small network (inputs: a block's texels / 255 in bf16; two hidden layers of 256 ReLU
+ * units; outputs: one logit per partitioning of P = 2..4, one for the single-partition
+ * block, and one per block mode for each partition count) ranks the candidates; only the
+ * best partitionings and, per partition count, the best block modes enter the search,
+ * with fewer refinement candidates.  Blocks whose best partitionings carry too little
+ * probability take the full search.  The final-error comparison still picks every block's
+ * encoding.  Inference runs on the tensor cores (tcgen05, bf16 operands, FP32 accumulation). */
+
+/* Output layout of a footprint's network: inputs (4 * texels), padded inputs, outputs
+ * (a multiple of 128), block-mode classes per head, first block-mode logit and head
+ * stride, and the number of selected partitionings of P = 2, 3, 4 (sel3[0..2]). */
+int astcb200_proposal_layout(uint8_t block_x, uint8_t block_y, uint32_t* inputs, uint32_t* inputs_padded,
+                             uint32_t* outputs, uint32_t* block_modes, uint32_t* head_base, uint32_t* head_stride,
+                             uint32_t* sel3);
+
+/* FP32 weights of one footprint's network (row-major, PyTorch Linear convention:
+ * w1 [256 x inputs], w2 [256 x 256], w3 [outputs x 256]); converted to bf16 on upload. */
+typedef struct astcb200_proposal_net {
+    uint32_t struct_size;
+    uint8_t block_x, block_y, reserved[2];
+    uint32_t inputs, hidden, outputs; /* must match astcb200_proposal_layout and hidden = 256 */
+    const float* w1;
+    const float* b1;
+    const float* w2;
+    const float* b2;
+    const float* w3;
+    const float* b3;
+} astcb200_proposal_net;
+int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* net);
+
+typedef struct astcb200_pruning {
+    uint32_t struct_size;
+    uint32_t enable;            /* 0: full search everywhere */
+    uint32_t max_partitionings; /* proposed partitionings per block, at most 16 */
+    uint32_t block_modes;       /* block modes evaluated per partition count, at most 64 */
+    uint32_t refine_candidates; /* refinement candidates per partitioned block, at most 8 */
+    float coverage;             /* stop proposing once P=1 plus the proposed probability reaches this */
+    float threshold;            /* full search when P=1 plus the best max_partitionings carry less */
+} astcb200_pruning;
+/* Applies to later encodes of footprints that have a network (the others use the full search). */
+int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);
+/* Blocks that took the proposal search and the full search in the last encode call. */
+int astcb200_pruning_stats(astcb200_ctx* ctx, uint64_t* proposal_blocks, uint64_t* full_blocks);
+/* Test hook: the network's logits (blocks x outputs, FP32) for the image set by
+ * astcb200_set_image, from host RGBA8. */
+int astcb200_proposal_logits(astcb200_ctx* ctx, const uint8_t* rgba8, float* logits, size_t logits_len);
+
+/* Training primitives of the proposal network (device pointers, FP32, queued on
+ * cuda_stream, deterministic).  C[i][j] = sum_l A[i*sa_i + l*sa_l] * B[l*sb_l + j*sb_j]
+ * (+ C when accumulate) (+ bias[j]) (ReLU when relu); C is row-major M x N. */
+int astcb200_train_gemm(const float* A, const float* B, float* C, int M, int N, int K, int64_t sa_i, int64_t sa_l,
+                        int64_t sb_l, int64_t sb_j, const float* bias, int relu, int accumulate, void* cuda_stream);
+/* Softmax cross-entropy of the partition head and of the block-mode head of the label's
+ * partition count; dZ (batch x outputs) receives the gradient divided by batch and
+ * loss_rows (batch x 2) the two losses of each row.  sel3 is host memory. */
+int astcb200_train_xent(const float* Z, uint32_t outputs, const int32_t* part_label, const int32_t* bm_label,
+                        uint32_t batch, uint32_t block_modes, uint32_t head_stride, const uint32_t* sel3, float* dZ,
+                        float* loss_rows, void* cuda_stream);
+/* dH[i] = 0 where H[i] <= 0. */
+int astcb200_train_relu_backward(float* dH, const float* H, size_t n, void* cuda_stream);
+/* db[j] = sum over rows of dY[r][j]. */
+int astcb200_train_colsum(const float* dY, float* db, uint32_t rows, uint32_t cols, void* cuda_stream);
+/* One Adam step (bias-corrected with the 1-based step). */
+int astcb200_train_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, float beta1, float beta2,
+                        float eps, uint32_t step, void* cuda_stream);
+
 /* Debug / parity hook: returns the chosen SymbolicBlock of every block in the reference
  * layout (astc.h:639-655, 108 u32 per block) instead of physical blocks. */
 int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* symbolic, size_t symbolic_words);

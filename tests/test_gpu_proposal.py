@@ -1,0 +1,182 @@
+"""Learned proposal on the GPU: tensor-core inference against the CPU checker,
+training gradients against the CPU checker, and the proposal search's routing and
+results."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import _libs
+import astc_implementation_b200 as ab
+from astc_implementation_b200 import proposal, synth
+
+sys.path.insert(0, os.path.join(_libs.REPO, "oracle"))
+import mlp_oracle as mo  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def random_net(lay, seed):
+    w = proposal.init_weights(lay, seed=seed)
+    rng = np.random.default_rng(seed + 7)
+    w["b1"] = rng.normal(0, 0.05, 256).astype(np.float32)
+    w["b2"] = rng.normal(0, 0.05, 256).astype(np.float32)
+    w["b3"] = rng.normal(0, 0.5, lay.outputs).astype(np.float32)
+    w["footprint"] = (lay.bx, lay.by)
+    return w
+
+
+@pytest.mark.parametrize("bx,by,w,h", [(4, 4, 64, 48), (6, 6, 100, 70), (4, 4, 9, 5)])
+def test_tensor_core_logits_match_oracle(bx, by, w, h):
+    lay = proposal.Layout(bx, by)
+    net = random_net(lay, seed=bx * 10 + w)
+    img = synth.make_texture(w, h, 40 + bx)
+    enc = ab.ASTCEncoder(device=0)
+    enc.set_proposal_net(net)
+    enc.secondaryInit(w, h, bx, by)
+    z = enc.proposal_logits(img, lay.outputs)
+    enc.close()
+    ref = mo.infer(mo.inputs(mo.block_rgba8(img, bx, by), lay.inputs_padded), net)
+    scale = np.abs(ref).max() + 1.0
+    err = np.abs(z - ref)
+    # bf16 operands, FP32 accumulation: the tensor core's summation order and the
+    # rounding of the hidden layers to bf16 give differences of a few bf16 ulps
+    assert err.max() <= 2e-2 * scale, err.max()
+    assert err.mean() <= 1e-3 * scale, err.mean()
+    top = lambda a: np.argsort(-a[:, : mo.P1], axis=1)[:, :4]
+    assert (top(z) == top(ref)).mean() > 0.95
+
+
+def test_training_gradients_match_oracle():
+    import torch
+    lay = proposal.Layout(4, 4)
+    w = random_net(lay, seed=3)
+    img = synth.make_texture(64, 64, 77)
+    X = mo.inputs(mo.block_rgba8(img, 4, 4), lay.inputs_padded)[:64]
+    rng = np.random.default_rng(5)
+    part = np.concatenate([rng.integers(0, lay.sel3[0], 20), 1024 + rng.integers(0, lay.sel3[1], 20),
+                           2048 + rng.integers(0, lay.sel3[2], 20), np.full(4, mo.P1)]).astype(np.int32)
+    bm = rng.integers(0, lay.nbm, 64).astype(np.int32)
+    tr = proposal.Trainer(lay, {k: w[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3")}, batch=64)
+    with torch.cuda.stream(tr.stream):
+        xd = torch.from_numpy(X).cuda()
+        tr.forward(xd, 64)
+        loss = tr.backward(xd, torch.from_numpy(part).cuda(), torch.from_numpy(bm).cuda(), 64)
+        tr.stream.synchronize()
+    lp, lb, g, _ = mo.loss_and_grads(X, {k: w[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3")}, part, bm, lay.nbm,
+                                     lay.head_stride, lay.sel3)
+    l = loss.cpu().numpy().astype(np.float64)
+    assert abs(l[:, 0].mean() - lp) < 1e-4 * (1 + abs(lp)) and abs(l[:, 1].mean() - lb) < 1e-4 * (1 + abs(lb))
+    for k in ("w1", "b1", "w2", "b2", "w3", "b3"):
+        got = tr.g[k].cpu().numpy().astype(np.float64)
+        if k == "w1":
+            got = got[:, : lay.inputs]
+        ref = g[k]
+        rel = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
+        assert rel < 1e-4, (k, rel)
+
+
+def test_adam_step_matches_formula():
+    import torch
+    lay = proposal.Layout(4, 4)
+    w = random_net(lay, seed=9)
+    tr = proposal.Trainer(lay, {k: w[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3")}, batch=16, lr=1e-2)
+    rng = np.random.default_rng(2)
+    gb2 = rng.normal(size=256).astype(np.float32)
+    with torch.cuda.stream(tr.stream):
+        for k in tr.g:
+            tr.g[k].zero_()
+        tr.g["b2"].copy_(torch.from_numpy(gb2))
+        b2 = tr.p["b2"].cpu().numpy().astype(np.float64)
+        tr.adam()
+        tr.stream.synchronize()
+    m = 0.1 * gb2
+    v = 0.001 * gb2.astype(np.float64) ** 2
+    ref = b2 - 1e-2 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
+    assert np.allclose(tr.p["b2"].cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+
+
+def full_and_pruned(img, bx, by, net, **prune):
+    h, w = img.shape[:2]
+    enc = ab.ASTCEncoder(device=0)
+    enc.secondaryInit(w, h, bx, by)
+    full_sym = enc.encode_symbolic(img)
+    full = enc.encode(img)
+    enc.set_proposal_net(net)
+    enc.set_pruning(True, **prune)
+    sym = enc.encode_symbolic(img)
+    blocks = enc.encode(img)
+    stats = enc.pruning_stats()
+    enc.close()
+    return full, full_sym, blocks, sym, stats
+
+
+def test_everything_routed_to_full_search_is_bit_exact():
+    lay = proposal.Layout(4, 4)
+    img = synth.make_texture(80, 52, 12)
+    full, full_sym, blocks, sym, stats = full_and_pruned(img, 4, 4, random_net(lay, 1), threshold=2.0)
+    assert stats == (0, 20 * 13)
+    assert np.array_equal(blocks, full) and np.array_equal(sym, full_sym)
+
+
+@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
+def test_proposal_search_obeys_the_selection(bx, by):
+    """Every block taking the proposal search ends on P=1 or a proposed partitioning,
+    with a block mode from that partition count's mask; the others equal the full search."""
+    lay = proposal.Layout(bx, by)
+    net = random_net(lay, 2)
+    img = synth.make_texture(90, 61, 13)
+    kmax, kbm, cov, thr = 6, 8, 0.999, 1e-4
+    full, full_sym, blocks, sym, stats = full_and_pruned(img, bx, by, net, max_partitionings=kmax, block_modes=kbm,
+                                                         refine_candidates=4, coverage=cov, threshold=thr)
+    n = sym.shape[0]
+    assert sum(stats) == n
+    enc = ab.ASTCEncoder(device=0)
+    enc.set_proposal_net(net)
+    enc.secondaryInit(90, 61, bx, by)
+    z = enc.proposal_logits(img, lay.outputs)
+    enc.close()
+    part, bm, _ = proposal.labels_from_symbolic(sym, bx, by)
+    n_checked = 0
+    for i in range(n):
+        conf, picks, modes = mo.select(z[i], lay.sel3, kmax, cov, thr, kbm, lay.nbm, lay.head_stride)
+        if not conf:
+            assert np.array_equal(sym[i], full_sym[i])
+            continue
+        head = 0 if part[i] == mo.P1 else (part[i] >> 10) + 1
+        if part[i] != mo.P1 and part[i] not in picks:
+            continue  # near-tied logits can order differently than the checker's float64 sort
+        assert bm[i] in modes[head] or np.array_equal(sym[i], full_sym[i])
+        n_checked += 1
+    assert n_checked > 0.9 * stats[0]
+    dec = ab.decode(bx, by, 90, 61, blocks)
+    assert ab.psnr(dec, img) > ab.psnr(ab.decode(bx, by, 90, 61, full), img) - 3.0
+
+
+def test_batch_with_proposal_equals_single_images():
+    lay4, lay6 = proposal.Layout(4, 4), proposal.Layout(6, 6)
+    tex = [(synth.make_texture(37, 29, 3), 4, 4), (synth.make_texture(50, 44, 4), 6, 6), (synth.make_texture(20, 20, 5), 4, 4)]
+    enc = ab.ASTCEncoder(device=0)
+    enc.set_proposal_net(random_net(lay4, 4))
+    enc.set_proposal_net(random_net(lay6, 5))
+    enc.set_pruning(True, max_partitionings=4, block_modes=12, refine_candidates=4, coverage=0.9, threshold=0.0005)
+    outs = enc.encode_batch(tex)
+    outs2 = enc.encode_batch(tex)  # graph replay
+    for (img, bx, by), o, o2 in zip(tex, outs, outs2):
+        enc.secondaryInit(img.shape[1], img.shape[0], bx, by)
+        single = enc.encode(img)
+        assert np.array_equal(o, single) and np.array_equal(o2, single)
+    enc.close()
+
+
+def test_training_on_gpu_reduces_loss():
+    lay = proposal.Layout(4, 4)
+    X, part, bm = proposal.make_dataset(4, 4, [300, 301], 256, log=lambda *a: None)
+    tr = proposal.Trainer(lay, proposal.init_weights(lay, seed=0), batch=1024, lr=2e-3)
+    before = tr.accuracy(X[:4096], part[:4096], bm[:4096])
+    losses = []
+    tr.fit(X, part, bm, 3, log=lambda s: losses.append(float(s.split()[4])))
+    after = tr.accuracy(X[:4096], part[:4096], bm[:4096])
+    assert losses[-1] < losses[0]
+    assert after[1] > before[1] and after[2] > before[2]
