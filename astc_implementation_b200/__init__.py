@@ -72,7 +72,7 @@ class ProposalNet(ctypes.Structure):
 class Pruning(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("enable", ctypes.c_uint32), ("max_partitionings", ctypes.c_uint32),
                 ("block_modes", ctypes.c_uint32), ("refine_candidates", ctypes.c_uint32), ("coverage", ctypes.c_float),
-                ("threshold", ctypes.c_float)]
+                ("threshold", ctypes.c_float), ("reroute_error", ctypes.c_float)]
 
 
 def load_library():
@@ -96,6 +96,8 @@ def load_library():
         "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
         "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
         "astcb200_stage_times": (I32, [P, P, P]),
+        "astcb200_stage_times_detail": (I32, [P, P, P]),
+        "astcb200_work_counters": (I32, [P, P]),
         "astcb200_encode_noalloc": (I32, [I32, P, U32, U32, ctypes.c_uint8, ctypes.c_uint8, P, P]),
         "astcb200_fp32_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double)]),
         "astcb200_encode_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Stats)]),
@@ -253,11 +255,11 @@ class ASTCEncoder:
                           arrs["w3"].shape[0], *[arrs[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")])
         _check(load_library().astcb200_set_proposal_net(self._ctx, ctypes.byref(net)), self._ctx)
 
-    def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=4, coverage=0.95,
-                    threshold=0.5):
+    def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98,
+                    threshold=0.5, reroute_error=8.0):
         """Proposal-search settings for later encodes of footprints with a network."""
         cfg = Pruning(ctypes.sizeof(Pruning), 1 if enable else 0, max_partitionings, block_modes, refine_candidates,
-                      coverage, threshold)
+                      coverage, threshold, reroute_error)
         _check(load_library().astcb200_set_pruning(self._ctx, ctypes.byref(cfg)), self._ctx)
 
     def pruning_stats(self):
@@ -279,6 +281,19 @@ class ASTCEncoder:
         n = np.zeros(4, np.uint32)
         _check(load_library().astcb200_stage_times(self._ctx, _ptr(ms), _ptr(n)), self._ctx)
         return ms, n
+
+    def stage_times_detail(self):
+        """Per-launch milliseconds of the last encode by position in the chunk sequence (9 entries)."""
+        ms = np.zeros(9, np.float32)
+        k = np.zeros(9, np.int32)
+        _check(load_library().astcb200_stage_times_detail(self._ctx, _ptr(ms), _ptr(k)), self._ctx)
+        return ms, k
+
+    def work_counters(self):
+        """Work counters of the last encode (needs stage_timing=True); see astcb200_work_counters."""
+        c = np.zeros(16, np.uint64)
+        _check(load_library().astcb200_work_counters(self._ctx, _ptr(c)), self._ctx)
+        return c
 
     def close(self):
         if getattr(self, "_ctx", None):

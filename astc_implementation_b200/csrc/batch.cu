@@ -135,7 +135,7 @@ std::vector<const void*> baked_buffers(const astcb200_ctx* ctx, uint32_t streams
     for (uint32_t i = 0; i < streams; i++) {
         const Scratch& sc = ctx->bscratch[i];
         for (const void* q : {(const void*)sc.picks, (const void*)sc.pbrec, (const void*)sc.snaps, (const void*)sc.logits,
-                              (const void*)sc.lists, (const void*)sc.prop, (const void*)sc.masks})
+                              (const void*)sc.lists, (const void*)sc.prop, (const void*)sc.masks, (const void*)sc.pbl, (const void*)sc.full_err})
             v.push_back(q);
     }
     return v;

@@ -67,7 +67,7 @@ int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots) {
 
 void free_scratch(Scratch& sc) {
     cudaFree(sc.picks); cudaFree(sc.pbrec); cudaFree(sc.snaps);
-    cudaFree(sc.logits); cudaFree(sc.lists); cudaFree(sc.prop); cudaFree(sc.masks);
+    cudaFree(sc.logits); cudaFree(sc.lists); cudaFree(sc.prop); cudaFree(sc.masks); cudaFree(sc.pbl); cudaFree(sc.full_err);
     sc = Scratch();
 }
 
@@ -88,6 +88,9 @@ int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t
     if ((rc = begin_routes(ctx, nchunks))) return rc;
     constexpr int E = kStageIntervals + 1;
     if (timing) {
+        if (!ctx->d_work) CK(cudaMalloc((void**)&ctx->d_work, kWorkCounters * sizeof(unsigned long long)), "cudaMalloc work counters");
+        CK(cudaMemsetAsync(ctx->d_work, 0, kWorkCounters * sizeof(unsigned long long), s), "reset work counters");
+        a.work = ctx->d_work;
         while ((int)ctx->stage_ev.size() < E * nchunks) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e), "cudaEventCreate");
@@ -158,7 +161,7 @@ int astcb200_destroy(astcb200_ctx* ctx) {
     free_scratch(ctx->scratch);
     for (FootTables* f : ctx->feet) { cudaFree(f->d); delete f; }
     for (NetDev* nd : ctx->nets) { cudaFree(nd->mem); delete nd; }
-    cudaFree(ctx->d_counts); cudaFree(ctx->d_mlp_error);
+    cudaFree(ctx->d_counts); cudaFree(ctx->d_mlp_error); cudaFree(ctx->d_work);
     cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -259,6 +262,34 @@ int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* n4) {
             ms4[k] += ms;
             if (n4) n4[k]++;
         }
+    return ASTCB200_OK;
+}
+
+int astcb200_stage_times_detail(astcb200_ctx* ctx, float* ms9, int32_t* stage9) {
+    if (!ctx || !ms9) return ASTCB200_BAD_ARG;
+    for (int i = 0; i < kStageIntervals; i++) { ms9[i] = 0.0f; if (stage9) stage9[i] = -1; }
+    constexpr int E = kStageIntervals + 1;
+    for (int c = 0; c < ctx->stage_chunks; c++)
+        for (int i = 0; i < kStageIntervals; i++) {
+            const int k = ctx->stage_kind[(size_t)kStageIntervals * c + i];
+            if (k < 0) break;
+            cudaEvent_t e1 = ctx->stage_ev[(size_t)E * c + i + 1];
+            CK(cudaEventSynchronize(e1), "stage event");
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ctx->stage_ev[(size_t)E * c + i], e1), "cudaEventElapsedTime");
+            ms9[i] += ms;
+            if (stage9) stage9[i] = k;
+        }
+    return ASTCB200_OK;
+}
+
+int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16) {
+    if (!ctx || !counters16) return ASTCB200_BAD_ARG;
+    for (int i = 0; i < kWorkCounters; i++) counters16[i] = 0;
+    if (!ctx->d_work) return ASTCB200_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    CK(cudaMemcpy(counters16, ctx->d_work, kWorkCounters * sizeof(uint64_t), cudaMemcpyDeviceToHost), "read work counters");
     return ASTCB200_OK;
 }
 

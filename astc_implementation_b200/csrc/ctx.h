@@ -31,9 +31,11 @@ struct Scratch {
     // proposal search: logits and the routes of one chunk
     float* logits = nullptr;
     int* lists = nullptr;          // [2][blocks]: proposal-search blocks, full-search blocks
+    float* full_err = nullptr;     // [blocks]: error already written for a full-search block
     PropPicks* prop = nullptr;
     uint64_t* masks = nullptr;
-    size_t cap_logits = 0, cap_lists = 0, cap_prop = 0, cap_masks = 0;
+    uint32_t* pbl = nullptr;       // [4][blocks * kMaxProposals] partitioned-block work lists
+    size_t cap_logits = 0, cap_lists = 0, cap_prop = 0, cap_masks = 0, cap_pbl = 0, cap_ferr = 0;
 };
 
 // A footprint's proposal network on the device.
@@ -45,8 +47,10 @@ struct NetDev {
 
 struct Pruning {
     bool enable = false;
-    int kmax = 4, kbm = 16, topn = 4;
-    float coverage = 0.95f, threshold = 0.5f;
+    int kmax = 4, kbm = 16, topn = 2;
+    float coverage = 0.98f, threshold = 0.5f;
+    float reroute_error = 8.0f;  // per-texel weighted squared error (8-bit units) above which
+                                 // a proposal-search block also takes the full search; 0: off
 };
 
 // A batch shape: texture sizes and footprints in call order.
@@ -102,10 +106,11 @@ struct astcb200_ctx {
     // learned proposal search
     std::vector<astcb200::NetDev*> nets;
     astcb200::Pruning pruning;
-    int* d_counts = nullptr;     // [chunks][2] routed blocks of the last encode
+    int* d_counts = nullptr;     // [chunks][mlp::kRouteCounters] routed blocks of the last encode
     size_t counts_cap = 0;
     uint32_t counts_used = 0;    // chunk entries written by the last encode
     int* d_mlp_error = nullptr;  // set by an inference CTA that gave up waiting
+    unsigned long long* d_work = nullptr;  // work counters of the last timed encode (kWorkCounters)
     std::string err;
 };
 

@@ -81,7 +81,27 @@ struct KernelArgs {
     const uint64_t* bm_mask;  // per list position and P = 1..4: block modes the front evaluates
     int* reroute_list;        // blocks that end without any candidate are appended here (and
     int* reroute_count;       // left unwritten) instead of being encoded; null: never
+    float reroute_above;      // blocks whose best error exceeds this are encoded and also appended
+    float* reroute_err;       // [list position]: error of the block already written (3e38: none)
+    const float* prev_err;    // full-search pass: write a block only if its error is below this
+    // Partitioned-block work list of the proposal pass: four lists (P = 1..4) of
+    // position << 5 | slot, pb_stride apart, with counts pb_count[0..3].  Null: every
+    // slot of every block is an item.
+    const uint32_t* pb_list;
+    const int* pb_count;
+    int pb_stride;
+    // Work counters (null: not counted): [0..3] partitioned blocks searched by the front,
+    // by P; [4] decimation modes and [5] block modes it evaluated; [6..9] candidates
+    // refined, by P; [10..12] partition searches, P = 2..4.
+    unsigned long long* work;
 };
+constexpr int kWorkCounters = 16;
+
+// Launch grid caps for kernels that walk device-side lists (grid-stride loops).
+constexpr int kListGridFront = 148 * 8 * 4;
+constexpr int kListGridRefine = 148 * 6 * 4;
+constexpr int kListGridSearch = 148 * 4 * 4;
+constexpr int kListGridPack = 148 * 8;
 
 // Global index of the chunk's lb-th block, or -1 past the end of a block list.
 __host__ __device__ inline int chunk_block(const KernelArgs& a, int lb) {
@@ -91,6 +111,23 @@ __host__ __device__ inline int chunk_block(const KernelArgs& a, int lb) {
 }
 
 #ifdef __CUDACC__
+// Blocks a launch covers: the chunk, or the device-side count of its block list.
+__device__ __forceinline__ int list_blocks(const KernelArgs& a) {
+    return a.block_list ? min(*a.block_count, a.nblocks) : a.nblocks;
+}
+
+// Partitioned blocks of the proposal pass, and item i's list position and slot.
+__device__ __forceinline__ int pb_total(const KernelArgs& a) {
+    return a.pb_count[0] + a.pb_count[1] + a.pb_count[2] + a.pb_count[3];
+}
+__device__ __forceinline__ void pb_item(const KernelArgs& a, int i, int& lb, int& slot) {
+    int p = 0;
+    while (p < 3 && i >= a.pb_count[p]) { i -= a.pb_count[p]; p++; }
+    const uint32_t v = a.pb_list[(size_t)p * a.pb_stride + i];
+    lb = (int)(v >> 5);
+    slot = (int)(v & 31);
+}
+
 // Where block blk's texels come from: the image, its size and the block's
 // top-left texel.
 struct BlockSrc {

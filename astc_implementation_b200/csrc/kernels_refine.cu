@@ -555,55 +555,71 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     int* keys = reinterpret_cast<int*>(tps + ((kRefinePBs * T + 15) & ~15));
     float* uwc_all = reinterpret_cast<float*>(keys + kRefineThreads);
     const int tid = threadIdx.x;
-    // slot-major order: consecutive CTAs hold partitioned blocks of the same slot
-    // (hence the same partition count), so co-resident warps run the same code
-    const int npb = a.nblocks * a.slots;
-    {
-        const int pbl = tid / kNumCand, k = tid % kNumCand;
-        const int li = blockIdx.x * kRefinePBs + pbl;
-        int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
-        const int blk = li < npb ? chunk_block(a, li % a.nblocks) : -1;
-        if (blk >= 0) {
-            const int slot = li / a.nblocks, lb = li % a.nblocks;
-            const PBRec& r = a.pbrec[lb * a.slots + slot];
-            if (k < (int)r.ncand) key = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
-            if (r.ncand > 0) {
-                const int P = r.P;
-                const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
-                const BlockSrc src = block_src(a, blk);
-                for (int t = k; t < T; t += kNumCand) {
-                    pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
-                    tps[pbl * T + t] = P > 1 ? prow[t] : 0;
+    // Items: every slot of every block in slot-major order (consecutive CTAs hold
+    // partitioned blocks of the same slot, hence the same partition count, so
+    // co-resident warps run the same code), or the proposal pass's work list.
+    const int nb = list_blocks(a);
+    const int npb = a.pb_list ? pb_total(a) : nb * a.slots;
+    const int ngroups = (npb + kRefinePBs - 1) / kRefinePBs;
+    __shared__ unsigned int refined[4];  // candidates refined by this CTA, by P (work counters)
+    if (tid < 4) refined[tid] = 0;
+    for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        int my_lb = -1, my_slot = 0;  // this thread's partitioned block in the staging order
+        {
+            const int pbl = tid / kNumCand, k = tid % kNumCand;
+            const int li = grp * kRefinePBs + pbl;
+            int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
+            if (li < npb) {
+                int slot, lb;
+                if (a.pb_list) pb_item(a, li, lb, slot);
+                else { slot = li / nb; lb = li % nb; }
+                my_lb = lb; my_slot = slot;
+                const PBRec& r = a.pbrec[lb * a.slots + slot];
+                if (k < (int)r.ncand) key = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
+                if (r.ncand > 0) {
+                    const int P = r.P;
+                    const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
+                    const BlockSrc src = block_src(a, chunk_block(a, lb));
+                    for (int t = k; t < T; t += kNumCand) {
+                        pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
+                        tps[pbl * T + t] = P > 1 ? prow[t] : 0;
+                    }
                 }
             }
+            keys[tid] = key * kRefineThreads + tid;  // unique keys: decimation mode, then position
+            cs[tid].pad = (uint32_t)(my_lb + 1) | ((uint32_t)my_slot << 27);  // item of staging position tid
         }
-        keys[tid] = key * kRefineThreads + tid;  // unique keys: decimation mode, then position
-    }
-    __syncthreads();
-    // Thread tid takes the candidate of rank tid in decimation-mode order, so a
-    // warp's candidates mostly share loop bounds and table rows.
-    int mine = 0;
-    {
-        const int kk = keys[tid];
-        int rank = 0;
-        for (int j = 0; j < kRefineThreads; j++) rank += keys[j] < kk;
         __syncthreads();
-        keys[rank] = tid;
-        __syncthreads();
-        mine = keys[tid];
+        // Thread tid takes the candidate of rank tid in decimation-mode order, so a
+        // warp's candidates mostly share loop bounds and table rows.
+        int mine = 0;
+        {
+            const int kk = keys[tid];
+            int rank = 0;
+            for (int j = 0; j < kRefineThreads; j++) rank += keys[j] < kk;
+            __syncthreads();
+            keys[rank] = tid;
+            __syncthreads();
+            mine = keys[tid];
+        }
+        const int pbl = mine / kNumCand, k = mine % kNumCand;
+        const uint32_t item = cs[pbl * kNumCand].pad;  // written by the thread that staged partitioned block pbl
+        __syncthreads();  // every thread has read the item words before the candidate state overwrites them
+        if (item != 0) {
+            const int lb = (int)(item & 0x07FFFFFFu) - 1, slot = (int)(item >> 27);
+            const int pb = lb * a.slots + slot;
+            const PBRec& rec = a.pbrec[pb];
+            Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
+            snap->err = ERR_DEFAULT;  // inert slot unless refined below
+            if (k < (int)rec.ncand) {
+                float* uwc = T <= kUwCacheTexels ? uwc_all + tid : nullptr;
+                refine_candidate(a, rec, (int)rec.P, k, pxs + pbl * T, tps + pbl * T, cs[tid], uwc, snap);
+                if (a.work) atomicAdd(&refined[rec.P - 1], 1u);
+            }
+        }
+        __syncthreads();  // the next group reuses shared memory
     }
-    const int pbl = mine / kNumCand, k = mine % kNumCand;
-    const int li = blockIdx.x * kRefinePBs + pbl;
-    if (li >= npb) return;
-    const int slot = li / a.nblocks, lb = li % a.nblocks;
-    if (chunk_block(a, lb) < 0) return;
-    const int pb = lb * a.slots + slot;
-    const PBRec& rec = a.pbrec[pb];
-    Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
-    snap->err = ERR_DEFAULT;  // inert slot unless refined below
-    if (k >= (int)rec.ncand) return;
-    float* uwc = T <= kUwCacheTexels ? uwc_all + tid : nullptr;
-    refine_candidate(a, rec, (int)rec.P, k, pxs + pbl * T, tps + pbl * T, cs[tid], uwc, snap);
+    if (a.work && tid < 4 && refined[tid]) atomicAdd(a.work + 6 + tid, (unsigned long long)refined[tid]);
 }
 
 // ------------------------------------------------------------ k_select_pack
@@ -673,14 +689,12 @@ __device__ __forceinline__ int bitrev8(int p) {
     return p;
 }
 
-__global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ KernelArgs a) {
-    const int lb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lb >= a.nblocks) return;
-    const int blk = chunk_block(a, lb);
-    if (blk < 0) return;
+__device__ __noinline__ void select_pack_one(const KernelArgs& a, int lb, int blk) {
     float best = 1e30f;
     int win_slot = -1, win_k = 0;
-    for (int s = 0; s < a.slots; s++) {
+    // slots the front filled: all of them, or P=1 plus the proposed partitionings
+    const int nslots = a.prop ? 1 + (int)a.prop[lb].n : a.slots;
+    for (int s = 0; s < nslots; s++) {
         const PBRec& r = a.pbrec[(size_t)lb * a.slots + s];
         const int n = r.ncand;
         for (int k = 0; k < n; k++) {
@@ -689,8 +703,17 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
         }
     }
     if (win_slot < 0 && a.reroute_list) {  // proposal search found nothing: hand the block to the full search
-        a.reroute_list[atomicAdd(a.reroute_count, 1)] = blk;
+        const int pos = atomicAdd(a.reroute_count, 1);
+        a.reroute_list[pos] = blk;
+        a.reroute_err[pos] = 3e38f;
         return;
+    }
+    if (a.prev_err && !(best < a.prev_err[lb])) return;  // the proposal search's result stands
+    if (a.reroute_list && a.reroute_above > 0.0f && best > a.reroute_above) {
+        // a poor proposal-search result: write it, and let the full search try to beat it
+        const int pos = atomicAdd(a.reroute_count, 1);
+        a.reroute_list[pos] = blk;
+        a.reroute_err[pos] = best;
     }
     uint8_t blockbytes[18];
     uint32_t sym[8 + 4 + 32];  // header words of the SymbolicBlock record
@@ -766,6 +789,12 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
     }
 }
 
+__global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ KernelArgs a) {
+    const int nb = list_blocks(a);
+    for (int lb = blockIdx.x * blockDim.x + threadIdx.x; lb < nb; lb += gridDim.x * blockDim.x)
+        select_pack_one(a, lb, chunk_block(a, lb));
+}
+
 }  // namespace
 
 size_t refine_smem_bytes(const TableLayout& L) {
@@ -798,12 +827,16 @@ cudaError_t configure_kernels(const TableLayout& L) {
 
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
     const int npb = a.nblocks * a.slots;
-    k_refine<<<(npb + kRefinePBs - 1) / kRefinePBs, kRefineThreads, refine_smem_bytes(a.L), s>>>(a);
+    int grid = (npb + kRefinePBs - 1) / kRefinePBs;
+    if (a.block_list) grid = std::min(grid, kListGridRefine);
+    k_refine<<<grid, kRefineThreads, refine_smem_bytes(a.L), s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_select_pack(const KernelArgs& a, cudaStream_t s) {
-    k_select_pack<<<(a.nblocks + 127) / 128, 128, 0, s>>>(a);
+    int grid = (a.nblocks + 127) / 128;
+    if (a.block_list) grid = std::min(grid, kListGridPack);
+    k_select_pack<<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

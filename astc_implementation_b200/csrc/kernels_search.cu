@@ -13,6 +13,8 @@
 // Sums whose order the reference leaves to float atomics are taken in ascending
 // texel / weight order by a single thread, so results are bit-identical to the
 // CPU oracle (oracle/astc_oracle.cpp), which fixes the same order.
+#include <algorithm>
+
 #include "device_math.cuh"
 #include "kernels.h"
 
@@ -327,15 +329,18 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
 __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kSearchWarps + warp;
-    if (item >= a.nblocks * 3) return;
-    const int lb = item % a.nblocks, P = item / a.nblocks + 2;  // P-major: a CTA's warps share P
     uint8_t* ws = smem + warp * kSearchWarpBytes;
-    const int blk = chunk_block(a, lb);
-    if (blk < 0) return;
-    if (P == 2) search_one<2>(a, blk, lb, ws, lane);
-    else if (P == 3) search_one<3>(a, blk, lb, ws, lane);
-    else search_one<4>(a, blk, lb, ws, lane);
+    const int nb = list_blocks(a);
+    // P-major items: a CTA's warps share P; one pass for a chunk, a grid-stride loop over a block list
+    for (int item = blockIdx.x * kSearchWarps + warp; item < nb * 3; item += gridDim.x * kSearchWarps) {
+        const int lb = item % nb, P = item / nb + 2;
+        const int blk = chunk_block(a, lb);
+        if (P == 2) search_one<2>(a, blk, lb, ws, lane);
+        else if (P == 3) search_one<3>(a, blk, lb, ws, lane);
+        else search_one<4>(a, blk, lb, ws, lane);
+        if (a.work && lane == 0) atomicAdd(a.work + 10 + (P - 2), 1ull);
+        __syncwarp();
+    }
 }
 
 // ============================================================ passes 01-12
@@ -838,6 +843,21 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     }
     __syncthreads();
     PBRec& rec = a.pbrec[(size_t)lb * a.slots + slot_in_block];
+    if (a.work && tid == 0) {
+        int nbm_run = nbm;
+        if (bmm) {
+            nbm_run = 0;
+            for (int w = 0; w < kMaskWords; w++) {
+                const int lo = w * 64;
+                if (lo >= nbm) break;
+                const uint64_t valid = nbm - lo >= 64 ? ~0ull : ((1ull << (nbm - lo)) - 1);
+                nbm_run += __popcll(bmm[w] & valid);
+            }
+        }
+        atomicAdd(a.work + (P - 1), 1ull);
+        atomicAdd(a.work + 4, (unsigned long long)ndm_run);
+        atomicAdd(a.work + 5, (unsigned long long)nbm_run);
+    }
     if (tid == 0) {
         int n = 0;
         while (n < a.topn && M.top[n] >= 0) n++;
@@ -871,32 +891,36 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
 
 __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
-    // slot-major order so that co-resident CTAs work on the same partition count
-    const int li = blockIdx.x;
-    if (li >= a.nblocks * a.slots) return;
-    const int k = li / a.nblocks, lb = li % a.nblocks;
-    const int blk = chunk_block(a, lb);
-    if (blk < 0) return;
-    if (k == 0) { front_body(a, 1, lb, blk, 0, 0, smem); return; }
-    int P, entry;
-    bool present;
-    if (a.prop) {
-        const PropPicks& pp = a.prop[lb];
-        present = k - 1 < (int)pp.n;
-        const int v = present ? pp.v[k - 1] : 0;
-        P = 2 + (v >> 10); entry = v & 1023;
-    } else {
-        P = 2 + (k - 1) / 4;
-        const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
-        const int i = (k - 1) % 4;
-        present = i < pk[4];
-        entry = present ? pk[i] : 0;
+    // Items: every slot of every block in slot-major order (co-resident CTAs work on the
+    // same partition count), or the proposal pass's work list grouped by partition count.
+    const int nb = list_blocks(a);
+    const int items = a.pb_list ? pb_total(a) : nb * a.slots;
+    for (int li = blockIdx.x; li < items; li += gridDim.x) {
+        int k, lb;
+        if (a.pb_list) pb_item(a, li, lb, k);
+        else { k = li / nb; lb = li % nb; }
+        const int blk = chunk_block(a, lb);
+        int P = 1, entry = 0;
+        bool present = true;
+        if (k > 0 && a.prop) {
+            const PropPicks& pp = a.prop[lb];
+            present = k - 1 < (int)pp.n;
+            const int v = present ? pp.v[k - 1] : 0;
+            P = 2 + (v >> 10); entry = v & 1023;
+        } else if (k > 0) {
+            P = 2 + (k - 1) / 4;
+            const uint16_t* pk = a.picks[lb].v + (P - 2) * 5;
+            const int i = (k - 1) % 4;
+            present = i < pk[4];
+            entry = present ? pk[i] : 0;
+        }
+        if (!present) {
+            if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * a.slots + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
+            continue;  // uniform across the CTA
+        }
+        front_body(a, P, lb, blk, k, entry, smem);
+        __syncthreads();  // the next item reuses shared memory
     }
-    if (!present) {
-        if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * a.slots + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
-        return;
-    }
-    front_body(a, P, lb, blk, k, entry, smem);
 }
 
 }  // namespace
@@ -912,13 +936,16 @@ cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
 
 cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
     const int items = a.nblocks * 3;
-    const int grid = (items + kSearchWarps - 1) / kSearchWarps;
+    int grid = (items + kSearchWarps - 1) / kSearchWarps;
+    if (a.block_list) grid = std::min(grid, kListGridSearch);
     k_partition_search<<<grid, kSearchWarps * 32, search_smem_bytes(a.L), s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
-    k_front<<<a.nblocks * a.slots, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
+    int grid = a.nblocks * a.slots;
+    if (a.block_list) grid = std::min(grid, kListGridFront);
+    k_front<<<grid, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
     return cudaGetLastError();
 }
 

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     if (lane == 0) pos = atomicAdd(&r.counts[confident ? 0 : 1], 1);
     pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
     if (!confident) {
-        if (lane == 0) r.full[pos] = blk;
+        if (lane == 0) { r.full[pos] = blk; r.full_err[pos] = 3e38f; }
         return;
     }
     // propose the shortest best-first prefix whose mass reaches the coverage
@@ -405,6 +405,12 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
         PropPicks& pp = r.prop[pos];
         pp.n = (uint16_t)used;
         for (int k = 0; k < kMaxProposals; k++) pp.v[k] = k < used ? picks[k] : 0;
+        // the work list: slot 0 (P = 1) and one slot per proposed partitioning, by P
+        r.pb_list[atomicAdd(&r.counts[2], 1)] = (uint32_t)pos << 5;
+        for (int k = 0; k < used; k++) {
+            const int p = 1 + (picks[k] >> 10);  // list of P = 2 + (v >> 10)
+            r.pb_list[(size_t)p * r.pb_stride + atomicAdd(&r.counts[2 + p], 1)] = ((uint32_t)pos << 5) | (uint32_t)(k + 1);
+        }
     }
     // block-mode masks: the kbm best modes of each partition count's head
     uint64_t* mk = r.masks + (size_t)pos * 4 * kMaskWords;

@@ -71,13 +71,19 @@ struct Select {
 
 // Output of the selection kernel for one chunk.
 struct Routes {
-    int* counts;          // [0] pruned blocks, [1] full-search blocks (zeroed before the launch)
+    int* counts;          // [0] pruned blocks, [1] full-search blocks, [2..5] partitioned blocks
+                          // of P = 1..4 in pb_list (zeroed before the launch)
     int* pruned;          // [chunk] global block indices taking the proposal search
     int* full;            // [chunk] global block indices taking the full search
+    float* full_err;      // [chunk] error of a result already written for full[i] (3e38: none)
     PropPicks* prop;      // [chunk] by position in `pruned`
     uint64_t* masks;      // [chunk][4][kMaskWords] by position in `pruned`
     float* confidence;    // [chunk] by chunk row (P=1 plus kmax-best probability), may be null
+    uint32_t* pb_list;    // [4][pb_stride]: position << 5 | slot of every partitioned block to search
+    int pb_stride;
 };
+
+constexpr int kRouteCounters = 8;  // ints per chunk: routes, then partitioned-block counts, padding
 
 constexpr int kMlpSmemBytes = 65536 + 131072 + 1024 + 1024;
 

@@ -37,12 +37,14 @@ int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const Fo
     if ((rc = ensure_buf(ctx, sc.logits, sc.cap_logits, blocks * nd->net.s.nout * sizeof(float), "cudaMalloc logits"))) return rc;
     if ((rc = ensure_buf(ctx, sc.lists, sc.cap_lists, blocks * 2 * sizeof(int), "cudaMalloc block lists"))) return rc;
     if ((rc = ensure_buf(ctx, sc.prop, sc.cap_prop, blocks * sizeof(PropPicks), "cudaMalloc proposals"))) return rc;
-    return ensure_buf(ctx, sc.masks, sc.cap_masks, blocks * 4 * kMaskWords * sizeof(uint64_t), "cudaMalloc block-mode masks");
+    if ((rc = ensure_buf(ctx, sc.masks, sc.cap_masks, blocks * 4 * kMaskWords * sizeof(uint64_t), "cudaMalloc block-mode masks"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.full_err, sc.cap_ferr, blocks * sizeof(float), "cudaMalloc full-search errors"))) return rc;
+    return ensure_buf(ctx, sc.pbl, sc.cap_pbl, blocks * 4 * kMaxProposals * sizeof(uint32_t), "cudaMalloc work lists");
 }
 
 int begin_routes(astcb200_ctx* ctx, size_t chunks) {
     ctx->counts_used = 0;
-    int rc = ensure_buf(ctx, ctx->d_counts, ctx->counts_cap, std::max<size_t>(chunks, 1) * 2 * sizeof(int), "cudaMalloc route counters");
+    int rc = ensure_buf(ctx, ctx->d_counts, ctx->counts_cap, std::max<size_t>(chunks, 1) * mlp::kRouteCounters * sizeof(int), "cudaMalloc route counters");
     if (rc) return rc;
     if (!ctx->d_mlp_error) {
         size_t cap = 0;
@@ -88,8 +90,11 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     }
     const Pruning& pr = ctx->pruning;
     const size_t n = (size_t)a.nblocks;
-    if (ctx->counts_used * 2 + 2 > ctx->counts_cap / sizeof(int)) { ctx->err = "route counters exhausted"; return ASTCB200_BAD_ARG; }
-    int* counts = ctx->d_counts + 2 * ctx->counts_used++;
+    if ((ctx->counts_used + 1) * mlp::kRouteCounters > ctx->counts_cap / sizeof(int)) {
+        ctx->err = "route counters exhausted";
+        return ASTCB200_BAD_ARG;
+    }
+    int* counts = ctx->d_counts + mlp::kRouteCounters * ctx->counts_used++;
     mlp::Select sel;
     sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
     for (int i = 0; i < 3; i++) sel.sel[i] = (int)ft->L.count_selected[i + 1];
@@ -97,9 +102,12 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     r.counts = counts;
     r.pruned = sc.lists;
     r.full = sc.lists + n;
+    r.full_err = sc.full_err;
     r.prop = sc.prop;
     r.masks = sc.masks;
     r.confidence = nullptr;
+    r.pb_list = sc.pbl;
+    r.pb_stride = (int)(n * kMaxProposals);
 
     KernelArgs ap = a;  // proposal-search pass
     ap.block_first = 0;
@@ -107,14 +115,21 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     ap.prop = r.prop; ap.bm_mask = r.masks;
     ap.slots = 1 + pr.kmax; ap.topn = pr.topn;
     ap.reroute_list = r.full; ap.reroute_count = counts + 1;  // blocks left without a candidate
+    ap.pb_list = r.pb_list; ap.pb_count = counts + 2; ap.pb_stride = r.pb_stride;
+    ap.reroute_err = r.full_err;
+    {   // the threshold in the search's error units: 8-bit per-texel error x texels x (65536/255)^2
+        const float s8 = 65536.0f / 255.0f;
+        ap.reroute_above = pr.reroute_error > 0.0f ? pr.reroute_error * (float)ft->L.T * s8 * s8 : 0.0f;
+    }
     KernelArgs af = a;  // full-search pass over the low-confidence and rerouted blocks
     af.block_first = 0;
     af.block_list = r.full; af.block_count = counts + 1;
+    af.prev_err = r.full_err;
     af.slots = kSlotsPerBlock; af.topn = kNumCand;
     af.pbrec = sc.pbrec + n * kMaxSlots;
     af.snaps = sc.snaps + n * kMaxSlots * kNumCand;
 
-    CK(cudaMemsetAsync(counts, 0, 2 * sizeof(int), s), "reset route counters");
+    CK(cudaMemsetAsync(counts, 0, mlp::kRouteCounters * sizeof(int), s), "reset route counters");
     if ((rc = done(mlp::launch_mlp_logits(a, nd->net, sc.logits, ctx->d_mlp_error, s), "k_mlp_logits", 0))) return rc;
     if ((rc = done(mlp::launch_select(a, nd->net, sc.logits, sel, r, s), "k_select", 0))) return rc;
     if ((rc = done(launch_front(ap, s), "k_front", 1))) return rc;
@@ -226,7 +241,7 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     if (!ctx || !cfg || cfg->struct_size < sizeof(astcb200_pruning)) return ASTCB200_BAD_ARG;
     if (cfg->enable && (cfg->max_partitionings > (uint32_t)kMaxProposals || cfg->block_modes == 0 || cfg->block_modes > 64 ||
                         cfg->refine_candidates == 0 || cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
-                        !(cfg->threshold >= 0.0f)))
+                        !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f)))
         return ASTCB200_BAD_ARG;
     Pruning& p = ctx->pruning;
     p.enable = cfg->enable != 0;
@@ -235,6 +250,7 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.topn = (int)cfg->refine_candidates;
     p.coverage = cfg->coverage;
     p.threshold = cfg->threshold;
+    p.reroute_error = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->reroute_error : 0.0f;
     release_batches(ctx);  // captured graphs hold the previous settings
     return ASTCB200_OK;
 }
@@ -245,9 +261,12 @@ int astcb200_pruning_stats(astcb200_ctx* ctx, uint64_t* proposal_blocks, uint64_
     if (!ctx->counts_used) return ASTCB200_OK;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     CK(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
-    std::vector<int> c(2 * ctx->counts_used);
+    std::vector<int> c((size_t)mlp::kRouteCounters * ctx->counts_used);
     CK(cudaMemcpy(c.data(), ctx->d_counts, c.size() * sizeof(int), cudaMemcpyDeviceToHost), "read route counters");
-    for (uint32_t i = 0; i < ctx->counts_used; i++) { *proposal_blocks += (uint64_t)c[2 * i]; *full_blocks += (uint64_t)c[2 * i + 1]; }
+    for (uint32_t i = 0; i < ctx->counts_used; i++) {
+        *proposal_blocks += (uint64_t)c[mlp::kRouteCounters * i];
+        *full_blocks += (uint64_t)c[mlp::kRouteCounters * i + 1];
+    }
     int err = 0;
     if (ctx->d_mlp_error) CK(cudaMemcpy(&err, ctx->d_mlp_error, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
     if (err) { ctx->err = "a network inference CTA gave up waiting for its copies or MMAs"; return ASTCB200_TIMEOUT; }

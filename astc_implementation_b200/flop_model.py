@@ -40,6 +40,52 @@ def _tables(lib, bx, by):
     return c, bms, dmodes, dinfo
 
 
+def _parts(lib, bx, by):
+    c, bms, dmodes, dinfo = _tables(lib, bx, by)
+    T = bx * by
+    valid_dm = [i for i in range(len(dmodes)) if dmodes[i, 2] & 0xFF]
+    Ws = np.array([int(dinfo[i, 1]) for i in valid_dm], float)
+    Es = np.array([int(dinfo[i, 8:8 + T].sum()) for i in valid_dm], float)
+    Ss = np.array([int(dinfo[i, 5]) for i in valid_dm], float)
+    valid_set = set(valid_dm)
+    nbm = sum(1 for b in bms if b[4] == 0 and int(b[1]) in valid_set)
+    Wm, Em = Ws.mean(), Es.mean()
+    dm_costs = [((13 * E + 4 * W) if W < T else 0.0) + (35 * W + 320) + (10 * S * W + 10 * S) + 200 for W, E, S in zip(Ws, Es, Ss)]
+    p16 = float(np.mean([35 * T if W == T else E * (2 * E / T + 38) for W, E in zip(Ws, Es)]))
+    return c, T, nbm, Wm, Em, dm_costs, p16
+
+
+def from_work(lib, bx, by, work, mlp_blocks=0):
+    """FP32 operations of each kernel for the work counters of astcb200_work_counters
+    (the per-partitioned-block, per-decimation-mode, per-block-mode, per-candidate and
+    per-partition-search terms of the model above, counted as the kernels ran them), and
+    the tensor-core operations of the proposal network for mlp_blocks blocks."""
+    c, T, nbm, Wm, Em, dm_costs, p16 = _parts(lib, bx, by)
+    w = np.asarray(work, np.float64)
+    front = sum(w[P - 1] * (40 * T + 60 * T + 680 * P + 2 * nbm) for P in (1, 2, 3, 4))
+    front += w[4] * float(np.mean(dm_costs)) + w[5] * (12 * Wm + 2 * Em + 4 * T + 30)
+
+    def refine_cand(P):
+        p13 = Wm + 2 * Em + 45 * T + 60 * P
+        p17 = 2 * Em + 20 * T
+        return p17 + 6 * (p13 + 900 * P + 40 * P + p16 + p17)
+
+    refine = sum(w[6 + P - 1] * refine_cand(P) for P in (1, 2, 3, 4))
+    search = sum(w[10 + P - 2] * (48 * T * P + 6 * int(c[5 + P - 1]) * P * P + 3 * (1024 * 55 / 2) + 128 * 60 * T)
+                 for P in (2, 3, 4))
+    return {"search": search, "front": front, "refine": refine, "mlp": mlp_blocks * mlp_flops(lib, bx, by)}
+
+
+def mlp_flops(lib, bx, by):
+    """Multiply-add operations (2 per MAC) of the proposal network for one block."""
+    import ctypes
+    u = [ctypes.c_uint32() for _ in range(6)]
+    sel = (ctypes.c_uint32 * 3)()
+    lib.astcb200_proposal_layout(bx, by, *[ctypes.byref(x) for x in u], sel)
+    k0p, nout = u[1].value, u[2].value
+    return 2.0 * (k0p * 256 + 256 * 256 + 256 * nout)
+
+
 def per_block(lib, bx, by):
     """Returns {'search':, 'front':, 'refine':, 'total':, 'bytes':} per block."""
     c, bms, dmodes, dinfo = _tables(lib, bx, by)

@@ -247,6 +247,15 @@ def run_batch(args):
 
 
 # ---------------------------------------------------------------- B200 arm
+PRUNING = dict(max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98, threshold=0.5, reroute_error=8.0)
+CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    return json.load(open(path)) if os.path.exists(path) else {}
+
+
 def main():
     global SIZE, FOOTPRINTS
     ap = argparse.ArgumentParser()
@@ -259,6 +268,10 @@ def main():
     ap.add_argument("--size", type=int, default=SIZE, help="texture side (default: the 2048x2048 workload)")
     ap.add_argument("--footprints", default="4x4,6x6")
     ap.add_argument("--workload", default="plain", choices=["plain", "batch"])
+    ap.add_argument("--method", default="proposal", choices=["proposal", "full"],
+                    help="timed method: the learned proposal search (headline) or the full search alone")
+    ap.add_argument("--skip-full", action="store_true",
+                    help="do not run the full search for comparison (profiling the timed method alone)")
     args = ap.parse_args()
     SIZE = args.size
     FOOTPRINTS = [tuple(int(v) for v in f.split("x")) for f in args.footprints.split(",")]
@@ -269,7 +282,7 @@ def main():
 
     import torch
     import astc_implementation_b200 as ab
-    from astc_implementation_b200 import flop_model, synth
+    from astc_implementation_b200 import flop_model, proposal, synth
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
@@ -281,50 +294,87 @@ def main():
 
     seeds = rank_seeds(rank)
     imgs = [synth.make_texture(SIZE, SIZE, s) for s in seeds]
-    d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
     # a created stream: handle 0 (the legacy default stream) would select the encoder's own stream
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
+    d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
+    use_prop = args.method == "proposal"
     encs, outs = [], []
     for bx, by in FOOTPRINTS:
-        e = ab.ASTCEncoder(device=local, stage_timing=True)
+        e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, stage_timing=True)
         e.init()
         e.secondaryInit(SIZE, SIZE, bx, by)
+        if use_prop:
+            e.set_proposal_net(proposal.load_weights(bx, by))
         encs.append(e)
         outs.append(torch.empty(e.numBlocks * 16, dtype=torch.uint8, device="cuda"))
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    stage_ms = np.zeros((len(FOOTPRINTS), 4))
-    stage_n = np.zeros((len(FOOTPRINTS), 4))
+    names = ["k_partition_search / k_mlp_logits + k_select", "k_front", "k_refine", "k_select_pack"]
 
-    def step(i, record):
-        flush.fill_(i & 0xFF)
-        for k, e in enumerate(encs):
-            e.encode_device(d_imgs[i % 4].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
-            if record:
-                ms, n = e.stage_times()
-                stage_ms[k] += ms
-                stage_n[k] += n
+    def set_method(prop):
+        for e in encs:
+            if use_prop:
+                e.set_pruning(prop, **PRUNING)
 
-    for i in range(args.warmup):
-        step(i, False)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    def run(steps, warmup, record):
+        """Mean ms per step over `steps` timed steps (max over ranks), per-stage ms and
+        launches, and the work counters, summed over the timed steps."""
+        stage_ms = np.zeros((len(FOOTPRINTS), 4))
+        stage_n = np.zeros((len(FOOTPRINTS), 4))
+        work = np.zeros((len(FOOTPRINTS), 16))
+
+        def step(i, rec):
+            flush.fill_(i & 0xFF)
+            for k, e in enumerate(encs):
+                e.encode_device(d_imgs[i % 4].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
+                if rec:
+                    ms, n = e.stage_times()
+                    stage_ms[k] += ms
+                    stage_n[k] += n
+                    work[k] += e.work_counters().astype(np.float64)
+
+        for i in range(warmup):
+            step(i, False)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for i in range(steps):
+            step(i, record)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1), stage_ms, stage_n, work
+
+    def psnrs():
+        out = []
+        for k, (bx, by) in enumerate(FOOTPRINTS):
+            for im in imgs:
+                out.append(ab.psnr(ab.decode(bx, by, SIZE, SIZE, encs[k].encode(im)), im))
+        return out
+
+    # the full search on the same images: its speed and quality are the reference point
+    full_rate, full_ms, full_psnr = None, None, None
+    if not args.skip_full:
+        set_method(False)
+        full_ms, _, _, _ = run(max(1, min(args.steps, 3)), 1, True)
+        full_rate, full_ms = job_rate(texels_per_step() * max(1, min(args.steps, 3)), full_ms, dist, "cuda")
+        full_psnr = psnrs() if use_prop else None
+
+    # the timed method
+    set_method(True)
     clocks = ClockSampler(local)
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    t0.record(stream)
-    for i in range(args.steps):
-        step(i, True)
-    t1.record(stream)
-    torch.cuda.synchronize()
+    ms, stage_ms, stage_n, work = run(args.steps, args.warmup, True)
     clk = clocks.stop()
-    value, ms = job_rate(texels_per_step() * args.steps, t0.elapsed_time(t1), dist, "cuda")
+    value, ms = job_rate(texels_per_step() * args.steps, ms, dist, "cuda")
     if dist:
         dist.barrier()
     launches = int(stage_n.sum())
+    prop_psnr = psnrs() if use_prop and full_psnr else None
+    routes = [e.pruning_stats() for e in encs] if use_prop else None
 
-    # e2e through the public host API
+    # e2e through the public host API, same method
     host_steps = max(1, min(args.steps, 3))
     t_e2e = time.perf_counter()
     for i in range(host_steps):
@@ -339,53 +389,80 @@ def main():
             dist.destroy_process_group()
         return 0
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: the op-count model applied to the work counters
     lib = ab.load_library()
-    names = ["k_partition_search", "k_front", "k_refine", "k_select_pack"]
-    model_keys = ["search", "front", "refine", None]
-    models = [flop_model.per_block(lib, bx, by) for bx, by in FOOTPRINTS]
     tot_ms = stage_ms.sum(axis=0)
-    dom = int(np.argmax(tot_ms))
-    dom_flops = sum(models[k][model_keys[dom]] * blocks_of(*FOOTPRINTS[k]) for k in range(len(FOOTPRINTS))) * args.steps \
-        if model_keys[dom] else 0.0
-    dom_launches = int(stage_n[:, dom].sum())
-    avg_launch_ms = tot_ms[dom] / max(dom_launches, 1)
-    achieved = dom_flops / dom_launches / (avg_launch_ms / 1000.0) / 1e12 if dom_launches else 0.0
+    dom = int(np.argmax(tot_ms[1:]) + 1) if use_prop else int(np.argmax(tot_ms))
+    flops = {"search": 0.0, "front": 0.0, "refine": 0.0, "mlp": 0.0}
+    for k, (bx, by) in enumerate(FOOTPRINTS):
+        f = flop_model.from_work(lib, bx, by, work[k], blocks_of(bx, by) * args.steps if use_prop else 0)
+        for key in flops:
+            flops[key] += f[key]
+    dom_key = ["search", "front", "refine", None][dom]
+    dom_ms = tot_ms[dom]
+    achieved = flops[dom_key] / (dom_ms / 1000.0) / 1e12 if dom_key and dom_ms > 0 else 0.0
     peak = ab.fp32_peak_tflops(local)
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        per_block = json.load(open(tpath)).get(names[dom], {}).get("dram_bytes_per_block")
-        if per_block:  # measured DRAM bytes per block (ncu) x blocks per launch
-            blocks = sum(blocks_of(*fp) for fp in FOOTPRINTS) * args.steps
-            traffic = round(per_block * blocks / max(dom_launches, 1))
+    if os.path.exists(tpath) and dom_key in ("front", "refine") and stage_n[:, dom].sum():
+        # DRAM bytes measured by ncu per block of the full search (13 partitioned blocks,
+        # 104 candidates), scaled to the partitioned blocks / candidates this run processed
+        kname = "k_front" if dom_key == "front" else "k_refine"
+        per_block = json.load(open(tpath)).get(kname, {}).get("dram_bytes_per_block")
+        if per_block:
+            units = work[:, 0:4].sum() / 13.0 if dom_key == "front" else work[:, 6:10].sum() / 104.0
+            traffic = round(per_block * units / stage_n[:, dom].sum())
+    peaks = measured_peaks()
     cpu = None
     if not args.no_cpu_baseline:
         rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample)
         cpu = {"value": round(rate, 4), "unit": "Mtexel/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": "%dx%d crop of the seed-1 texture at 4x4 and 6x6 (%.1f s of CPU time)" % (args.cpu_sample, args.cpu_sample, secs)}
-    total_model = sum(models[k]["total"] * blocks_of(*FOOTPRINTS[k]) for k in range(len(FOOTPRINTS))) * args.steps * world
+               "sample": "%dx%d crop of the seed-1 texture at %s, full search (%.1f s of CPU time)"
+                         % (args.cpu_sample, args.cpu_sample, " and ".join("%dx%d" % f for f in FOOTPRINTS), secs)}
+    fp_names = " and ".join("%dx%d" % f for f in FOOTPRINTS)
+    method = ("learned proposal search (%s), full search for low-confidence and poorly encoded blocks"
+              % ", ".join("%s=%s" % kv for kv in PRUNING.items())) if use_prop else "full search"
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mtexel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "%dx%d RGBA8 synthetic texture (seeds 1-4 per rank), full search at %s per step"
-                               % (SIZE, SIZE, " and ".join("%dx%d" % f for f in FOOTPRINTS)),
-                   "method": "full search (plain, no learned proposal)", "image": [SIZE, SIZE],
-                   "footprints": ["%dx%d" % f for f in FOOTPRINTS], "l2": "512 MiB memset before every step, inside the timed region",
+        "config": {"workload": "%dx%d RGBA8 synthetic texture (generator seeds 1-4 per rank), encoded at %s per step"
+                               % (SIZE, SIZE, fp_names),
+                   "method": method, "image": [SIZE, SIZE], "footprints": ["%dx%d" % f for f in FOOTPRINTS],
+                   "chunk_blocks": CHUNK, "l2": "512 MiB memset before every step, inside the timed region",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "per_footprint_ms": {"%dx%d" % fp: round(float(stage_ms[k].sum() / args.steps), 3) for k, fp in enumerate(FOOTPRINTS)},
+        "full_search": {"value": round(full_rate, 3), "unit": "Mtexel/s",
+                        "ms_per_step": round(full_ms / max(1, min(args.steps, 3)), 3)} if full_rate else None,
+        "speedup_vs_full_search": round(value / full_rate, 3) if full_rate else None,
         "stage_ms_per_step": {names[i]: round(float(tot_ms[i] / args.steps), 3) for i in range(4)},
-        "model_tflops_whole_step": round(total_model / (ms / 1000.0) / 1e12, 3),
         "roofline": {"kernel": names[dom], "bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2),
                      "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak else None, "traffic": traffic,
                      "peak_source": "FP32 FMA microbenchmark on this GPU in this run (an FMA counts 2 ops); "
-                                    "MEASURED_PEAKS.json has no FP32 figure"},
+                                    "MEASURED_PEAKS.json has no FP32 figure",
+                     "flops": "op-count model (flop_model.py) applied to the work the kernel did (device counters)"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e, 3), "unit": "Mtexel/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if use_prop and prop_psnr:
+        d = [p - f for p, f in zip(prop_psnr, full_psnr)]
+        line["psnr"] = {"mean_delta_db": round(float(np.mean(d)), 3), "min_delta_db": round(float(np.min(d)), 3),
+                        "full_search_db": [round(v, 3) for v in full_psnr], "proposal_db": [round(v, 3) for v in prop_psnr],
+                        "order": ["%dx%d seed %d" % (fp[0], fp[1], s) for fp in FOOTPRINTS for s in seeds]}
+    if use_prop:
+        line["routes"] = {"%dx%d" % fp: {"proposal_blocks": int(r[0]), "full_search_blocks": int(r[1])}
+                          for fp, r in zip(FOOTPRINTS, routes)}
+        det = [e.stage_times_detail() for e in encs]  # last step, per launch position
+        mlp_ms = sum(float(m[0]) for m, _ in det)
+        mlp_last = sum(flop_model.mlp_flops(lib, bx, by) * blocks_of(bx, by) for bx, by in FOOTPRINTS)
+        bf16_peak = peaks.get("bf16_tflops")
+        if mlp_ms:
+            ach = mlp_last / (mlp_ms / 1000.0) / 1e12
+            line["roofline_mlp"] = {"kernel": "k_mlp_logits", "bound": "tensor", "achieved": round(ach, 2),
+                                    "peak": bf16_peak, "unit": "TFLOP/s",
+                                    "frac": round(ach / bf16_peak, 4) if bf16_peak else None,
+                                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

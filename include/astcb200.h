@@ -175,6 +175,10 @@ typedef struct astcb200_pruning {
     uint32_t refine_candidates; /* refinement candidates per partitioned block, at most 8 */
     float coverage;             /* stop proposing once P=1 plus the proposed probability reaches this */
     float threshold;            /* full search when P=1 plus the best max_partitionings carry less */
+    float reroute_error;        /* a block whose proposal-search result has a larger per-texel error
+                                   (weighted squared, 8-bit units; weights R 0.675, G 1.3275,
+                                   B 0.2475, A 1) also takes the full search, and the better of
+                                   the two results is kept; 0 disables */
 } astcb200_pruning;
 /* Applies to later encodes of footprints that have a network (the others use the full search). */
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);
@@ -222,6 +226,19 @@ int astcb200_decode(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t
  * refine, select/pack) by the last encode call, summed over chunks; needs
  * ASTCB200_FLAG_STAGE_TIMING.  launches[4] receives the launch counts (optional). */
 int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* launches4);
+
+/* Per-launch device milliseconds of the last encode, summed over chunks by the launch's
+ * position in its chunk's sequence (full search: 4 launches; proposal search: network,
+ * selection, front, refine, select-pack of the proposal pass, then partition search, front,
+ * refine, select-pack of the full-search pass); stage9 receives each position's stage
+ * (0-3 as for astcb200_stage_times, -1 unused).  Needs ASTCB200_FLAG_STAGE_TIMING. */
+int astcb200_stage_times_detail(astcb200_ctx* ctx, float* ms9, int32_t* stage9);
+
+/* Work the search kernels did in the last encode with ASTCB200_FLAG_STAGE_TIMING (for
+ * an operation-count roofline): [0..3] partitioned blocks searched by the front kernel by
+ * partition count; [4] decimation modes and [5] block modes it evaluated; [6..9]
+ * candidates refined by partition count; [10..12] partition searches for P = 2, 3, 4. */
+int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16);
 
 /* Measures the device's FP32 throughput with a dependent-FMA-chain kernel (diagnostic
  * used by bench.py for the roofline denominator): TFLOP/s counting an FMA as 2 flops. */

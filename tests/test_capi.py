@@ -59,3 +59,19 @@ def test_flop_model_matches_survey():
     lib = ab.load_library()
     assert abs(flop_model.per_block(lib, 4, 4)["total"] / 1e6 - 4.29) < 0.01
     assert abs(flop_model.per_block(lib, 6, 6)["total"] / 1e6 - 9.61) < 0.01
+
+
+def test_work_counter_model_reproduces_the_per_block_model():
+    """The op-count model applied to full-search work counters equals the per-block model."""
+    from astc_implementation_b200 import flop_model
+    lib = ab.load_library()
+    for bx, by, ndm, nbm in [(4, 4, 6, 53), (6, 6, 22, 198)]:
+        w = np.zeros(16)
+        w[0], w[1:4] = 1, 4                # partitioned blocks by P
+        w[4], w[5] = ndm * 13, nbm * 13    # decimation and block modes evaluated
+        w[6], w[7:10] = 8, 32              # candidates refined by P
+        w[10:13] = 1                       # partition searches
+        f = flop_model.from_work(lib, bx, by, w)
+        pb = flop_model.per_block(lib, bx, by)
+        for k in ("search", "front", "refine"):
+            assert abs(f[k] - pb[k]) <= 1e-9 * pb[k], (bx, k)

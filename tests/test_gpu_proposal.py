@@ -115,7 +115,7 @@ def full_and_pruned(img, bx, by, net, **prune):
 def test_everything_routed_to_full_search_is_bit_exact():
     lay = proposal.Layout(4, 4)
     img = synth.make_texture(80, 52, 12)
-    full, full_sym, blocks, sym, stats = full_and_pruned(img, 4, 4, random_net(lay, 1), threshold=2.0)
+    full, full_sym, blocks, sym, stats = full_and_pruned(img, 4, 4, random_net(lay, 1), threshold=2.0, reroute_error=0.0)
     assert stats == (0, 20 * 13)
     assert np.array_equal(blocks, full) and np.array_equal(sym, full_sym)
 
@@ -129,7 +129,7 @@ def test_proposal_search_obeys_the_selection(bx, by):
     img = synth.make_texture(90, 61, 13)
     kmax, kbm, cov, thr = 6, 8, 0.999, 1e-4
     full, full_sym, blocks, sym, stats = full_and_pruned(img, bx, by, net, max_partitionings=kmax, block_modes=kbm,
-                                                         refine_candidates=4, coverage=cov, threshold=thr)
+                                                         refine_candidates=4, coverage=cov, threshold=thr, reroute_error=0.0)
     n = sym.shape[0]
     assert sum(stats) == n
     enc = ab.ASTCEncoder(device=0)
@@ -152,6 +152,50 @@ def test_proposal_search_obeys_the_selection(bx, by):
     assert n_checked > 0.9 * stats[0]
     dec = ab.decode(bx, by, 90, 61, blocks)
     assert ab.psnr(dec, img) > ab.psnr(ab.decode(bx, by, 90, 61, full), img) - 3.0
+
+
+@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
+def test_reroute_keeps_the_better_of_both_searches(bx, by):
+    """With every proposal-search block also sent to the full search, each block ends
+    with the lower of the two errors, bit-identical to the search that produced it."""
+    net = proposal.load_weights(bx, by)
+    img = synth.make_texture(96, 72, 61)
+    prune = dict(max_partitionings=2, block_modes=8, refine_candidates=2, coverage=0.9, threshold=0.0)
+    _, full_sym, _, prop_sym, stats0 = full_and_pruned(img, bx, by, net, reroute_error=0.0, **prune)
+    _, _, blocks, both_sym, stats = full_and_pruned(img, bx, by, net, reroute_error=1e-9, **prune)
+    n = full_sym.shape[0]
+    assert stats0[0] == n and stats[0] == n
+    ef, ep, eb = (s[:, 0].view(np.float32) for s in (full_sym, prop_sym, both_sym))
+    above = np.float32(1e-9 * bx * by * (65536.0 / 255.0) ** 2)  # the threshold in the search's error units
+    rer = ep > above  # blocks sent on to the full search (exactly encoded blocks are not)
+    assert stats[1] == rer.sum() and rer.mean() > 0.5
+    assert np.all(eb[~rer] == ep[~rer]) and np.array_equal(both_sym[~rer], prop_sym[~rer])
+    assert np.all(eb[rer] == np.minimum(ef, ep)[rer])
+    take_full = rer & (ef < ep)
+    assert np.array_equal(both_sym[take_full], full_sym[take_full])
+    assert np.array_equal(both_sym[rer & ~take_full], prop_sym[rer & ~take_full])
+    assert take_full.any() and (rer & ~take_full).any()
+
+
+def test_shipped_networks_beat_the_full_search():
+    """The trained networks (astc_implementation_b200/weights) with the default settings:
+    held-out textures (generator seeds 7-9, never used for training) encode at least as
+    well as with the full search, and the untrained network of the same shape does worse."""
+    for bx in (4, 6):
+        imgs = [synth.make_texture(256, 256, s) for s in (7, 8, 9)]
+        enc = ab.ASTCEncoder(device=0)
+        enc.secondaryInit(256, 256, bx, bx)
+        dec = lambda: [ab.psnr(ab.decode(bx, bx, 256, 256, enc.encode(im)), im) for im in imgs]
+        full = dec()
+        enc.set_proposal_net(proposal.load_weights(bx, bx))
+        enc.set_pruning(True)
+        trained = dec()
+        untrained_net = dict(proposal.init_weights(proposal.Layout(bx, bx), seed=3), footprint=(bx, bx))
+        enc.set_proposal_net(untrained_net)
+        untrained = dec()
+        enc.close()
+        assert np.mean(trained) >= np.mean(full) - 0.1, (bx, trained, full)
+        assert np.mean(trained) > np.mean(untrained) + 0.5, (bx, trained, untrained)
 
 
 def test_batch_with_proposal_equals_single_images():
