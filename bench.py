@@ -246,6 +246,105 @@ def run_batch(args):
     return 0
 
 
+# ---------------------------------------------------------------- combined workload
+def combined_textures(count, min_side, max_side, seed=5):
+    """`count` textures with sides log-uniform in [min_side, max_side] per axis, generator
+    seeds 5000+i (never used for training)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        w, h = (int(round(np.exp(rng.uniform(np.log(min_side), np.log(max_side))))) for _ in range(2))
+        out.append((w, h, 5000 + i))
+    return out
+
+
+def run_combined(args):
+    """Learned proposal + batched encoder against the full search on the same batches: every
+    texture with its full box-filtered mip chain (down to 1x1, built on the GPU), at 6x6 and
+    4x4, encoded as one batch per method."""
+    import torch
+    import astc_implementation_b200 as ab
+    from astc_implementation_b200 import proposal, synth
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    spec = combined_textures(args.count, args.min_side, args.max_side)
+    levels = []  # (device tensor, w, h)
+    for w, h, seed in spec:
+        d = torch.from_numpy(synth.make_texture(w, h, seed).reshape(-1)).cuda()
+        dims = ab.mip_dims(w, h)
+        levels.append((d, w, h))
+        for (pw, ph), (cw, ch) in zip(dims[:-1], dims[1:]):
+            nxt = torch.empty(cw * ch * 4, dtype=torch.uint8, device="cuda")
+            ab.downsample_device(levels[-1][0].data_ptr(), pw, ph, nxt.data_ptr(), stream.cuda_stream)
+            levels.append((nxt, cw, ch))
+    torch.cuda.synchronize()
+    desc, outs = [], []
+    for fp in (6, 4):
+        for d, w, h in levels:
+            n = ((w + fp - 1) // fp) * ((h + fp - 1) // fp)
+            o = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+            outs.append(o)
+            desc.append((d.data_ptr(), w, h, fp, fp, o.data_ptr(), n * 16))
+    texels = sum(w * h for _, w, h in levels) * 2
+
+    def timed(enc, steps):
+        enc.encode_batch_device(desc, stream.cuda_stream)  # capture
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            enc.encode_batch_device(desc, stream.cuda_stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / steps
+
+    def quality():
+        q = []
+        k = 0
+        for fp in (6, 4):
+            for d, w, h in levels:
+                img = d.cpu().numpy().reshape(h, w, 4)
+                q.append(ab.psnr(ab.decode(fp, fp, w, h, outs[k].cpu().numpy()), img))
+                k += 1
+        return np.array(q)
+
+    full = ab.ASTCEncoder(device=local)
+    ms_full = timed(full, 1)
+    q_full = quality()
+    full.close()
+    enc = ab.ASTCEncoder(device=local)
+    for fp in (4, 6):
+        enc.set_proposal_net(proposal.load_weights(fp, fp))
+    enc.set_pruning(True, **PRUNING)
+    clocks = ClockSampler(local)
+    ms = timed(enc, args.steps)
+    clk = clocks.stop()
+    routes = enc.pruning_stats()
+    q = quality()
+    enc.close()
+    finite = np.isfinite(q) & np.isfinite(q_full)
+    d = q[finite] - q_full[finite]
+    print(json.dumps({
+        "metric": "Mtexel/s, learned proposal + batched encoder vs full search (textures with mip chains)",
+        "value": round(texels / (ms / 1000.0) / 1e6, 3), "unit": "Mtexel/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": 1, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "%d textures, sides log-uniform %d-%d per axis, full box-filtered mip chains to 1x1, "
+                               "at 6x6 and 4x4, one batch per step" % (args.count, args.min_side, args.max_side),
+                   "textures_with_mips": len(levels), "texels_per_step": texels},
+        "full_search": {"value": round(texels / (ms_full / 1000.0) / 1e6, 3), "ms_per_step": round(ms_full, 3)},
+        "speedup_vs_full_search": round(ms_full / ms, 3),
+        "psnr": {"mean_delta_db": round(float(d.mean()), 3), "min_delta_db": round(float(d.min()), 3),
+                 "levels_compared": int(finite.sum()), "levels_lossless_in_both": int((~finite).sum())},
+        "routes": {"proposal_blocks": int(routes[0]), "full_search_blocks": int(routes[1])},
+        "clocks": clk,
+    }))
+    return 0
+
+
 # ---------------------------------------------------------------- B200 arm
 PRUNING = dict(max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98, threshold=0.5, reroute_error=8.0)
 CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
@@ -267,7 +366,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="texture side (default: the 2048x2048 workload)")
     ap.add_argument("--footprints", default="4x4,6x6")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "combined"])
+    ap.add_argument("--count", type=int, default=32, help="combined workload: textures (256 in the full configuration)")
+    ap.add_argument("--min-side", type=int, default=256)
+    ap.add_argument("--max-side", type=int, default=1024, help="combined workload: 4096 in the full configuration")
     ap.add_argument("--method", default="proposal", choices=["proposal", "full"],
                     help="timed method: the learned proposal search (headline) or the full search alone")
     ap.add_argument("--skip-full", action="store_true",
@@ -279,6 +381,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "combined":
+        return run_combined(args)
 
     import torch
     import astc_implementation_b200 as ab
