@@ -94,6 +94,7 @@ struct KernelArgs {
     // by P; [4] decimation modes and [5] block modes it evaluated; [6..9] candidates
     // refined, by P; [10..12] partition searches, P = 2..4.
     unsigned long long* work;
+    int front_threads;        // threads per front CTA: 128 (0 selects it), 64 or 32
 };
 constexpr int kWorkCounters = 16;
 
@@ -178,7 +179,7 @@ __device__ __forceinline__ uint4* block_dst(const KernelArgs& a, int blk) {
 #endif
 
 // Shared-memory sizes the launches need for one footprint.
-size_t front_smem_bytes(const TableLayout& L);
+size_t front_smem_bytes(const TableLayout& L, int threads = 128);
 size_t refine_smem_bytes(const TableLayout& L);
 size_t search_smem_bytes(const TableLayout& L);
 

@@ -289,8 +289,17 @@ __device__ __noinline__ void unpack_endpoints(uint32_t fmt, const uint8_t* v, ui
 }
 
 // ------------------------------------------------------------ k_refine
-constexpr int kRefinePBs = 16;
-constexpr int kRefineThreads = kRefinePBs * kNumCand;
+constexpr int kRefineThreads = 128;
+
+// Candidate threads per partitioned block (the refinement top-N rounded up to a power of
+// two) and partitioned blocks per CTA: 16 x 8 for the full search; more, narrower ones when
+// the proposal search keeps fewer candidates, capped so the staged texels stay <= 40 KB.
+__host__ __device__ inline int refine_cpb(int topn) { return topn <= 1 ? 1 : topn <= 2 ? 2 : topn <= 4 ? 4 : 8; }
+__host__ __device__ inline int refine_pbs(int T, int topn) {
+    const int by_threads = kRefineThreads / refine_cpb(topn);
+    const int by_smem = 40960 / (T * 16);
+    return by_threads < by_smem ? by_threads : (by_smem > 16 ? by_smem : 16);
+}
 
 // Per-thread candidate state in shared memory (41 words: an odd stride, so a
 // warp's threads hit distinct banks).  Endpoints live in per-thread local arrays.
@@ -546,13 +555,18 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     }
 }
 
+// CPB: candidate threads per partitioned block (refine_cpb of the launch's top-N), a
+// template parameter so that the full search's instance (8) keeps constant indexing.
+template <int CPB>
 __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int T = a.L.T;
+    constexpr int cpb = CPB;
+    const int pbs = CPB == 8 ? kRefineThreads / 8 : refine_pbs(T, CPB);
     CandSmem* cs = reinterpret_cast<CandSmem*>(smem);
     float4* pxs = reinterpret_cast<float4*>(smem + sizeof(CandSmem) * kRefineThreads);
-    uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefinePBs * T);
-    int* keys = reinterpret_cast<int*>(tps + ((kRefinePBs * T + 15) & ~15));
+    uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + pbs * T);
+    int* keys = reinterpret_cast<int*>(tps + ((pbs * T + 15) & ~15));
     float* uwc_all = reinterpret_cast<float*>(keys + kRefineThreads);
     const int tid = threadIdx.x;
     // Items: every slot of every block in slot-major order (consecutive CTAs hold
@@ -560,16 +574,16 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     // co-resident warps run the same code), or the proposal pass's work list.
     const int nb = list_blocks(a);
     const int npb = a.pb_list ? pb_total(a) : nb * a.slots;
-    const int ngroups = (npb + kRefinePBs - 1) / kRefinePBs;
+    const int ngroups = (npb + pbs - 1) / pbs;
     __shared__ unsigned int refined[4];  // candidates refined by this CTA, by P (work counters)
     if (tid < 4) refined[tid] = 0;
     for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
         int my_lb = -1, my_slot = 0;  // this thread's partitioned block in the staging order
         {
-            const int pbl = tid / kNumCand, k = tid % kNumCand;
-            const int li = grp * kRefinePBs + pbl;
+            const int pbl = tid / cpb, k = tid % cpb;
+            const int li = grp * pbs + pbl;
             int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
-            if (li < npb) {
+            if (pbl < pbs && li < npb) {
                 int slot, lb;
                 if (a.pb_list) pb_item(a, li, lb, slot);
                 else { slot = li / nb; lb = li % nb; }
@@ -580,7 +594,7 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
                     const int P = r.P;
                     const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
                     const BlockSrc src = block_src(a, chunk_block(a, lb));
-                    for (int t = k; t < T; t += kNumCand) {
+                    for (int t = k; t < T; t += cpb) {
                         pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
                         tps[pbl * T + t] = P > 1 ? prow[t] : 0;
                     }
@@ -602,8 +616,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
             __syncthreads();
             mine = keys[tid];
         }
-        const int pbl = mine / kNumCand, k = mine % kNumCand;
-        const uint32_t item = cs[pbl * kNumCand].pad;  // written by the thread that staged partitioned block pbl
+        const int pbl = mine / cpb, k = mine % cpb;
+        const uint32_t item = cs[pbl * cpb].pad;  // written by the threads that staged partitioned block pbl
         __syncthreads();  // every thread has read the item words before the candidate state overwrites them
         if (item != 0) {
             const int lb = (int)(item & 0x07FFFFFFu) - 1, slot = (int)(item >> 27);
@@ -797,9 +811,16 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
 
 }  // namespace
 
-size_t refine_smem_bytes(const TableLayout& L) {
-    return sizeof(CandSmem) * kRefineThreads + (size_t)kRefinePBs * L.T * 16 + (((size_t)kRefinePBs * L.T + 15) & ~(size_t)15) +
-           kRefineThreads * 4 + (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
+size_t refine_smem_bytes(const TableLayout& L, int topn) {
+    const size_t pbs = (size_t)refine_pbs(L.T, topn);
+    return sizeof(CandSmem) * kRefineThreads + pbs * L.T * 16 + ((pbs * L.T + 15) & ~(size_t)15) + kRefineThreads * 4 +
+           (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
+}
+
+size_t refine_smem_bytes(const TableLayout& L) {  // the largest over the refinement top-N
+    size_t m = 0;
+    for (int topn : {1, 2, 4, 8}) m = std::max(m, refine_smem_bytes(L, topn));
+    return m;
 }
 
 cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes);
@@ -822,14 +843,21 @@ cudaError_t configure_kernels(const TableLayout& L) {
     for (int i = 0; i < 3; i++) m[i] = std::max(m[i], need[i]);
     e = configure_search_kernels(m[0], m[1]);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m[2]);
+    for (auto f : {k_refine<1>, k_refine<2>, k_refine<4>, k_refine<8>})
+        if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m[2])) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
-    const int npb = a.nblocks * a.slots;
-    int grid = (npb + kRefinePBs - 1) / kRefinePBs;
+    const int cpb = refine_cpb(a.topn);
+    const int npb = a.nblocks * a.slots, pbs = refine_pbs(a.L.T, cpb);
+    int grid = (npb + pbs - 1) / pbs;
     if (a.block_list) grid = std::min(grid, kListGridRefine);
-    k_refine<<<grid, kRefineThreads, refine_smem_bytes(a.L), s>>>(a);
+    const size_t smem = refine_smem_bytes(a.L, cpb);
+    if (cpb == 1) k_refine<1><<<grid, kRefineThreads, smem, s>>>(a);
+    else if (cpb == 2) k_refine<2><<<grid, kRefineThreads, smem, s>>>(a);
+    else if (cpb == 4) k_refine<4><<<grid, kRefineThreads, smem, s>>>(a);
+    else k_refine<8><<<grid, kRefineThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -344,8 +344,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
 }
 
 // ============================================================ passes 01-12
-constexpr int kFrontThreads = 128;
-constexpr int kFrontWarps = kFrontThreads / 32;
+// One CTA of NT threads per partitioned block: 128 for the full search; the proposal
+// search, whose partitioned blocks evaluate few block modes, may use 64 or 32 so that more
+// of them are resident per SM.  Every value is computed by the same thread sequence
+// whatever NT is (loops only spread independent items), so results do not depend on it.
 
 struct FrontLayout {
     int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, dml, total;
@@ -368,7 +370,7 @@ struct FrontMisc {
 };
 
 __host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
-__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w) {
+__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w, int nt) {
     FrontLayout f;
     int o = 0;
     f.px = take16(o, T * 16);
@@ -378,13 +380,13 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.dec = take16(o, ndm * 64 * 4);
     f.lo = take16(o, ndm * 8 * 4);
     f.hi = take16(o, ndm * 8 * 4);
-    f.scratch = take16(o, kFrontWarps * kScratchPerWarp);
+    f.scratch = take16(o, (nt / 32) * kScratchPerWarp);
     f.bm_err = take16(o, nbm * 4);
     f.bm_bits = take16(o, nbm * 4);
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    f.qf = take16(o, max_w * kFrontThreads * 4);
+    f.qf = take16(o, max_w * nt * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.dml = take16(o, 16 + ndm * 2);
     f.total = o;
@@ -425,11 +427,13 @@ __device__ __forceinline__ int bm_quant_weight(const Tabs& tb, const BmQuant& s,
     return v;
 }
 
+template <int NT>
 __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, int slot_in_block, uint32_t entry, uint8_t* sm) {
+    constexpr int kFrontThreads = NT, kFrontWarps = NT / 32;
     const Tabs tb{a.tables, &a.L};
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w);
+    const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w, NT);
     float4* px = reinterpret_cast<float4*>(sm + fl.px);
     float* iw = reinterpret_cast<float*>(sm + fl.w);
     float* wes = reinterpret_cast<float*>(sm + fl.wes);
@@ -889,7 +893,8 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     }
 }
 
-__global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__ KernelArgs a) {
+template <int NT>
+__global__ void __launch_bounds__(NT) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     // Items: every slot of every block in slot-major order (co-resident CTAs work on the
     // same partition count), or the proposal pass's work list grouped by partition count.
@@ -918,7 +923,7 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__
             if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * a.slots + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
             continue;  // uniform across the CTA
         }
-        front_body(a, P, lb, blk, k, entry, smem);
+        front_body<NT>(a, P, lb, blk, k, entry, smem);
         __syncthreads();  // the next item reuses shared memory
     }
 }
@@ -926,12 +931,15 @@ __global__ void __launch_bounds__(kFrontThreads) k_front(const __grid_constant__
 }  // namespace
 
 size_t search_smem_bytes(const TableLayout&) { return (size_t)kSearchWarps * kSearchWarpBytes; }
-size_t front_smem_bytes(const TableLayout& L) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w).total; }
+size_t front_smem_bytes(const TableLayout& L, int nt) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w, nt).total; }
 
+// front_bytes: the 128-thread layout, the largest of the three.
 cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
     cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_front, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+    return e;
 }
 
 cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
@@ -943,9 +951,13 @@ cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
+    const int nt = a.front_threads == 32 || a.front_threads == 64 ? a.front_threads : 128;
     int grid = a.nblocks * a.slots;
-    if (a.block_list) grid = std::min(grid, kListGridFront);
-    k_front<<<grid, kFrontThreads, front_smem_bytes(a.L), s>>>(a);
+    if (a.block_list) grid = std::min(grid, kListGridFront * (128 / nt));
+    const size_t smem = front_smem_bytes(a.L, nt);
+    if (nt == 32) k_front<32><<<grid, 32, smem, s>>>(a);
+    else if (nt == 64) k_front<64><<<grid, 64, smem, s>>>(a);
+    else k_front<128><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -114,6 +114,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     ap.block_list = r.pruned; ap.block_count = counts;
     ap.prop = r.prop; ap.bm_mask = r.masks;
     ap.slots = 1 + pr.kmax; ap.topn = pr.topn;
+    ap.front_threads = pr.front_threads;
     ap.reroute_list = r.full; ap.reroute_count = counts + 1;  // blocks left without a candidate
     ap.pb_list = r.pb_list; ap.pb_count = counts + 2; ap.pb_stride = r.pb_stride;
     ap.reroute_err = r.full_err;
@@ -241,7 +242,8 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     if (!ctx || !cfg || cfg->struct_size < sizeof(astcb200_pruning)) return ASTCB200_BAD_ARG;
     if (cfg->enable && (cfg->max_partitionings > (uint32_t)kMaxProposals || cfg->block_modes == 0 || cfg->block_modes > 64 ||
                         cfg->refine_candidates == 0 || cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
-                        !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f)))
+                        !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f) ||
+                        (cfg->front_threads && cfg->front_threads != 32 && cfg->front_threads != 64 && cfg->front_threads != 128)))
         return ASTCB200_BAD_ARG;
     Pruning& p = ctx->pruning;
     p.enable = cfg->enable != 0;
@@ -250,7 +252,8 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.topn = (int)cfg->refine_candidates;
     p.coverage = cfg->coverage;
     p.threshold = cfg->threshold;
-    p.reroute_error = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->reroute_error : 0.0f;
+    p.reroute_error = cfg->reroute_error;
+    p.front_threads = cfg->front_threads ? (int)cfg->front_threads : 128;
     release_batches(ctx);  // captured graphs hold the previous settings
     return ASTCB200_OK;
 }

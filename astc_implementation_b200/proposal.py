@@ -102,23 +102,39 @@ def labels_from_symbolic(sym, bx, by):
     return part.astype(np.int32), np.maximum(bm, 0).astype(np.int32), usable
 
 
-def make_dataset(bx, by, seeds, side, device=0, log=print):
+def mip_down(img):
+    """Next mip level: max(1, w/2) x max(1, h/2), each texel the rounded mean (sum + 2) / 4 of
+    the 2x2 source texels, source coordinates clamped (astcb200_downsample_device's rule)."""
+    h, w = img.shape[:2]
+    dh, dw = max(1, h // 2), max(1, w // 2)
+    y0, y1 = np.minimum(2 * np.arange(dh), h - 1), np.minimum(2 * np.arange(dh) + 1, h - 1)
+    x0, x1 = np.minimum(2 * np.arange(dw), w - 1), np.minimum(2 * np.arange(dw) + 1, w - 1)
+    s = img[y0][:, x0].astype(np.int32) + img[y0][:, x1] + img[y1][:, x0] + img[y1][:, x1] + 2
+    return (s >> 2).astype(np.uint8)
+
+
+def make_dataset(bx, by, seeds, side, device=0, log=print, mips=0):
     """Inputs (n, k0p) float32 and labels of every block of side x side textures of the
-    given generator seeds, labelled by the full search on the GPU."""
+    given generator seeds and of their first `mips` mip levels, labelled by the full search
+    on the GPU."""
     from . import synth
     lay = Layout(bx, by)
     enc = ASTCEncoder(device=device)
     enc.init()
-    enc.secondaryInit(side, side, bx, by)
     xs, ps, bs = [], [], []
     t0 = time.time()
     for s in seeds:
         img = synth.make_texture(side, side, s)
-        sym = enc.encode_symbolic(img)
-        part, bm, ok = labels_from_symbolic(sym, bx, by)
-        xs.append(network_inputs(block_rgba8(img, bx, by)[ok], lay.inputs_padded))
-        ps.append(part[ok])
-        bs.append(bm[ok])
+        for level in range(mips + 1):
+            if level:
+                img = mip_down(img)
+            h, w = img.shape[:2]
+            enc.secondaryInit(w, h, bx, by)
+            sym = enc.encode_symbolic(img)
+            part, bm, ok = labels_from_symbolic(sym, bx, by)
+            xs.append(network_inputs(block_rgba8(img, bx, by)[ok], lay.inputs_padded))
+            ps.append(part[ok])
+            bs.append(bm[ok])
     enc.close()
     log("labelled %d blocks in %.1f s" % (sum(len(p) for p in ps), time.time() - t0))
     return np.concatenate(xs), np.concatenate(ps), np.concatenate(bs)
@@ -288,9 +304,10 @@ def main():
     ap = argparse.ArgumentParser(description="train the proposal network of one footprint on the GPU")
     ap.add_argument("--footprint", default="4x4")
     ap.add_argument("--blocks", type=int, default=2_000_000, help="training blocks (seeds 100-199)")
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--batch", type=int, default=2048)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--mips", type=int, default=2, help="also train on this many mip levels of each texture")
     ap.add_argument("--out", required=True)
     args = ap.parse_args()
     bx, by = (int(v) for v in args.footprint.split("x"))
@@ -298,7 +315,7 @@ def main():
     seeds = list(range(100, 200))
     per = args.blocks / len(seeds)
     side = int(np.ceil(np.sqrt(per))) * max(bx, by)  # about blocks/100 blocks per texture
-    X, part, bm = make_dataset(bx, by, seeds, side)
+    X, part, bm = make_dataset(bx, by, seeds, side, mips=args.mips)
     nval = min(65536, len(X) // 20)
     tr = Trainer(lay, init_weights(lay, seed=1), batch=args.batch, lr=args.lr)
     t0 = time.time()

@@ -327,6 +327,10 @@ def run_combined(args):
     enc.close()
     finite = np.isfinite(q) & np.isfinite(q_full)
     d = q[finite] - q_full[finite]
+    sizes = [(fp, w, h) for fp in (6, 4) for _, w, h in levels]
+    idx = np.where(finite)[0]
+    worst = [{"footprint": sizes[i][0], "size": [sizes[i][1], sizes[i][2]], "full_db": round(float(q_full[i]), 2),
+              "proposal_db": round(float(q[i]), 2)} for i in idx[np.argsort(d)[:4]]]
     print(json.dumps({
         "metric": "Mtexel/s, learned proposal + batched encoder vs full search (textures with mip chains)",
         "value": round(texels / (ms / 1000.0) / 1e6, 3), "unit": "Mtexel/s", "n_gpus": 1, "steps": args.steps,
@@ -338,7 +342,10 @@ def run_combined(args):
         "full_search": {"value": round(texels / (ms_full / 1000.0) / 1e6, 3), "ms_per_step": round(ms_full, 3)},
         "speedup_vs_full_search": round(ms_full / ms, 3),
         "psnr": {"mean_delta_db": round(float(d.mean()), 3), "min_delta_db": round(float(d.min()), 3),
-                 "levels_compared": int(finite.sum()), "levels_lossless_in_both": int((~finite).sum())},
+                 "levels_compared": int(finite.sum()),
+                 "levels_lossless_in_both": int((~np.isfinite(q) & ~np.isfinite(q_full)).sum()),
+                 "levels_lossless_full_search_only": int((np.isfinite(q) & ~np.isfinite(q_full)).sum()),
+                 "levels_lossless_proposal_only": int((~np.isfinite(q) & np.isfinite(q_full)).sum()), "worst": worst},
         "routes": {"proposal_blocks": int(routes[0]), "full_search_blocks": int(routes[1])},
         "clocks": clk,
     }))

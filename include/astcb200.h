@@ -179,6 +179,8 @@ typedef struct astcb200_pruning {
                                    (weighted squared, 8-bit units; weights R 0.675, G 1.3275,
                                    B 0.2475, A 1) also takes the full search, and the better of
                                    the two results is kept; 0 disables */
+    uint32_t front_threads;     /* threads per CTA of the proposal pass's front kernel: 32, 64 or
+                                   128 (0 = 128); results do not depend on it */
 } astcb200_pruning;
 /* Applies to later encodes of footprints that have a network (the others use the full search). */
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);
