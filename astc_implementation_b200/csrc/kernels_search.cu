@@ -833,17 +833,33 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     }
     __syncthreads();
     // ---------------- pass12: the 8 best trials (first minimum wins ties)
-    if (tid < kNumCand) M.top[tid] = -1;
-    __syncthreads();
-    for (int i = tid; i < nbm; i += kFrontThreads) {
-        const float e = ccr_tot[i];
-        if (!(e < ERR_DEFAULT)) continue;
-        int rank = 0;
-        for (int j = 0; j < nbm && rank < kNumCand; j++) {
-            const float f = ccr_tot[j];
-            if (f < ERR_DEFAULT && (f < e || (f == e && j < i))) rank++;
+    // warp 0 picks them in order: each round the (error, index)-smallest mode after the
+    // previous pick -- the order in which counting, for every mode, the modes ranked
+    // before it would place them
+    if (warp == 0) {
+        float pv = 0.0f;
+        int pi = -1;
+        for (int r = 0; r < kNumCand; r++) {
+            float be = 3.4e38f;
+            int bi = 0x7FFFFFFF;
+            for (int i = lane; i < nbm; i += 32) {
+                const float e = ccr_tot[i];
+                if (!(e < ERR_DEFAULT)) continue;
+                if (r > 0 && !(e > pv || (e == pv && i > pi))) continue;
+                if (e < be || (e == be && i < bi)) { be = e; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float oe = __shfl_xor_sync(0xFFFFFFFFu, be, o);
+                const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+                if (oe < be || (oe == be && oi < bi)) { be = oe; bi = oi; }
+            }
+            if (bi == 0x7FFFFFFF) {  // fewer than kNumCand usable modes
+                if (lane >= r && lane < kNumCand) M.top[lane] = -1;
+                break;
+            }
+            if (lane == 0) M.top[r] = bi;
+            pv = be; pi = bi;
         }
-        if (rank < kNumCand) M.top[rank] = i;
     }
     __syncthreads();
     PBRec& rec = a.pbrec[(size_t)lb * a.slots + slot_in_block];
@@ -894,7 +910,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_front(const __grid_constant__ KernelArgs a) {
+__global__ void __launch_bounds__(NT, 1024 / NT) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     // Items: every slot of every block in slot-major order (co-resident CTAs work on the
     // same partition count), or the proposal pass's work list grouped by partition count.
