@@ -597,8 +597,17 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
             for (int w = lane; w < W; w += 32) smp[w] = f2u(rintf(clampf(dw[w], 0.0f, 1.0f) * (1024.0f - 1.0f)));
             __syncwarp();
             if (lane < 16) {
+                // table values fetched four at a time, then summed in weight order
                 float ax = 0.0f, ay = 0.0f;
-                for (int j = 0; j < W; j++) { const int k = smp[j] * 16 + lane; ax = ax + tb.cos_t(k); ay = ay + tb.sin_t(k); }
+                int j = 0;
+                for (; j + 4 <= W; j += 4) {
+                    float c[4], sn[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) { const int k = smp[j + u] * 16 + lane; c[u] = tb.cos_t(k); sn[u] = tb.sin_t(k); }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) { ax = ax + c[u]; ay = ay + sn[u]; }
+                }
+                for (; j < W; j++) { const int k = smp[j] * 16 + lane; ax = ax + tb.cos_t(k); ay = ay + tb.sin_t(k); }
                 ang[lane] = atan2_search(ay, ax) * (1.0f / (2.0f * 3.14159265358979323846f));
             }
             __syncwarp();
@@ -622,32 +631,54 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
                 o[0] = minidx; o[1] = __int_as_float(span); o[2] = ev * esc; o[3] = cl * esc; o[4] = ch * esc;
             }
             __syncwarp();
-            // pass05: best angular step per weight span, low/high value per quant level
-            if (lane == 0) {
-                float be[36], bi[36], bc[36];
+            // pass05: best angular step per weight span, then low/high value per quant level.
+            // Lane x keeps spans x and x + 32 and applies, step by step in order, the updates
+            // of the sequential scan that target them, so each keeps the same first minimum.
+            {
                 const int nb = min((int)dmi.max_quant_steps + 4, 36);
-                for (int i = 0; i < nb; i++) { be[i] = 1e37f; bi[i] = -1.0f; bc[i] = 0.0f; }
+                float be0 = 1e37f, bi0 = -1.0f, bc0 = 0.0f, be1 = 1e37f, bi1 = -1.0f, bc1 = 0.0f;
+                const int x0 = lane, x1 = lane + 32;
                 for (int i = 0; i < S; i++) {
                     const float* o = lh + i * 5;
-                    const int s = __float_as_int(o[1]);
+                    const int sp = __float_as_int(o[1]);
                     const float e = o[2], cl = o[3], ch = o[4];
                     const float ecl = e + cl, ech = e + ch, eclh = (e + cl) + ch;
                     const float fi = (float)i;
-                    if (e < be[s]) { be[s] = e; bi[s] = fi; bc[s] = 0.0f; }
-                    if (ecl < be[s - 1]) { be[s - 1] = ecl; bi[s - 1] = fi; bc[s - 1] = 1.0f; }
-                    if (ech < be[s - 1]) { be[s - 1] = ech; bi[s - 1] = fi; bc[s - 1] = 0.0f; }
-                    if (eclh < be[s - 2]) { be[s - 2] = eclh; bi[s - 2] = fi; bc[s - 2] = 1.0f; }
+                    if (x0 < nb) {
+                        if (sp == x0 && e < be0) { be0 = e; bi0 = fi; bc0 = 0.0f; }
+                        if (sp - 1 == x0) {
+                            if (ecl < be0) { be0 = ecl; bi0 = fi; bc0 = 1.0f; }
+                            if (ech < be0) { be0 = ech; bi0 = fi; bc0 = 0.0f; }
+                        }
+                        if (sp - 2 == x0 && eclh < be0) { be0 = eclh; bi0 = fi; bc0 = 1.0f; }
+                    }
+                    if (x1 < nb) {
+                        if (sp == x1 && e < be1) { be1 = e; bi1 = fi; bc1 = 0.0f; }
+                        if (sp - 1 == x1) {
+                            if (ecl < be1) { be1 = ecl; bi1 = fi; bc1 = 1.0f; }
+                            if (ech < be1) { be1 = ech; bi1 = fi; bc1 = 0.0f; }
+                        }
+                        if (sp - 2 == x1 && eclh < be1) { be1 = eclh; bi1 = fi; bc1 = 1.0f; }
+                    }
                 }
-                for (int q = 0; q < 8; q++) { lov[m * 8 + q] = 0.0f; hiv[m * 8 + q] = 0.0f; }
-                for (int q = 0; q <= dmi.max_quant_level; q++) {
-                    const int qs = c_steps_for_quant[q];
-                    const int bsi = max(f2i(bi[qs]), 0);
-                    const float lwi = lh[bsi * 5] + bc[qs];
-                    const float hwi = (lwi + (float)qs) - 1.0f;
-                    const float step = 1.0f / (1.0f + (float)bsi);
-                    const float off = ang[bsi];
-                    lov[m * 8 + q] = (off + lwi) * step;
-                    hiv[m * 8 + q] = (off + hwi) * step;
+                const int q = lane;  // lanes 0..7: quant level q
+                const bool live = q < 8 && q <= (int)dmi.max_quant_level;
+                const int qs = live ? c_steps_for_quant[q] : 0;
+                const float bl = __shfl_sync(0xFFFFFFFFu, bi0, qs & 31), bh = __shfl_sync(0xFFFFFFFFu, bi1, qs & 31);
+                const float cl_ = __shfl_sync(0xFFFFFFFFu, bc0, qs & 31), ch_ = __shfl_sync(0xFFFFFFFFu, bc1, qs & 31);
+                if (q < 8) {
+                    float lo_v = 0.0f, hi_v = 0.0f;
+                    if (live) {
+                        const int bsi = max(f2i(qs < 32 ? bl : bh), 0);
+                        const float lwi = lh[bsi * 5] + (qs < 32 ? cl_ : ch_);
+                        const float hwi = (lwi + (float)qs) - 1.0f;
+                        const float step = 1.0f / (1.0f + (float)bsi);
+                        const float off = ang[bsi];
+                        lo_v = (off + lwi) * step;
+                        hi_v = (off + hwi) * step;
+                    }
+                    lov[m * 8 + q] = lo_v;
+                    hiv[m * 8 + q] = hi_v;
                 }
             }
             __syncwarp();
