@@ -386,7 +386,7 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    f.qf = take16(o, max_w * nt);  // quantised weights (0..64), one byte per weight and thread
+    f.qf = take16(o, max_w * nt * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.dml = take16(o, 16 + ndm * 2);
     f.total = o;
@@ -446,7 +446,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     float* ccr_tot = reinterpret_cast<float*>(sm + fl.ccr_tot);
     uint8_t* ccr_q = sm + fl.ccr_q;
     uint8_t* ccr_fmt = sm + fl.ccr_fmt;
-    uint8_t* qvs = sm + fl.qf;
+    float* qfs = reinterpret_cast<float*>(sm + fl.qf);
     FrontMisc& M = *reinterpret_cast<FrontMisc*>(sm + fl.misc);
     const float4 cw = chan_w();
 
@@ -696,17 +696,13 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         const DevDm dmi = tb.dm(bm.dm);
         const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
         const float* dw = dec + bm.dm * 64;
-        for (int w = 0; w < dmi.W; w++) { float qf; qvs[w * kFrontThreads + tid] = (uint8_t)bm_quant_weight(tb, s, dw[w], &qf); }
+        for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
         float err = 0.0f;
         for (int t = 0; t < T; t++) {
             const uint64_t e4 = tb.tw4(bm.dm, t);
             float v = 0.0f;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
-                const float qf = (float)qvs[(e & 0xFF) * kFrontThreads + tid] * s.rscale + s.low;  // bm_quant_weight's value
-                v = v + qf * ((float)(e >> 8) * (1.0f / 16.0f));
-            }
+            for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
             const float d = v - iw[t];
             err = err + (d * d) * wes[is_const ? 0 : t];
         }

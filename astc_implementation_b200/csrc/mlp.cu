@@ -330,67 +330,83 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
     return v;
 }
-// Warp argmax of (value, index) pairs: larger value, then smaller index.
-__device__ __forceinline__ void warp_argmax(float& v, int& i) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ov = __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        const int oi = __shfl_xor_sync(0xFFFFFFFFu, i, o);
-        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
-    }
-}
-// (value, index) strictly after (pv, pi) in the order value desc, index asc.
-__device__ __forceinline__ bool after(float v, int i, float pv, int pi) { return v < pv || (v == pv && i > pi); }
-
 __device__ __forceinline__ bool part_valid(int c, const Select& sel) {
     return c == kClassP1 || (c < kPartClasses && (c & 1023) < sel.sel[c >> 10]);
 }
 
+// Monotone map of a finite float to an unsigned key (larger value, larger key).
+__device__ __forceinline__ uint32_t okey(float v) {
+    const uint32_t u = __float_as_uint(v);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float okey_value(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k ^ 0x80000000u) : ~k);
+}
+
+// K: length of each lane's list of its best partition classes (>= kmax), so one pass over
+// the logits finds them; the warp then merges the lanes' lists with two redux steps per pick.
+template <int K>
 __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelArgs a, const __grid_constant__ Shape S,
                                                  const float* __restrict__ logits, const __grid_constant__ Select sel,
                                                  const __grid_constant__ Routes r) {
+    constexpr uint32_t kFull = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int lb = blockIdx.x * 4 + (threadIdx.x >> 5);
     if (lb >= a.nblocks) return;
     const int blk = chunk_block(a, lb);
     if (blk < 0) return;
     const float* z = logits + (size_t)lb * S.nout;
-    // softmax over the partition classes
+    // one pass: the softmax maximum and this lane's K best partitionings (value desc, index asc)
     float mx = -3.0e38f;
-    for (int c = lane; c <= kClassP1; c += 32)
-        if (part_valid(c, sel)) mx = fmaxf(mx, z[c]);
+    float lv[K];
+    int lc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) { lv[k] = -3.0e38f; lc[k] = 0x7FFFFFFF; }
+    for (int c = lane; c <= kClassP1; c += 32) {
+        if (!part_valid(c, sel)) continue;
+        const float v = z[c];
+        mx = fmaxf(mx, v);
+        if (c < kPartClasses && v > lv[K - 1]) {  // a lane sees its classes in increasing order
+            lv[K - 1] = v; lc[K - 1] = c;
+#pragma unroll
+            for (int k = K - 1; k > 0; k--)
+                if (lv[k] > lv[k - 1]) {
+                    const float tv = lv[k]; lv[k] = lv[k - 1]; lv[k - 1] = tv;
+                    const int tc = lc[k]; lc[k] = lc[k - 1]; lc[k - 1] = tc;
+                }
+        }
+    }
     mx = warp_max(mx);
     float se = 0.0f;
     for (int c = lane; c <= kClassP1; c += 32)
         if (part_valid(c, sel)) se += __expf(z[c] - mx);
     se = warp_sum(se);
     const float p1 = __expf(z[kClassP1] - mx) / se;
-    // the kmax best partitionings
+    // the kmax best partitionings, merged from the lanes' lists
     uint16_t picks[kMaxProposals];
     float mass[kMaxProposals];
-    float pv = 3.0e38f;
-    int pi = -1, n = 0;
+    int n = 0;
     float acc = p1;
     for (int k = 0; k < sel.kmax; k++) {
-        float bv = -3.0e38f;
-        int bi = 0x7FFFFFFF;
-        for (int c = lane; c < kPartClasses; c += 32) {
-            if ((c & 1023) >= sel.sel[c >> 10]) continue;
-            const float v = z[c];
-            if (after(v, c, pv, pi) && (v > bv || (v == bv && c < bi))) { bv = v; bi = c; }
+        const uint32_t key = lc[0] == 0x7FFFFFFF ? 0u : okey(lv[0]);
+        const uint32_t best = __reduce_max_sync(kFull, key);
+        if (best == 0u) break;
+        const uint32_t ci = __reduce_min_sync(kFull, key == best ? (uint32_t)lc[0] : 0xFFFFFFFFu);
+        if ((uint32_t)lc[0] == ci) {  // the winning lane drops it from its list
+#pragma unroll
+            for (int j = 0; j < K - 1; j++) { lv[j] = lv[j + 1]; lc[j] = lc[j + 1]; }
+            lv[K - 1] = -3.0e38f; lc[K - 1] = 0x7FFFFFFF;
         }
-        warp_argmax(bv, bi);
-        if (bi == 0x7FFFFFFF) break;
-        picks[n] = (uint16_t)(((bi >> 10) << 10) | (bi & 1023));
-        acc += __expf(bv - mx) / se;
+        picks[n] = (uint16_t)ci;
+        acc += __expf(okey_value(best) - mx) / se;
         mass[n] = acc;
         n++;
-        pv = bv; pi = bi;
     }
     const bool confident = acc >= sel.threshold;
     if (r.confidence && lane == 0) r.confidence[lb] = acc;
     int pos = 0;
     if (lane == 0) pos = atomicAdd(&r.counts[confident ? 0 : 1], 1);
-    pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+    pos = __shfl_sync(kFull, pos, 0);
     if (!confident) {
         if (lane == 0) { r.full[pos] = blk; r.full_err[pos] = 3e38f; }
         return;
@@ -400,6 +416,8 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     for (int k = 0; k < n; k++)
         if (mass[k] >= sel.coverage) { used = k + 1; break; }
     if (p1 >= sel.coverage) used = 0;
+    uint32_t heads = 1;  // block-mode heads the front will read: P = 1 and the proposed counts
+    for (int k = 0; k < used; k++) heads |= 2u << (picks[k] >> 10);
     if (lane == 0) {
         r.pruned[pos] = blk;
         PropPicks& pp = r.prop[pos];
@@ -412,26 +430,39 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
             r.pb_list[(size_t)p * r.pb_stride + atomicAdd(&r.counts[2 + p], 1)] = ((uint32_t)pos << 5) | (uint32_t)(k + 1);
         }
     }
-    // block-mode masks: the kbm best modes of each partition count's head
+    // block-mode masks: the kbm best modes of each needed head; lane l holds modes l + 32u
     uint64_t* mk = r.masks + (size_t)pos * 4 * kMaskWords;
     for (int p = 0; p < 4; p++) {
+        if (!((heads >> p) & 1)) continue;
         const float* h = z + kHeadBase + p * S.nbm_pad;
-        uint32_t bits[kMaskWords * 2] = {};
-        float qv = 3.0e38f;
-        int qi = -1;
-        for (int k = 0; k < sel.kbm && k < S.nbm; k++) {
-            float bv = -3.0e38f;
-            int bi = 0x7FFFFFFF;
-            for (int c = lane; c < S.nbm; c += 32) {
-                const float v = h[c];
-                if (after(v, c, qv, qi) && (v > bv || (v == bv && c < bi))) { bv = v; bi = c; }
-            }
-            warp_argmax(bv, bi);
-            if (bi == 0x7FFFFFFF) break;
-            bits[bi >> 5] |= 1u << (bi & 31);
-            qv = bv; qi = bi;
+        float hv[2 * kMaskWords];
+        uint32_t picked = 0;
+#pragma unroll
+        for (int u = 0; u < 2 * kMaskWords; u++) {
+            const int c = lane + 32 * u;
+            hv[u] = c < S.nbm ? h[c] : 0.0f;
+            if (c >= S.nbm) picked |= 1u << u;  // absent: never offered
         }
-        if (lane < kMaskWords) mk[p * kMaskWords + lane] = (uint64_t)bits[2 * lane] | ((uint64_t)bits[2 * lane + 1] << 32);
+        for (int k = 0; k < sel.kbm && k < S.nbm; k++) {
+            uint32_t key = 0;
+            int mine = -1;
+            float mv = 0.0f;
+#pragma unroll
+            for (int u = 0; u < 2 * kMaskWords; u++)
+                if (!((picked >> u) & 1) && (mine < 0 || hv[u] > mv)) { mine = u; mv = hv[u]; }
+            if (mine >= 0) key = okey(mv);
+            const uint32_t best = __reduce_max_sync(kFull, key);
+            if (best == 0u) break;
+            const uint32_t ci = __reduce_min_sync(kFull, key == best ? (uint32_t)(lane + 32 * mine) : 0xFFFFFFFFu);
+            if (mine >= 0 && (uint32_t)(lane + 32 * mine) == ci) picked |= 1u << mine;
+        }
+        uint64_t word = 0;
+#pragma unroll
+        for (int u = 0; u < 2 * kMaskWords; u++) {
+            const uint32_t chosen = __ballot_sync(kFull, ((picked >> u) & 1) && lane + 32 * u < S.nbm);
+            if (lane == (u >> 1)) word |= (uint64_t)chosen << (32 * (u & 1));
+        }
+        if (lane < kMaskWords) mk[p * kMaskWords + lane] = word;
     }
 }
 
@@ -449,7 +480,10 @@ cudaError_t launch_mlp_logits(const KernelArgs& a, const Net& net, float* logits
 
 cudaError_t launch_select(const KernelArgs& a, const Net& net, const float* logits, const Select& sel, const Routes& r,
                           cudaStream_t s) {
-    k_select<<<(a.nblocks + 3) / 4, 128, 0, s>>>(a, net.s, logits, sel, r);
+    const int grid = (a.nblocks + 3) / 4;
+    if (sel.kmax <= 4) k_select<4><<<grid, 128, 0, s>>>(a, net.s, logits, sel, r);
+    else if (sel.kmax <= 8) k_select<8><<<grid, 128, 0, s>>>(a, net.s, logits, sel, r);
+    else k_select<16><<<grid, 128, 0, s>>>(a, net.s, logits, sel, r);
     return cudaGetLastError();
 }
 
