@@ -17,7 +17,7 @@ namespace astcb200 {
 constexpr int kMaxTexels = 144;
 constexpr int kMaxWeights = 64;
 constexpr int kMaxDms = 87;
-constexpr int kMaxValidBms = 400;      // 12x12 has 339 single-plane trial modes
+constexpr int kMaxValidBms = 600;      // 12x12 has 521 single-plane trial block modes
 constexpr int kNumCand = 8;            // TUNE_MAX_TRIAL_CANDIDATES (astc.h:72)
 constexpr int kPartCandLimit = 128;    // TUNE_MAX_PARTITIONING_CANDIDATE_LIMIT (astc.h:25)
 
