@@ -50,7 +50,9 @@ struct Pruning {
     int kmax = 4, kbm = 16, topn = 2;
     float coverage = 0.98f, threshold = 0.5f;
     float reroute_error = 8.0f;
-    int front_threads = 128;  // per-texel weighted squared error (8-bit units) above which
+    int front_threads = 128;
+    int refine_iters = 3;
+    float p1_floor = 0.0f;  // per-texel weighted squared error (8-bit units) above which
                                  // a proposal-search block also takes the full search; 0: off
 };
 

@@ -20,8 +20,8 @@ constexpr int kMaskWords = 4;        // block-mode masks cover up to 256 block m
 struct PartPicks { uint16_t v[15]; uint16_t pad; };
 
 // Partitionings proposed for one block (proposal search): v[i] = (P - 2) << 10 | table entry,
-// best first; slot 1 + i of the block searches v[i].
-struct PropPicks { uint16_t n, pad; uint16_t v[kMaxProposals]; };
+// best first; slot 1 + i of the block searches v[i]; flags bit 0: slot 0 (P = 1) is not searched.
+struct PropPicks { uint16_t n, flags; uint16_t v[kMaxProposals]; };
 
 // Initial state of one refinement candidate (pass12 output).
 struct CandInit {
@@ -95,6 +95,7 @@ struct KernelArgs {
     // refined, by P; [10..12] partition searches, P = 2..4.
     unsigned long long* work;
     int front_threads;        // threads per front CTA: 128 (0 selects it), 64 or 32
+    int refine_iters;         // refinement iterations (0 selects the reference's 6)
 };
 constexpr int kWorkCounters = 16;
 

@@ -392,7 +392,8 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
         }
     };
 
-    for (int it = 0; it < 6; it++) {
+    const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
+    for (int it = 0; it < iters; it++) {
         fill_uw();
         // ---------------- pass13: least-squares endpoints from the current weights
 #pragma unroll 1
@@ -706,9 +707,10 @@ __device__ __forceinline__ int bitrev8(int p) {
 __device__ __noinline__ void select_pack_one(const KernelArgs& a, int lb, int blk) {
     float best = 1e30f;
     int win_slot = -1, win_k = 0;
-    // slots the front filled: all of them, or P=1 plus the proposed partitionings
+    // slots the front filled: all of them, or P=1 (unless skipped) plus the proposed partitionings
     const int nslots = a.prop ? 1 + (int)a.prop[lb].n : a.slots;
-    for (int s = 0; s < nslots; s++) {
+    const int s0 = a.prop && (a.prop[lb].flags & 1) ? 1 : 0;
+    for (int s = s0; s < nslots; s++) {
         const PBRec& r = a.pbrec[(size_t)lb * a.slots + s];
         const int n = r.ncand;
         for (int k = 0; k < n; k++) {

@@ -361,6 +361,7 @@ struct FrontMisc {
     uint32_t is_const, gray, calpha;
     float ece_rgb_scale[4], ece_lum[4], ece_alpha_drop[4];
     uint32_t ece_can_offset[4], ece_can_bc[4];
+    float p9[4][4];  // pass09 inputs per partition: rre, are, brgb, ba
     float cerr[4][21][4];
     uint8_t cfmt[4][21][4];
     float combo_err[21][13];
@@ -496,19 +497,22 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         iw[t] = clampf((pr - M.mn[p]) / span, 0.0f, 1.0f);
         wes[t] = M.lsq[p] * ew;
     }
-    if (tid == 0) {
-        bool ic = true;
-        for (int p = 1; p < 4; p++) ic = ic && M.lsq[p] == M.lsq[0];
-        M.is_const = ic;
-        float4 me = mk(10.0f);
-        for (int p = 0; p < 4; p++) {
-            const float4 ep = (mk(1.0f) - M.ep0[p]) / ((M.ep1[p] - M.ep0[p]) + mk(1e-9f));
-            if (ep.x > 0.5f && ep.x < me.x) me.x = ep.x;
-            if (ep.y > 0.5f && ep.y < me.y) me.y = ep.y;
-            if (ep.z > 0.5f && ep.z < me.z) me.z = ep.z;
-            if (ep.w > 0.5f && ep.w < me.w) me.w = ep.w;
+    if (warp == 0) {
+        if (tid == 0) {
+            bool ic = true;
+            for (int p = 1; p < 4; p++) ic = ic && M.lsq[p] == M.lsq[0];
+            M.is_const = ic;
         }
-        M.min_cutoff = fminf(me.x, fminf(me.y, fminf(me.z, me.w)));
+        // min_cutoff: the smallest (1 - ep0) / ((ep1 - ep0) + 1e-9) above 0.5 over partitions and
+        // channels (10 when none); lane 4p + c computes partition p, channel c, and the minimum
+        // of these values (never NaN, never 0) does not depend on the order it is taken in
+        const int pp = (lane >> 2) & 3, ch = lane & 3;
+        const float e0c = ch == 0 ? M.ep0[pp].x : ch == 1 ? M.ep0[pp].y : ch == 2 ? M.ep0[pp].z : M.ep0[pp].w;
+        const float e1c = ch == 0 ? M.ep1[pp].x : ch == 1 ? M.ep1[pp].y : ch == 2 ? M.ep1[pp].z : M.ep1[pp].w;
+        const float epc = (1.0f - e0c) / ((e1c - e0c) + 1e-9f);
+        float me = (lane < 16 && epc > 0.5f) ? epc : 10.0f;
+        for (int o = 16; o > 0; o >>= 1) me = fminf(me, __shfl_xor_sync(0xFFFFFFFFu, me, o));
+        if (lane == 0) M.min_cutoff = me;
     }
     __syncthreads();
     const bool is_const = M.is_const != 0;
@@ -752,37 +756,43 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         M.ece_rgb_scale[p] = (acc2 - acc1) * 0.7f;
         M.ece_lum[p] = (acc4 - acc1) * 3.0f;
         M.ece_alpha_drop[p] = acc0 * 3.0f;
-        // pass09: colour error per quant level and integer count
+        // pass09 inputs of this partition; the 4 x 21 cells are filled below, one per thread
         const float ps = (float)(P == 1 ? T : tb.part_count(P, entry, p));
         const float4 e0h = vmax(e0 - mk(65535.0f), mk(0.0f)), e1h = vmax(e1 - mk(65535.0f), mk(0.0f));
         const float4 e0l = vmin(e0, mk(0.0f)), e1l = vmin(e1, mk(0.0f));
         const float4 sre = ((e0l * e0l + e1l * e1l) + e0h * e0h) + e1h * e1h;
-        const float rre = (dot3(sre, cw) * 0.5f) * ps;
-        const float are = ((sre.w * cw.w) * 0.5f) * ps;
-        const float brgb = ((cw.x + cw.y) + cw.z) * ps, ba = cw.w * ps;
+        M.p9[p][0] = (dot3(sre, cw) * 0.5f) * ps;
+        M.p9[p][1] = ((sre.w * cw.w) * 0.5f) * ps;
+        M.p9[p][2] = ((cw.x + cw.y) + cw.z) * ps;
+        M.p9[p][3] = cw.w * ps;
+    }
+    __syncthreads();
+    // ---------------- pass09: colour error per partition, quant level and integer count
+    for (int c = tid; c < P * 21; c += kFrontThreads) {
+        const int p = c / 21, q = c % 21;
+        if (q < 4) {
+            for (int j = 0; j < 4; j++) M.cerr[p][q][j] = ERR_DEFAULT;
+            M.cfmt[p][q][0] = FMT_LUMINANCE; M.cfmt[p][q][1] = FMT_RGB_SCALE; M.cfmt[p][q][2] = FMT_RGB; M.cfmt[p][q][3] = FMT_RGBA;
+            continue;
+        }
+        const int i = q - 4;
+        const float rre = M.p9[p][0], are = M.p9[p][1], brgb = M.p9[p][2], ba = M.p9[p][3];
         const bool cbc = M.ece_can_bc[p] == 1, coe = M.ece_can_offset[p] == 1;
         const float bcrgba = cbc ? 0.625f : 1.0f, oergba = coe ? 0.5f : 1.0f, bcrgb = cbc ? 0.5f : 1.0f, oergb = coe ? 0.25f : 1.0f;
         const float rgbs_e = M.ece_rgb_scale[p], lum_e = M.ece_lum[p], ad_e = M.ece_alpha_drop[p];
-        for (int q = 0; q < 4; q++) {
-            for (int j = 0; j < 4; j++) M.cerr[p][q][j] = ERR_DEFAULT;
-            M.cfmt[p][q][0] = FMT_LUMINANCE; M.cfmt[p][q][1] = FMT_RGB_SCALE; M.cfmt[p][q][2] = FMT_RGB; M.cfmt[p][q][3] = FMT_RGBA;
-        }
-        for (int i = 0; i < 17; i++) {
-            const int q = i + 4;
-            const float orgba = q >= 19 ? 1.0f : oergba, orgb = q >= 19 ? 1.0f : oergb;
-            const float bq = tb.bqe(i);
-            const float qrgb = brgb * bq, qrgba = (brgb + ba) * bq;
-            M.cerr[p][q][3] = (((qrgba * bcrgba) * orgba) + rre) + are; M.cfmt[p][q][3] = FMT_RGBA;
-            const float full = (((qrgb * bcrgb) * orgb) + rre) + ad_e;
-            const float rgbsa = ((qrgba + rgbs_e) + rre) + are;
-            if (rgbsa < full) { M.cerr[p][q][2] = rgbsa; M.cfmt[p][q][2] = FMT_RGB_SCALE_ALPHA; }
-            else { M.cerr[p][q][2] = full; M.cfmt[p][q][2] = FMT_RGB; }
-            const float lrgbs = ((qrgb + rre) + ad_e) + rgbs_e;
-            const float la_e = ((qrgba + rre) + are) + lum_e;
-            if (lrgbs < la_e) { M.cerr[p][q][1] = lrgbs; M.cfmt[p][q][1] = FMT_RGB_SCALE; }
-            else { M.cerr[p][q][1] = la_e; M.cfmt[p][q][1] = FMT_LUMINANCE_ALPHA; }
-            M.cerr[p][q][0] = ((qrgb + rre) + ad_e) + lum_e; M.cfmt[p][q][0] = FMT_LUMINANCE;
-        }
+        const float orgba = q >= 19 ? 1.0f : oergba, orgb = q >= 19 ? 1.0f : oergb;
+        const float bq = tb.bqe(i);
+        const float qrgb = brgb * bq, qrgba = (brgb + ba) * bq;
+        M.cerr[p][q][3] = (((qrgba * bcrgba) * orgba) + rre) + are; M.cfmt[p][q][3] = FMT_RGBA;
+        const float full = (((qrgb * bcrgb) * orgb) + rre) + ad_e;
+        const float rgbsa = ((qrgba + rgbs_e) + rre) + are;
+        if (rgbsa < full) { M.cerr[p][q][2] = rgbsa; M.cfmt[p][q][2] = FMT_RGB_SCALE_ALPHA; }
+        else { M.cerr[p][q][2] = full; M.cfmt[p][q][2] = FMT_RGB; }
+        const float lrgbs = ((qrgb + rre) + ad_e) + rgbs_e;
+        const float la_e = ((qrgba + rre) + are) + lum_e;
+        if (lrgbs < la_e) { M.cerr[p][q][1] = lrgbs; M.cfmt[p][q][1] = FMT_RGB_SCALE; }
+        else { M.cerr[p][q][1] = la_e; M.cfmt[p][q][1] = FMT_LUMINANCE_ALPHA; }
+        M.cerr[p][q][0] = ((qrgb + rre) + ad_e) + lum_e; M.cfmt[p][q][0] = FMT_LUMINANCE;
     }
     __syncthreads();
     // ---------------- pass10: best format combination per quant level and integer total

@@ -416,15 +416,17 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     for (int k = 0; k < n; k++)
         if (mass[k] >= sel.coverage) { used = k + 1; break; }
     if (p1 >= sel.coverage) used = 0;
-    uint32_t heads = 1;  // block-mode heads the front will read: P = 1 and the proposed counts
+    const bool skip_p1 = used > 0 && p1 < sel.p1_floor;
+    uint32_t heads = skip_p1 ? 0u : 1u;  // block-mode heads the front will read: P = 1 and the proposed counts
     for (int k = 0; k < used; k++) heads |= 2u << (picks[k] >> 10);
     if (lane == 0) {
         r.pruned[pos] = blk;
         PropPicks& pp = r.prop[pos];
         pp.n = (uint16_t)used;
+        pp.flags = skip_p1 ? 1 : 0;
         for (int k = 0; k < kMaxProposals; k++) pp.v[k] = k < used ? picks[k] : 0;
         // the work list: slot 0 (P = 1) and one slot per proposed partitioning, by P
-        r.pb_list[atomicAdd(&r.counts[2], 1)] = (uint32_t)pos << 5;
+        if (!skip_p1) r.pb_list[atomicAdd(&r.counts[2], 1)] = (uint32_t)pos << 5;
         for (int k = 0; k < used; k++) {
             const int p = 1 + (picks[k] >> 10);  // list of P = 2 + (v >> 10)
             r.pb_list[(size_t)p * r.pb_stride + atomicAdd(&r.counts[2 + p], 1)] = ((uint32_t)pos << 5) | (uint32_t)(k + 1);

@@ -66,6 +66,7 @@ struct Select {
     float coverage;    // stop proposing once P=1 plus the proposed mass reaches this
     float threshold;   // the block takes the full search when P=1 plus the kmax best mass is below this
     int kbm;           // block modes per partition count in the masks (<= 64)
+    float p1_floor;    // with proposals, P = 1 is searched only when its probability reaches this
     int sel[3];        // selected table entries for P = 2, 3, 4 (valid classes)
 };
 

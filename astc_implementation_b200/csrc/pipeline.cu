@@ -97,6 +97,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     int* counts = ctx->d_counts + mlp::kRouteCounters * ctx->counts_used++;
     mlp::Select sel;
     sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
+    sel.p1_floor = pr.p1_floor;
     for (int i = 0; i < 3; i++) sel.sel[i] = (int)ft->L.count_selected[i + 1];
     mlp::Routes r;
     r.counts = counts;
@@ -115,6 +116,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     ap.prop = r.prop; ap.bm_mask = r.masks;
     ap.slots = 1 + pr.kmax; ap.topn = pr.topn;
     ap.front_threads = pr.front_threads;
+    ap.refine_iters = pr.refine_iters;
     ap.reroute_list = r.full; ap.reroute_count = counts + 1;  // blocks left without a candidate
     ap.pb_list = r.pb_list; ap.pb_count = counts + 2; ap.pb_stride = r.pb_stride;
     ap.reroute_err = r.full_err;
@@ -243,7 +245,8 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     if (cfg->enable && (cfg->max_partitionings > (uint32_t)kMaxProposals || cfg->block_modes == 0 || cfg->block_modes > 64 ||
                         cfg->refine_candidates == 0 || cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
                         !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f) ||
-                        (cfg->front_threads && cfg->front_threads != 32 && cfg->front_threads != 64 && cfg->front_threads != 128)))
+                        (cfg->front_threads && cfg->front_threads != 32 && cfg->front_threads != 64 && cfg->front_threads != 128) ||
+                        cfg->refine_iterations > 6 || !(cfg->single_partition_floor >= 0.0f)))
         return ASTCB200_BAD_ARG;
     Pruning& p = ctx->pruning;
     p.enable = cfg->enable != 0;
@@ -254,6 +257,8 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.threshold = cfg->threshold;
     p.reroute_error = cfg->reroute_error;
     p.front_threads = cfg->front_threads ? (int)cfg->front_threads : 128;
+    p.refine_iters = cfg->struct_size >= sizeof(astcb200_pruning) && cfg->refine_iterations ? (int)cfg->refine_iterations : 3;
+    p.p1_floor = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->single_partition_floor : 0.0f;
     release_batches(ctx);  // captured graphs hold the previous settings
     return ASTCB200_OK;
 }

@@ -181,6 +181,10 @@ typedef struct astcb200_pruning {
                                    the two results is kept; 0 disables */
     uint32_t front_threads;     /* threads per CTA of the proposal pass's front kernel: 32, 64 or
                                    128 (0 = 128); results do not depend on it */
+    uint32_t refine_iterations; /* refinement iterations of the proposal pass, 1..6 (0 = 3; the
+                                   reference and the full-search pass run 6) */
+    float single_partition_floor; /* blocks with proposed partitionings skip the single-partition
+                                   candidate when its probability is below this (0 = never) */
 } astcb200_pruning;
 /* Applies to later encodes of footprints that have a network (the others use the full search). */
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);

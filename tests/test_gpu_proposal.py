@@ -224,3 +224,26 @@ def test_training_on_gpu_reduces_loss():
     after = tr.accuracy(X[:4096], part[:4096], bm[:4096])
     assert losses[-1] < losses[0]
     assert after[1] > before[1] and after[2] > before[2]
+
+
+def test_pruning_settings_are_checked_and_applied():
+    """refine_iterations and single_partition_floor change only the proposal pass: a floor
+    above 1 drops the single-partition candidate of every block that has proposals."""
+    img = synth.make_texture(72, 64, 71)
+    net = proposal.load_weights(4, 4)
+    enc = ab.ASTCEncoder(device=0)
+    enc.set_proposal_net(net)
+    enc.secondaryInit(72, 64, 4, 4)
+    with pytest.raises(ab.ASTCError):
+        enc.set_pruning(True, refine_iterations=7)
+    with pytest.raises(ab.ASTCError):
+        enc.set_pruning(True, front_threads=48)
+    enc.set_pruning(True, max_partitionings=4, coverage=1.01, threshold=0.0, reroute_error=0.0, single_partition_floor=2.0)
+    sym = enc.encode_symbolic(img)
+    stats = enc.pruning_stats()
+    enc.close()
+    # coverage above 1 proposes all 4 partitionings for every block, so no block keeps P = 1
+    # unless the proposal search found nothing and handed it to the full search
+    n = sym.shape[0]
+    assert stats[0] == n
+    assert (sym[:, 2] > 1).sum() >= n - stats[1]
