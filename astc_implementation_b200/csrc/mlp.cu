@@ -1,7 +1,8 @@
 // Learned proposal: network inference on the tcgen05 tensor cores and the
 // selection of partitionings, block modes and routes from its logits.
 //
-// k_mlp_logits: one CTA of 4 warps per 128 blocks.  The block texels are
+// k_mlp_logits: one CTA of 8 warps per 128 blocks (two threads per block row,
+// each taking half of a row's accumulator columns).  The block texels are
 // staged in shared memory as bf16 in the tensor core's K-major core-matrix
 // layout; each layer is a chain of tcgen05.mma (M=128, K=16 per instruction,
 // A and B from shared memory, FP32 accumulators in tensor memory) issued by
@@ -9,11 +10,15 @@
 // mbarrier) already laid out on the host in the same core-matrix order.  The
 // two hidden layers' epilogues (bias, ReLU, bf16) read the accumulators with
 // tcgen05.ld and write the next layer's A operand in place; layer 3 runs in
-// 128-column chunks with double-buffered weights and accumulators, so the
-// epilogue of chunk j (bias, FP32 logits to global memory) overlaps the MMAs
-// of chunk j+1 and the copy of chunk j+2.  Every wait on an mbarrier is
-// bounded; a CTA that gives up sets *error_flag, waits (bounded) for its own
-// copies and MMAs in flight, frees its tensor memory and returns.
+// 64-column chunks with double-buffered weights and accumulators, so the
+// epilogue of chunk j overlaps the MMAs of chunk j+1 and the copy of chunk
+// j+2.  The layer-3 epilogue adds the bias, stages each row's 64 FP32 logits
+// in shared memory and writes the row with one 256-byte bulk copy to global
+// memory (instead of 64 strided stores per thread); CTAs start the chunk
+// sequence at different chunks so that they do not all fetch the same weights
+// from L2 at once.  Every wait on an mbarrier is bounded; a CTA that gives up
+// sets *error_flag, waits (bounded) for its own copies and MMAs in flight,
+// frees its tensor memory and returns.
 //
 // k_select: one warp per block turns the logits into the proposal search's
 // inputs: a softmax over the partition classes, the best partitionings (in
@@ -29,8 +34,13 @@ namespace mlp {
 namespace {
 
 constexpr uint32_t kOffA = 0;                 // 64 KB: X, then H1, then H2 (128 rows x up to 256 bf16)
-constexpr uint32_t kOffW = 65536;             // 128 KB: W1 | W2 | two W3 chunks of 64 KB
-constexpr uint32_t kOffBar = 65536 + 131072;  // mbarriers and flags
+constexpr uint32_t kOffW = 65536;             // 128 KB: W1 | W2 | two W3 chunks of 32 KB
+constexpr uint32_t kW3Buf = kChunkN * 256 * 2;               // one W3 chunk (bf16)
+constexpr uint32_t kStageStride = kChunkN + 4;                // floats per staged logit row (padded)
+constexpr uint32_t kStageBuf = kTileRows * kStageStride * 4;  // one staged chunk of logits
+constexpr uint32_t kOffStage = kOffW + 2 * kW3Buf;            // two staging buffers (free after layer 2)
+constexpr uint32_t kOffBar = kOffStage + 2 * kStageBuf;       // mbarriers and flags
+static_assert(kOffBar == 200704 && kOffBar + 1024 + 1024 <= (uint32_t)kMlpSmemBytes, "shared memory plan");
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kWaitLimit = 1u << 24;     // polls of an mbarrier before a CTA gives up
 constexpr uint32_t kCopyPiece = 32768;        // bytes per bulk copy instruction
@@ -125,10 +135,11 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
                       bf16_bits(v[4]) | (bf16_bits(v[5]) << 16), bf16_bits(v[6]) | (bf16_bits(v[7]) << 16));
 }
 
-// Hidden-layer epilogue: accumulator columns [col0, col0+256) of this thread's
-// row -> bias, ReLU, bf16 -> the A operand (128 rows x 256) for the next layer.
-__device__ void hidden_epilogue(uint32_t tmem_row, uint32_t col0, const float* __restrict__ bias, uint8_t* sA, int m) {
-    for (int c = 0; c < 256; c += 32) {
+// Hidden-layer epilogue: accumulator columns [col0 + c0, col0 + c0 + 128) of this thread's
+// row (c0: its half of the 256) -> bias, ReLU, bf16 -> the A operand (128 rows x 256) of the
+// next layer.
+__device__ void hidden_epilogue(uint32_t tmem_row, uint32_t col0, int c0, const float* __restrict__ bias, uint8_t* sA, int m) {
+    for (int c = c0; c < c0 + 128; c += 32) {
         float v[32];
         tmem_load32(tmem_row + col0 + c, v);
 #pragma unroll
@@ -141,7 +152,9 @@ __device__ void hidden_epilogue(uint32_t tmem_row, uint32_t col0, const float* _
     }
 }
 
-__global__ void __launch_bounds__(kTileRows, 1)
+constexpr int kMlpThreads = 2 * kTileRows;  // two threads per row, each taking half of the columns
+
+__global__ void __launch_bounds__(kMlpThreads, 1)
     k_mlp_logits(const __grid_constant__ KernelArgs a, const __grid_constant__ Net net, float* __restrict__ logits, int* error_flag) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -152,10 +165,16 @@ __global__ void __launch_bounds__(kTileRows, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bw + 5);
     int* abort_flag = reinterpret_cast<int*>(bw + 6);
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int m = tid;  // this thread's row (block) in the tile and tensor-memory lane
+    // this thread's row (block) in the tile and tensor-memory lane; warps w and w + 4 share
+    // the lanes of quarter w and split the columns (half)
+    const int m = tid % kTileRows, half = tid / kTileRows;
     const int lb = blockIdx.x * kTileRows + m;
     const Shape& S = net.s;
     const int nchunks = S.nout / kChunkN;
+    // CTAs walk the layer-3 chunks from different starting points, so that at any moment they
+    // read different parts of the weights from L2 instead of all the same chunk
+    const int j0 = blockIdx.x % nchunks;
+    auto chunk_of = [&](int j) { const int c = j0 + j; return c < nchunks ? c : c - nchunks; };
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols)
@@ -171,7 +190,7 @@ __global__ void __launch_bounds__(kTileRows, 1)
     __syncthreads();
     tc_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
 
     // thread 0's bookkeeping of weight copies and MMA commits in flight
     uint32_t w_issued[2] = {0, 0}, w_done[2] = {0, 0};
@@ -186,7 +205,7 @@ __global__ void __launch_bounds__(kTileRows, 1)
         const int T = a.L.T;
         BlockSrc src{};
         if (blk >= 0) src = block_src(a, blk);
-        for (int j = 0; j < S.k0p / 8; j++) {
+        for (int j = half; j < S.k0p / 8; j += 2) {
             float v[8];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
@@ -204,7 +223,7 @@ __global__ void __launch_bounds__(kTileRows, 1)
     __syncthreads();
 
     const uint32_t a_base = smem_u32(sA), w_base = smem_u32(sW);
-    constexpr uint32_t kLboA = (kTileRows / 8) * 128, kLboW256 = (256 / 8) * 128, kLboW128 = (kChunkN / 8) * 128;
+    constexpr uint32_t kLboA = (kTileRows / 8) * 128, kLboW256 = (256 / 8) * 128, kLboW3 = (kChunkN / 8) * 128;
 
     // ---- layer 1: X (128 x k0p) . W1^T -> tensor memory columns [0, 256)
     if (tid == 0) {
@@ -225,7 +244,7 @@ __global__ void __launch_bounds__(kTileRows, 1)
     if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
     tc_after();
     if (tid == 0) { load_weights(sW, net.w2, 256u * 256u * 2, &bw[0]); w_issued[0]++; }
-    hidden_epilogue(tmem_row, 0, net.b1, sA, m);
+    hidden_epilogue(tmem_row, 0, half * 128, net.b1, sA, m);
     async_proxy_fence();
     tc_before();
     __syncthreads();
@@ -250,11 +269,11 @@ __global__ void __launch_bounds__(kTileRows, 1)
     tc_after();
     if (tid == 0) {
         for (int j = 0; j < 2 && j < nchunks; j++) {
-            load_weights(sW + j * 65536, net.w3 + (size_t)j * kChunkN * 256, kChunkN * 256 * 2, &bw[j]);
+            load_weights(sW + j * kW3Buf, net.w3 + (size_t)chunk_of(j) * kChunkN * 256, kW3Buf, &bw[j]);
             w_issued[j]++;
         }
     }
-    hidden_epilogue(tmem_row, 256, net.b2, sA, m);
+    hidden_epilogue(tmem_row, 256, half * 128, net.b2, sA, m);
     async_proxy_fence();
     tc_before();
     __syncthreads();
@@ -270,7 +289,7 @@ __global__ void __launch_bounds__(kTileRows, 1)
                 if (!mbar_wait(&bw[bb], (w_done[bb]++) & 1)) { *abort_flag = 1; break; }
                 for (int kk = 0; kk < 16; kk++)
                     mma_bf16(tmem + bb * kChunkN, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
-                             smem_desc(w_base + bb * 65536 + kk * 2 * kLboW128, kLboW128, 128), instr_desc(128, kChunkN), kk > 0);
+                             smem_desc(w_base + bb * kW3Buf + kk * 2 * kLboW3, kLboW3, 128), instr_desc(128, kChunkN), kk > 0);
                 mma_commit(&bm[1 + bb]);
                 m_issued[1 + bb]++;
             }
@@ -282,27 +301,43 @@ __global__ void __launch_bounds__(kTileRows, 1)
         if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
         tc_after();
         if (tid == 0 && j + 2 < nchunks) {
-            load_weights(sW + b * 65536, net.w3 + (size_t)(j + 2) * kChunkN * 256, kChunkN * 256 * 2, &bw[b]);
+            load_weights(sW + b * kW3Buf, net.w3 + (size_t)chunk_of(j + 2) * kChunkN * 256, kW3Buf, &bw[b]);
             w_issued[b]++;
         }
+        // the row's 64 logits go to padded shared memory (32 from each of its two threads),
+        // then to global memory as one contiguous 256-byte bulk copy issued by the row's first
+        // thread (a warp's direct stores would touch 32 rows)
         const bool store = lb < a.nblocks;
-        float* out = logits + (size_t)lb * S.nout + j * kChunkN;
-        const float* bias = net.b3 + j * kChunkN;
-        for (int c = 0; c < kChunkN; c += 32) {
+        float* st = reinterpret_cast<float*>(sm + kOffStage + b * kStageBuf) + m * kStageStride;
+        {
+            const int c = half * 32;
+            const float* bias = net.b3 + chunk_of(j) * kChunkN + c;
             float v[32];
             tmem_load32(tmem_row + b * kChunkN + c, v);
-            if (store) {
 #pragma unroll
-                for (int q = 0; q < 8; q++)
-                    reinterpret_cast<float4*>(out + c)[q] = make_float4(v[4 * q] + __ldg(bias + c + 4 * q), v[4 * q + 1] + __ldg(bias + c + 4 * q + 1),
-                                                                        v[4 * q + 2] + __ldg(bias + c + 4 * q + 2), v[4 * q + 3] + __ldg(bias + c + 4 * q + 3));
-            }
+            for (int q = 0; q < 8; q++)
+                reinterpret_cast<float4*>(st + c)[q] = make_float4(v[4 * q] + __ldg(bias + 4 * q), v[4 * q + 1] + __ldg(bias + 4 * q + 1),
+                                                                   v[4 * q + 2] + __ldg(bias + 4 * q + 2), v[4 * q + 3] + __ldg(bias + 4 * q + 3));
         }
+        async_proxy_fence();
         tc_before();
-        __syncthreads();
+        __syncthreads();  // the row is staged; every read of this accumulator buffer is done
+        if (half == 0) {
+            if (store) {
+                float* out = logits + (size_t)lb * S.nout + chunk_of(j) * kChunkN;
+                asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(out), "r"(smem_u32(st)),
+                             "r"(kChunkN * 4)
+                             : "memory");
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            }
+            // the other buffer, written next, must have been read by its copy (chunk j - 1);
+            // the barrier at the top of the next iteration orders this before those writes
+            asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        }
     }
 
 cleanup:
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this thread's logit rows are written
     __syncthreads();
     if (failed) {
         // give up: record it, then let our own copies and MMAs drain (bounded) before the
@@ -476,7 +511,7 @@ cudaError_t configure_mlp() {
 
 cudaError_t launch_mlp_logits(const KernelArgs& a, const Net& net, float* logits, int* error_flag, cudaStream_t s) {
     const int grid = (a.nblocks + kTileRows - 1) / kTileRows;
-    k_mlp_logits<<<grid, kTileRows, kMlpSmemBytes, s>>>(a, net, logits, error_flag);
+    k_mlp_logits<<<grid, kMlpThreads, kMlpSmemBytes, s>>>(a, net, logits, error_flag);
     return cudaGetLastError();
 }
 

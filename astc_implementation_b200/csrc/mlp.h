@@ -23,12 +23,13 @@ constexpr int kPartClasses = 3072;
 constexpr int kClassP1 = 3072;
 constexpr int kHeadBase = 3200;
 constexpr int kTileRows = 128;   // blocks per CTA of the inference kernel
-constexpr int kChunkN = 128;     // output columns per layer-3 MMA chunk
+constexpr int kChunkN = 64;      // output columns per layer-3 MMA chunk
+constexpr int kOutAlign = 128;   // outputs are padded to a multiple of this
 
 struct Shape {
     int k0, k0p;        // inputs (4 * texels) and padded to a multiple of 16
     int nbm, nbm_pad;   // block-mode classes per head and the head stride
-    int nout;           // outputs, padded to a multiple of 128
+    int nout;           // outputs, padded to a multiple of kOutAlign
 };
 
 inline Shape shape_for(int texels, int nbm) {
@@ -37,7 +38,7 @@ inline Shape shape_for(int texels, int nbm) {
     s.k0p = (s.k0 + 15) & ~15;
     s.nbm = nbm;
     s.nbm_pad = (nbm + 31) & ~31;
-    s.nout = (kHeadBase + 4 * s.nbm_pad + kChunkN - 1) / kChunkN * kChunkN;
+    s.nout = (kHeadBase + 4 * s.nbm_pad + kOutAlign - 1) / kOutAlign * kOutAlign;
     return s;
 }
 
@@ -49,7 +50,7 @@ __host__ __device__ inline uint32_t core_index(uint32_t n, uint32_t k, uint32_t 
 }
 
 // Device copy of one footprint's network (weights bf16 in core_index order;
-// layer 3 as nout/128 chunks of 128 rows, each in its own core_index order).
+// layer 3 as nout/kChunkN chunks of kChunkN rows, each in its own core_index order).
 struct Net {
     const uint16_t* w1;   // [256 x k0p]
     const uint16_t* w2;   // [256 x 256]
@@ -86,7 +87,7 @@ struct Routes {
 
 constexpr int kRouteCounters = 8;  // ints per chunk: routes, then partitioned-block counts, padding
 
-constexpr int kMlpSmemBytes = 65536 + 131072 + 1024 + 1024;
+constexpr int kMlpSmemBytes = 200704 + 1024 + 1024;  // operands and staging, barriers, alignment slack
 
 cudaError_t configure_mlp();
 // logits[lb * nout + c] for the chunk's blocks lb < a.nblocks (addressing as for the search kernels)
