@@ -359,9 +359,11 @@ struct FrontMisc {
     float mn[4], mx[4], lsq[4];
     float min_cutoff;
     uint32_t is_const, gray, calpha;
-    float ece_rgb_scale[4], ece_lum[4], ece_alpha_drop[4];
     uint32_t ece_can_offset[4], ece_can_bc[4];
     float p9[4][4];  // pass09 inputs per partition: rre, are, brgb, ba
+    float sxyz[4][3][4];  // pass08: per partition, sums of the deviations along r, g, b (w = 0)
+    float acc[4][5];      // pass08: per partition, the five encoding-choice error sums
+    float4 axes[4][4];    // pass08: per partition, ub, ua, sb, la
     float cerr[4][21][4];
     uint8_t cfmt[4][21][4];
     float combo_err[21][13];
@@ -387,7 +389,9 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    f.qf = take16(o, max_w * nt * 4);
+    // pass07's quantised weights; before pass02 the same bytes hold the texel channels and
+    // projections (5 x T rounded up to 4, floats) and then pass08's error terms (5 x that)
+    f.qf = take16(o, (max_w * nt > 5 * ((T + 3) & ~3) ? max_w * nt : 5 * ((T + 3) & ~3)) * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.dml = take16(o, 16 + ndm * 2);
     f.total = o;
@@ -451,93 +455,262 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     FrontMisc& M = *reinterpret_cast<FrontMisc*>(sm + fl.misc);
     const float4 cw = chan_w();
 
+    // Per-partition sums over the texels are taken in ascending texel order, as the
+    // oracle does, by one lane per (partition, channel or term) over the whole block:
+    // texels of other partitions add +0.0f.  Every such sum starts at +0.0f and adds
+    // terms that are never -0.0f, so it is never -0.0f and adding +0.0f leaves it
+    // unchanged: the result is the member-only sum.  The lanes read four texels per
+    // step (the block padded to Tp texels whose partition byte matches none).
+    const int Tp = (T + 3) & ~3;
+    float* pxc = qfs;           // [4][Tp] texel channels, until pass01 ends
+    float* prj = qfs + 4 * Tp;  // [Tp] projections on the partition's direction, until iw is set
+    float* terms = qfs;         // [5][Tp] pass08 error terms, until they are summed
+    // Side work goes to the other warps first (role 0 is warp 1's lane 0); warp 0 takes
+    // pass01's chain.  With one warp, roles are its lanes.
+    const int role = (tid + kFrontThreads - 32) % kFrontThreads;
+
     const uint8_t* prow = P > 1 ? tb.part_texels(P, entry) : nullptr;
     const BlockSrc src = block_src(a, blk);
-    for (int t = tid; t < T; t += kFrontThreads) {
-        px[t] = src_texel(src, a.L.bx, t);
-        tp[t] = P > 1 ? prow[t] : 0;
+    for (int t = tid; t < Tp; t += kFrontThreads) {
+        float4 v = mk(0.0f);
+        uint8_t q = 0xFF;
+        if (t < T) { v = src_texel(src, a.L.bx, t); q = P > 1 ? prow[t] : 0; px[t] = v; }
+        pxc[t] = v.x; pxc[Tp + t] = v.y; pxc[2 * Tp + t] = v.z; pxc[3 * Tp + t] = v.w;
+        tp[t] = q;
     }
     __syncthreads();
-    {
-        bool gray = true, same_a = true;
-        for (int t = tid; t < T; t += kFrontThreads) {
-            gray = gray && px[t].x == px[t].y && px[t].x == px[t].z;
-            same_a = same_a && px[t].w == px[0].w;
-        }
-        gray = __syncthreads_and(gray);
-        same_a = __syncthreads_and(same_a);
-        if (tid == 0) { M.gray = gray; M.calpha = same_a; }
-    }
     // ---------------- pass01: per-partition average, direction, projections
-    if (tid < 4) {
-        const int p = tid;
-        float4 sum = mk(0.0f);
-        float cnt = 0.0f;
-        for (int t = 0; t < T; t++) if (tp[t] == p) { sum = sum + px[t]; cnt = cnt + 1.0f; }
-        const float4 avg = cnt > 0.0f ? sum / mk(cnt) : mk(0.0f);
-        float4 d = mk(0.0f);
-        for (int t = 0; t < T; t++) if (tp[t] == p) { const float4 pd = vmax(px[t] - avg, mk(0.0f)); d = d + pd * pd; }
-        d = normalize4(d);
+    // lane 4p + c of warp 0 takes partition p, channel c (lanes 16-31 repeat 0-15); all four
+    // partitions are computed whatever P is (empty ones feed is_const and min_cutoff)
+    const int gp = (lane >> 2) & 3, gc = lane & 3;
+    float avg_c = 0.0f;
+    if (warp == 0) {
+        const float* v = pxc + gc * Tp;
+        float s = 0.0f;
+        int n = 0;
+        for (int t = 0; t < Tp; t += 4) {
+            const float4 x = *reinterpret_cast<const float4*>(v + t);
+            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const bool m0 = (int)(q & 0xFF) == gp, m1 = (int)((q >> 8) & 0xFF) == gp;
+            const bool m2 = (int)((q >> 16) & 0xFF) == gp, m3 = (int)(q >> 24) == gp;
+            s = s + (m0 ? x.x : 0.0f); s = s + (m1 ? x.y : 0.0f);
+            s = s + (m2 ? x.z : 0.0f); s = s + (m3 ? x.w : 0.0f);
+            n += (int)m0 + (int)m1 + (int)m2 + (int)m3;
+        }
+        const float cnt = (float)n;  // the oracle's count of 1.0f additions, exact
+        avg_c = cnt > 0.0f ? s / cnt : 0.0f;
+        if (lane < 16) reinterpret_cast<float*>(&M.avg[gp])[gc] = avg_c;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const float* v = pxc + gc * Tp;
+        float dd = 0.0f;
+        for (int t = 0; t < Tp; t += 4) {
+            const float4 x = *reinterpret_cast<const float4*>(v + t);
+            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const float p0 = fmaxf(x.x - avg_c, 0.0f), p1 = fmaxf(x.y - avg_c, 0.0f);
+            const float p2 = fmaxf(x.z - avg_c, 0.0f), p3 = fmaxf(x.w - avg_c, 0.0f);
+            dd = dd + ((int)(q & 0xFF) == gp ? p0 * p0 : 0.0f);
+            dd = dd + ((int)((q >> 8) & 0xFF) == gp ? p1 * p1 : 0.0f);
+            dd = dd + ((int)((q >> 16) & 0xFF) == gp ? p2 * p2 : 0.0f);
+            dd = dd + ((int)(q >> 24) == gp ? p3 * p3 : 0.0f);
+        }
+        const int g0 = lane & ~3;
+        const float4 avg = make_float4(__shfl_sync(FULL, avg_c, g0), __shfl_sync(FULL, avg_c, g0 + 1),
+                                       __shfl_sync(FULL, avg_c, g0 + 2), __shfl_sync(FULL, avg_c, g0 + 3));
+        const float4 d = normalize4(make_float4(__shfl_sync(FULL, dd, g0), __shfl_sync(FULL, dd, g0 + 1),
+                                                __shfl_sync(FULL, dd, g0 + 2), __shfl_sync(FULL, dd, g0 + 3)));
+        if (lane < 16 && gc == 0) M.dir[gp] = d;
+        __syncwarp();
+        for (int t = lane; t < Tp; t += 32) {
+            float pr = 0.0f;
+            if (t < T) { const int p = tp[t]; pr = dot4(px[t] - M.avg[p], M.dir[p]); }
+            prj[t] = pr;
+        }
+        __syncwarp();
+        // range of the projections, taken in texel order as the oracle does
         float mn = 1e10f, mx = -1e10f;
-        for (int t = 0; t < T; t++) if (tp[t] == p) { const float pr = dot4(px[t] - avg, d); mn = fminf(mn, pr); mx = fmaxf(mx, pr); }
+        for (int t = 0; t < Tp; t += 4) {
+            const float4 x = *reinterpret_cast<const float4*>(prj + t);
+            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            if ((int)(q & 0xFF) == gp) { mn = fminf(mn, x.x); mx = fmaxf(mx, x.x); }
+            if ((int)((q >> 8) & 0xFF) == gp) { mn = fminf(mn, x.y); mx = fmaxf(mx, x.y); }
+            if ((int)((q >> 16) & 0xFF) == gp) { mn = fminf(mn, x.z); mx = fmaxf(mx, x.z); }
+            if ((int)(q >> 24) == gp) { mn = fminf(mn, x.w); mx = fmaxf(mx, x.w); }
+        }
         if (mn >= mx) { mn = 0.0f; mx = 1e-7f; }
         const float len = mx - mn;
-        M.lsq[p] = len * len;
-        M.mn[p] = mn; M.mx[p] = mx;
-        M.avg[p] = avg; M.dir[p] = d;
-        if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f && d.w == 0.0f) { M.ep0[p] = avg; M.ep1[p] = avg; }
-        else { M.ep0[p] = avg + d * mn; M.ep1[p] = avg + d * mx; }
-    }
-    __syncthreads();
-    const float ew = (((cw.x + cw.y) + cw.z) + cw.w) / 4.0f;
-    for (int t = tid; t < T; t += kFrontThreads) {
-        const int p = tp[t];
-        const float pr = dot4(px[t] - M.avg[p], M.dir[p]);
-        const float span = fmaxf(M.mx[p] - M.mn[p], 1e-6f);
-        iw[t] = clampf((pr - M.mn[p]) / span, 0.0f, 1.0f);
-        wes[t] = M.lsq[p] * ew;
-    }
-    if (warp == 0) {
-        if (tid == 0) {
-            bool ic = true;
-            for (int p = 1; p < 4; p++) ic = ic && M.lsq[p] == M.lsq[0];
-            M.is_const = ic;
-        }
+        const float lsq = len * len;
+        float4 e0 = avg, e1 = avg;
+        if (!(d.x == 0.0f && d.y == 0.0f && d.z == 0.0f && d.w == 0.0f)) { e0 = avg + d * mn; e1 = avg + d * mx; }
+        if (lane < 16 && gc == 0) { M.lsq[gp] = lsq; M.mn[gp] = mn; M.mx[gp] = mx; M.ep0[gp] = e0; M.ep1[gp] = e1; }
         // min_cutoff: the smallest (1 - ep0) / ((ep1 - ep0) + 1e-9) above 0.5 over partitions and
         // channels (10 when none); lane 4p + c computes partition p, channel c, and the minimum
         // of these values (never NaN, never 0) does not depend on the order it is taken in
-        const int pp = (lane >> 2) & 3, ch = lane & 3;
-        const float e0c = ch == 0 ? M.ep0[pp].x : ch == 1 ? M.ep0[pp].y : ch == 2 ? M.ep0[pp].z : M.ep0[pp].w;
-        const float e1c = ch == 0 ? M.ep1[pp].x : ch == 1 ? M.ep1[pp].y : ch == 2 ? M.ep1[pp].z : M.ep1[pp].w;
+        const float e0c = comp(e0, gc), e1c = comp(e1, gc);
         const float epc = (1.0f - e0c) / ((e1c - e0c) + 1e-9f);
         float me = (lane < 16 && epc > 0.5f) ? epc : 10.0f;
-        for (int o = 16; o > 0; o >>= 1) me = fminf(me, __shfl_xor_sync(0xFFFFFFFFu, me, o));
-        if (lane == 0) M.min_cutoff = me;
+        for (int o = 16; o > 0; o >>= 1) me = fminf(me, __shfl_xor_sync(FULL, me, o));
+        const float l1 = __shfl_sync(FULL, lsq, 4), l2 = __shfl_sync(FULL, lsq, 8), l3 = __shfl_sync(FULL, lsq, 12);
+        if (lane == 0) { M.min_cutoff = me; M.is_const = (l1 == lsq && l2 == lsq && l3 == lsq) ? 1u : 0u; }
+    }
+    // pass08, first part (needs only the averages): role 9p + 3s + c sums channel c of the
+    // deviations from the average over the texels of partition p whose channel s is above it
+    for (int v = role; v < 9 * P; v += kFrontThreads) {
+        const int p = v / 9, s = (v / 3) % 3, c = v % 3;
+        const float as = comp(M.avg[p], s), ac = comp(M.avg[p], c);
+        const float* xs = pxc + s * Tp;
+        const float* xc = pxc + c * Tp;
+        float sum = 0.0f;
+        for (int t = 0; t < Tp; t += 4) {
+            const float4 vs = *reinterpret_cast<const float4*>(xs + t), vc = *reinterpret_cast<const float4*>(xc + t);
+            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            sum = sum + (((int)(q & 0xFF) == p && vs.x - as > 0.0f) ? vc.x - ac : 0.0f);
+            sum = sum + (((int)((q >> 8) & 0xFF) == p && vs.y - as > 0.0f) ? vc.y - ac : 0.0f);
+            sum = sum + (((int)((q >> 16) & 0xFF) == p && vs.z - as > 0.0f) ? vc.z - ac : 0.0f);
+            sum = sum + (((int)(q >> 24) == p && vs.w - as > 0.0f) ? vc.w - ac : 0.0f);
+        }
+        M.sxyz[p][s][c] = sum;
+    }
+    if (warp == kFrontWarps - 1) {
+        bool gray = true, same_a = true;
+        for (int t = lane; t < T; t += 32) {
+            gray = gray && px[t].x == px[t].y && px[t].x == px[t].z;
+            same_a = same_a && px[t].w == px[0].w;
+        }
+        gray = __all_sync(FULL, gray);
+        same_a = __all_sync(FULL, same_a);
+        if (lane == 0) { M.gray = gray; M.calpha = same_a; }
     }
     __syncthreads();
     const bool is_const = M.is_const != 0;
+    const float ew = (((cw.x + cw.y) + cw.z) + cw.w) / 4.0f;
+    for (int t = tid; t < T; t += kFrontThreads) {
+        const int p = tp[t];
+        const float span = fmaxf(M.mx[p] - M.mn[p], 1e-6f);
+        iw[t] = clampf((prj[t] - M.mn[p]) / span, 0.0f, 1.0f);
+        wes[t] = M.lsq[p] * ew;
+    }
+    // pass08, second part: the encoding-choice axes of partition p (role p)
+    for (int p = role; p < P; p += kFrontThreads) {
+        const float4 sx = make_float4(M.sxyz[p][0][0], M.sxyz[p][0][1], M.sxyz[p][0][2], 0.0f);
+        const float4 sy = make_float4(M.sxyz[p][1][0], M.sxyz[p][1][1], M.sxyz[p][1][2], 0.0f);
+        const float4 sz = make_float4(M.sxyz[p][2][0], M.sxyz[p][2][1], M.sxyz[p][2][2], 0.0f);
+        const float pxx = dot4(sx, sx), pyy = dot4(sy, sy), pzz = dot4(sz, sz);
+        float4 bv = sx; float bs = pxx;
+        if (pyy > bs) { bv = sy; bs = pyy; }
+        if (pzz > bs) { bv = sz; bs = pzz; }
+        float4 avg = M.avg[p]; avg.w = 0.0f;
+        const float4 ub = normalize4(bv);
+        const float4 lbv = normalize4(make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+        M.axes[p][0] = ub;
+        M.axes[p][1] = avg - ub * dot4(avg, ub);
+        M.axes[p][2] = normalize4(avg);
+        M.axes[p][3] = avg - lbv * dot4(avg, lbv);
+        const float4 e0 = M.ep0[p], e1 = M.ep1[p];
+        const float lim = 0.12f * 65536.0f;
+        M.ece_can_offset[p] = fabsf(e1.x - e0.x) < lim && fabsf(e1.y - e0.y) < lim && fabsf(e1.z - e0.z) < lim;
+        M.ece_can_bc[p] = (M.gray && M.calpha) ? 0 : 1;
+        // pass09 inputs of this partition; the 4 x 21 cells are filled later, one per role
+        const float ps = (float)(P == 1 ? T : tb.part_count(P, entry, p));
+        const float4 e0h = vmax(e0 - mk(65535.0f), mk(0.0f)), e1h = vmax(e1 - mk(65535.0f), mk(0.0f));
+        const float4 e0l = vmin(e0, mk(0.0f)), e1l = vmin(e1, mk(0.0f));
+        const float4 sre = ((e0l * e0l + e1l * e1l) + e0h * e0h) + e1h * e1h;
+        M.p9[p][0] = (dot3(sre, cw) * 0.5f) * ps;
+        M.p9[p][1] = ((sre.w * cw.w) * 0.5f) * ps;
+        M.p9[p][2] = ((cw.x + cw.y) + cw.z) * ps;
+        M.p9[p][3] = cw.w * ps;
+    }
 
     // Block-mode subset of the proposal search: only its modes and their
     // decimation modes are evaluated; the others never become candidates.
     const uint64_t* bmm = a.bm_mask ? a.bm_mask + ((size_t)lb * 4 + (P - 1)) * kMaskWords : nullptr;
-    int ndm_run = ndm;
-    const int16_t* dm_run = nullptr;
+    uint32_t* flags = reinterpret_cast<uint32_t*>(sm + fl.dml);  // 4 words: one bit per decimation mode
+    int16_t* list = reinterpret_cast<int16_t*>(sm + fl.dml + 16);
+    if (bmm && tid < 4) flags[tid] = 0;
+    __syncthreads();
     if (bmm) {
-        uint32_t* flags = reinterpret_cast<uint32_t*>(sm + fl.dml);  // 4 words: one bit per decimation mode
-        int16_t* list = reinterpret_cast<int16_t*>(sm + fl.dml + 16);
-        if (tid < 4) flags[tid] = 0;
-        __syncthreads();
         for (int i = tid; i < nbm; i += kFrontThreads)
             if ((bmm[i >> 6] >> (i & 63)) & 1) { const int d = tb.bm(i).dm; atomicOr(&flags[d >> 5], 1u << (d & 31)); }
-        __syncthreads();
-        if (tid == 0) {
-            int n = 0;
-            for (int d = 0; d < ndm; d++) if ((flags[d >> 5] >> (d & 31)) & 1) list[n++] = (int16_t)d;
-            flags[0] = n;  // the flags are no longer needed
+    }
+    // pass08 error terms of every texel against its partition's axes
+    for (int t = tid; t < Tp; t += kFrontThreads) {
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f, t4 = 0.0f;
+        if (t < T) {
+            const int p = tp[t];
+            const float4 ub = M.axes[p][0], ua = M.axes[p][1], sb = M.axes[p][2], la = M.axes[p][3];
+            const float4 lbv = normalize4(make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+            float4 rgb = px[t]; rgb.w = 0.0f;
+            const float ad = px[t].w - 65536.0f;
+            t0 = (ad * ad) * cw.w;
+            const float4 du = (ua + ub * dot3(rgb, ub)) - rgb;
+            t1 = dot3(du * du, cw);
+            const float4 ds = sb * dot3(rgb, sb) - rgb;
+            t2 = dot3(ds * ds, cw);
+            const float4 dl = (la + lbv * dot3(rgb, lbv)) - rgb;
+            t3 = dot3(dl * dl, cw);
+            const float4 dn = lbv * dot3(rgb, lbv) - rgb;
+            t4 = dot3(dn * dn, cw);
         }
-        __syncthreads();
-        ndm_run = (int)flags[0];
-        dm_run = list;
+        terms[t] = t0; terms[Tp + t] = t1; terms[2 * Tp + t] = t2; terms[3 * Tp + t] = t3; terms[4 * Tp + t] = t4;
+    }
+    __syncthreads();
+    // the decimation modes to run, in ascending order (warp 0); pass08 sums (role 5p + k)
+    if (bmm && warp == 0) {
+        int n = 0;
+        for (int d0 = 0; d0 < ndm; d0 += 32) {
+            const int d = d0 + lane;
+            const bool f = d < ndm && ((flags[d >> 5] >> (d & 31)) & 1);
+            const uint32_t b = __ballot_sync(FULL, f);
+            if (f) list[n + __popc(b & ((1u << lane) - 1))] = (int16_t)d;
+            n += __popc(b);
+        }
+        __syncwarp();
+        if (lane == 0) flags[0] = n;  // the flags are no longer needed
+    }
+    for (int v = role; v < 5 * P; v += kFrontThreads) {
+        const int p = v / 5, k = v % 5;
+        const float* x = terms + k * Tp;
+        float s = 0.0f;
+        for (int t = 0; t < Tp; t += 4) {
+            const float4 y = *reinterpret_cast<const float4*>(x + t);
+            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            s = s + ((int)(q & 0xFF) == p ? y.x : 0.0f); s = s + ((int)((q >> 8) & 0xFF) == p ? y.y : 0.0f);
+            s = s + ((int)((q >> 16) & 0xFF) == p ? y.z : 0.0f); s = s + ((int)(q >> 24) == p ? y.w : 0.0f);
+        }
+        M.acc[p][k] = s;
+    }
+    __syncthreads();
+    const int ndm_run = bmm ? (int)flags[0] : ndm;
+    const int16_t* dm_run = bmm ? list : nullptr;
+    // ---------------- pass09: colour error per partition, quant level and integer count
+    // (role 21p + q; runs beside passes 02-05, which do not read it)
+    for (int c = role; c < P * 21; c += kFrontThreads) {
+        const int p = c / 21, q = c % 21;
+        if (q < 4) {
+            for (int j = 0; j < 4; j++) M.cerr[p][q][j] = ERR_DEFAULT;
+            M.cfmt[p][q][0] = FMT_LUMINANCE; M.cfmt[p][q][1] = FMT_RGB_SCALE; M.cfmt[p][q][2] = FMT_RGB; M.cfmt[p][q][3] = FMT_RGBA;
+            continue;
+        }
+        const int i = q - 4;
+        const float rre = M.p9[p][0], are = M.p9[p][1], brgb = M.p9[p][2], ba = M.p9[p][3];
+        const bool cbc = M.ece_can_bc[p] == 1, coe = M.ece_can_offset[p] == 1;
+        const float bcrgba = cbc ? 0.625f : 1.0f, oergba = coe ? 0.5f : 1.0f, bcrgb = cbc ? 0.5f : 1.0f, oergb = coe ? 0.25f : 1.0f;
+        const float acc0 = M.acc[p][0], acc1 = M.acc[p][1], acc2 = M.acc[p][2], acc4 = M.acc[p][4];
+        const float rgbs_e = (acc2 - acc1) * 0.7f, lum_e = (acc4 - acc1) * 3.0f, ad_e = acc0 * 3.0f;
+        const float orgba = q >= 19 ? 1.0f : oergba, orgb = q >= 19 ? 1.0f : oergb;
+        const float bq = tb.bqe(i);
+        const float qrgb = brgb * bq, qrgba = (brgb + ba) * bq;
+        M.cerr[p][q][3] = (((qrgba * bcrgba) * orgba) + rre) + are; M.cfmt[p][q][3] = FMT_RGBA;
+        const float full = (((qrgb * bcrgb) * orgb) + rre) + ad_e;
+        const float rgbsa = ((qrgba + rgbs_e) + rre) + are;
+        if (rgbsa < full) { M.cerr[p][q][2] = rgbsa; M.cfmt[p][q][2] = FMT_RGB_SCALE_ALPHA; }
+        else { M.cerr[p][q][2] = full; M.cfmt[p][q][2] = FMT_RGB; }
+        const float lrgbs = ((qrgb + rre) + ad_e) + rgbs_e;
+        const float la_e = ((qrgba + rre) + are) + lum_e;
+        if (lrgbs < la_e) { M.cerr[p][q][1] = lrgbs; M.cfmt[p][q][1] = FMT_RGB_SCALE; }
+        else { M.cerr[p][q][1] = la_e; M.cfmt[p][q][1] = FMT_LUMINANCE_ALPHA; }
+        M.cerr[p][q][0] = ((qrgb + rre) + ad_e) + lum_e; M.cfmt[p][q][0] = FMT_LUMINANCE;
     }
 
     // ---------------- passes 02-05, one warp per decimation mode
@@ -546,7 +719,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         float* inf = reinterpret_cast<float*>(scr);
         uint32_t* smp = reinterpret_cast<uint32_t*>(scr + 144 * 4);
         float* ang = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4);
-        float* lh = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4 + 16 * 4);  // [16][5]: lowest, span, err, cl, ch
+        float* lh = reinterpret_cast<float*>(scr + 144 * 4 + 64 * 4 + 16 * 4);  // pass05 keys [16] (u64), minidx [16]
         for (int mi = warp; mi < ndm_run; mi += kFrontWarps) {
             const int m = dm_run ? dm_run[mi] : mi;
             const DevDm dmi = tb.dm(m);
@@ -615,8 +788,21 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
                 ang[lane] = atan2_search(ay, ax) * (1.0f / (2.0f * 3.14159265358979323846f));
             }
             __syncwarp();
-            // pass04: per angular step, rounding error and cut errors
+            // pass04 + pass05: lane i < S evaluates angular step i (rounding error and cut
+            // errors over the weights) and offers its candidates to the weight spans the
+            // sequential scan of pass05 would update with them: span sp takes e, sp - 1 takes
+            // e + cl and then e + ch, sp - 2 takes e + cl + ch, each only when strictly below the
+            // span's best so far (initially 1e37), steps in ascending order.  That scan keeps,
+            // per span, the first minimum in this order, which is the smallest key
+            //   error bits << 32 | step << 2 | order within the step << 1 | low-cut flag:
+            // errors are sums of non-negative products (never -0.0f, NaN or 1e37), so their
+            // bit patterns order like their values.  Only spans 0..15 are read (q <= 7 needs
+            // span c_steps_for_quant[q] <= 12; S <= 12 for every valid decimation mode).
             const int S = dmi.max_angular_steps;
+            unsigned long long* best = reinterpret_cast<unsigned long long*>(lh);  // [16]
+            float* lmin = lh + 32;                                                 // [16] minidx per step
+            if (lane < 16) best[lane] = ~0ull;
+            __syncwarp();
             if (lane < S) {
                 float mnw = 3.4e38f, mxw = -3.4e38f;
                 for (int j = 0; j < W; j++) { const float v = dw[j]; if (v < mnw) mnw = v; if (v > mxw) mxw = v; }
@@ -629,61 +815,36 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
                     cl = cl + (r == minidx ? 1.0f - (2.0f * d) : 0.0f);
                     ch = ch + (r == maxidx ? 1.0f + (2.0f * d) : 0.0f);
                 }
-                const int span = min(max(f2i((maxidx - minidx) + 1.0f), 2), (int)dmi.max_quant_steps + 3);
+                const int sp = min(max(f2i((maxidx - minidx) + 1.0f), 2), (int)dmi.max_quant_steps + 3);
                 const float ss = 1.0f / rcp, esc = ss * ss;
-                float* o = lh + lane * 5;
-                o[0] = minidx; o[1] = __int_as_float(span); o[2] = ev * esc; o[3] = cl * esc; o[4] = ch * esc;
+                const float e = ev * esc, ecl0 = cl * esc, ech0 = ch * esc;
+                const float ecl = e + ecl0, ech = e + ech0, eclh = (e + ecl0) + ech0;
+                lmin[lane] = minidx;
+                const unsigned long long ik = (unsigned long long)lane << 2;
+                if (sp < 16 && e < 1e37f) atomicMin(&best[sp], ((unsigned long long)__float_as_uint(e) << 32) | ik);
+                if (sp - 1 < 16 && ecl < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ecl) << 32) | ik | 1ull);
+                if (sp - 1 < 16 && ech < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ech) << 32) | ik | 2ull);
+                if (sp - 2 < 16 && eclh < 1e37f) atomicMin(&best[sp - 2], ((unsigned long long)__float_as_uint(eclh) << 32) | ik | 1ull);
             }
             __syncwarp();
-            // pass05: best angular step per weight span, then low/high value per quant level.
-            // Lane x keeps spans x and x + 32 and applies, step by step in order, the updates
-            // of the sequential scan that target them, so each keeps the same first minimum.
-            {
-                const int nb = min((int)dmi.max_quant_steps + 4, 36);
-                float be0 = 1e37f, bi0 = -1.0f, bc0 = 0.0f, be1 = 1e37f, bi1 = -1.0f, bc1 = 0.0f;
-                const int x0 = lane, x1 = lane + 32;
-                for (int i = 0; i < S; i++) {
-                    const float* o = lh + i * 5;
-                    const int sp = __float_as_int(o[1]);
-                    const float e = o[2], cl = o[3], ch = o[4];
-                    const float ecl = e + cl, ech = e + ch, eclh = (e + cl) + ch;
-                    const float fi = (float)i;
-                    if (x0 < nb) {
-                        if (sp == x0 && e < be0) { be0 = e; bi0 = fi; bc0 = 0.0f; }
-                        if (sp - 1 == x0) {
-                            if (ecl < be0) { be0 = ecl; bi0 = fi; bc0 = 1.0f; }
-                            if (ech < be0) { be0 = ech; bi0 = fi; bc0 = 0.0f; }
-                        }
-                        if (sp - 2 == x0 && eclh < be0) { be0 = eclh; bi0 = fi; bc0 = 1.0f; }
-                    }
-                    if (x1 < nb) {
-                        if (sp == x1 && e < be1) { be1 = e; bi1 = fi; bc1 = 0.0f; }
-                        if (sp - 1 == x1) {
-                            if (ecl < be1) { be1 = ecl; bi1 = fi; bc1 = 1.0f; }
-                            if (ech < be1) { be1 = ech; bi1 = fi; bc1 = 0.0f; }
-                        }
-                        if (sp - 2 == x1 && eclh < be1) { be1 = eclh; bi1 = fi; bc1 = 1.0f; }
-                    }
+            // pass05: low/high value per quant level from the best step of its span (step 0
+            // and no low cut when no candidate got below 1e37)
+            if (lane < 8) {
+                const int q = lane;
+                float lo_v = 0.0f, hi_v = 0.0f;
+                if (q <= (int)dmi.max_quant_level) {
+                    const int qs = c_steps_for_quant[q];
+                    const unsigned long long k = best[qs];
+                    const int bsi = k == ~0ull ? 0 : (int)(((uint32_t)k) >> 2);
+                    const float lwi = lmin[bsi] + ((k != ~0ull && (k & 1ull)) ? 1.0f : 0.0f);
+                    const float hwi = (lwi + (float)qs) - 1.0f;
+                    const float step = 1.0f / (1.0f + (float)bsi);
+                    const float off = ang[bsi];
+                    lo_v = (off + lwi) * step;
+                    hi_v = (off + hwi) * step;
                 }
-                const int q = lane;  // lanes 0..7: quant level q
-                const bool live = q < 8 && q <= (int)dmi.max_quant_level;
-                const int qs = live ? c_steps_for_quant[q] : 0;
-                const float bl = __shfl_sync(0xFFFFFFFFu, bi0, qs & 31), bh = __shfl_sync(0xFFFFFFFFu, bi1, qs & 31);
-                const float cl_ = __shfl_sync(0xFFFFFFFFu, bc0, qs & 31), ch_ = __shfl_sync(0xFFFFFFFFu, bc1, qs & 31);
-                if (q < 8) {
-                    float lo_v = 0.0f, hi_v = 0.0f;
-                    if (live) {
-                        const int bsi = max(f2i(qs < 32 ? bl : bh), 0);
-                        const float lwi = lh[bsi * 5] + (qs < 32 ? cl_ : ch_);
-                        const float hwi = (lwi + (float)qs) - 1.0f;
-                        const float step = 1.0f / (1.0f + (float)bsi);
-                        const float off = ang[bsi];
-                        lo_v = (off + lwi) * step;
-                        hi_v = (off + hwi) * step;
-                    }
-                    lov[m * 8 + q] = lo_v;
-                    hiv[m * 8 + q] = hi_v;
-                }
+                lov[m * 8 + q] = lo_v;
+                hiv[m * 8 + q] = hi_v;
             }
             __syncwarp();
         }
@@ -713,91 +874,10 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         bm_err[i] = err;
         bm_bits[i] = bc;
     }
-    // ---------------- pass08: encoding-choice errors per partition
-    if (tid < P) {
-        const int p = tid;
-        const float4 pavg = M.avg[p];
-        float4 sx = mk(0.0f), sy = mk(0.0f), sz = mk(0.0f);
-        for (int t = 0; t < T; t++) {
-            if (tp[t] != p) continue;
-            float4 d = px[t] - pavg;
-            d.w = 0.0f;
-            if (d.x > 0.0f) sx = sx + d;
-            if (d.y > 0.0f) sy = sy + d;
-            if (d.z > 0.0f) sz = sz + d;
-        }
-        const float pxx = dot4(sx, sx), pyy = dot4(sy, sy), pzz = dot4(sz, sz);
-        float4 bv = sx; float bs = pxx;
-        if (pyy > bs) { bv = sy; bs = pyy; }
-        if (pzz > bs) { bv = sz; bs = pzz; }
-        float4 avg = pavg; avg.w = 0.0f;
-        const float4 ub = normalize4(bv), ua = avg - ub * dot4(avg, ub);
-        const float4 sb = normalize4(avg);
-        const float4 lb = normalize4(make_float4(1.0f, 1.0f, 1.0f, 0.0f)), la = avg - lb * dot4(avg, lb);
-        float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f, acc4 = 0.0f;
-        for (int t = 0; t < T; t++) {
-            if (tp[t] != p) continue;
-            float4 rgb = px[t]; rgb.w = 0.0f;
-            const float ad = px[t].w - 65536.0f;
-            acc0 = acc0 + (ad * ad) * cw.w;
-            const float4 du = (ua + ub * dot3(rgb, ub)) - rgb;
-            acc1 = acc1 + dot3(du * du, cw);
-            const float4 ds = sb * dot3(rgb, sb) - rgb;
-            acc2 = acc2 + dot3(ds * ds, cw);
-            const float4 dl = (la + lb * dot3(rgb, lb)) - rgb;
-            acc3 = acc3 + dot3(dl * dl, cw);
-            const float4 dn = lb * dot3(rgb, lb) - rgb;
-            acc4 = acc4 + dot3(dn * dn, cw);
-        }
-        const float4 e0 = M.ep0[p], e1 = M.ep1[p];
-        const float lim = 0.12f * 65536.0f;
-        M.ece_can_offset[p] = fabsf(e1.x - e0.x) < lim && fabsf(e1.y - e0.y) < lim && fabsf(e1.z - e0.z) < lim;
-        M.ece_can_bc[p] = (M.gray && M.calpha) ? 0 : 1;
-        M.ece_rgb_scale[p] = (acc2 - acc1) * 0.7f;
-        M.ece_lum[p] = (acc4 - acc1) * 3.0f;
-        M.ece_alpha_drop[p] = acc0 * 3.0f;
-        // pass09 inputs of this partition; the 4 x 21 cells are filled below, one per thread
-        const float ps = (float)(P == 1 ? T : tb.part_count(P, entry, p));
-        const float4 e0h = vmax(e0 - mk(65535.0f), mk(0.0f)), e1h = vmax(e1 - mk(65535.0f), mk(0.0f));
-        const float4 e0l = vmin(e0, mk(0.0f)), e1l = vmin(e1, mk(0.0f));
-        const float4 sre = ((e0l * e0l + e1l * e1l) + e0h * e0h) + e1h * e1h;
-        M.p9[p][0] = (dot3(sre, cw) * 0.5f) * ps;
-        M.p9[p][1] = ((sre.w * cw.w) * 0.5f) * ps;
-        M.p9[p][2] = ((cw.x + cw.y) + cw.z) * ps;
-        M.p9[p][3] = cw.w * ps;
-    }
-    __syncthreads();
-    // ---------------- pass09: colour error per partition, quant level and integer count
-    for (int c = tid; c < P * 21; c += kFrontThreads) {
-        const int p = c / 21, q = c % 21;
-        if (q < 4) {
-            for (int j = 0; j < 4; j++) M.cerr[p][q][j] = ERR_DEFAULT;
-            M.cfmt[p][q][0] = FMT_LUMINANCE; M.cfmt[p][q][1] = FMT_RGB_SCALE; M.cfmt[p][q][2] = FMT_RGB; M.cfmt[p][q][3] = FMT_RGBA;
-            continue;
-        }
-        const int i = q - 4;
-        const float rre = M.p9[p][0], are = M.p9[p][1], brgb = M.p9[p][2], ba = M.p9[p][3];
-        const bool cbc = M.ece_can_bc[p] == 1, coe = M.ece_can_offset[p] == 1;
-        const float bcrgba = cbc ? 0.625f : 1.0f, oergba = coe ? 0.5f : 1.0f, bcrgb = cbc ? 0.5f : 1.0f, oergb = coe ? 0.25f : 1.0f;
-        const float rgbs_e = M.ece_rgb_scale[p], lum_e = M.ece_lum[p], ad_e = M.ece_alpha_drop[p];
-        const float orgba = q >= 19 ? 1.0f : oergba, orgb = q >= 19 ? 1.0f : oergb;
-        const float bq = tb.bqe(i);
-        const float qrgb = brgb * bq, qrgba = (brgb + ba) * bq;
-        M.cerr[p][q][3] = (((qrgba * bcrgba) * orgba) + rre) + are; M.cfmt[p][q][3] = FMT_RGBA;
-        const float full = (((qrgb * bcrgb) * orgb) + rre) + ad_e;
-        const float rgbsa = ((qrgba + rgbs_e) + rre) + are;
-        if (rgbsa < full) { M.cerr[p][q][2] = rgbsa; M.cfmt[p][q][2] = FMT_RGB_SCALE_ALPHA; }
-        else { M.cerr[p][q][2] = full; M.cfmt[p][q][2] = FMT_RGB; }
-        const float lrgbs = ((qrgb + rre) + ad_e) + rgbs_e;
-        const float la_e = ((qrgba + rre) + are) + lum_e;
-        if (lrgbs < la_e) { M.cerr[p][q][1] = lrgbs; M.cfmt[p][q][1] = FMT_RGB_SCALE; }
-        else { M.cerr[p][q][1] = la_e; M.cfmt[p][q][1] = FMT_LUMINANCE_ALPHA; }
-        M.cerr[p][q][0] = ((qrgb + rre) + ad_e) + lum_e; M.cfmt[p][q][0] = FMT_LUMINANCE;
-    }
-    __syncthreads();
     // ---------------- pass10: best format combination per quant level and integer total
-    if (P > 1 && tid < 17) {
-        const int q = tid + 4;
+    // (role q - 4; beside pass07, which does not read it)
+    if (P > 1 && role < 17) {
+        const int q = role + 4;
         const int NC = P == 2 ? 7 : P == 3 ? 10 : 13;
         for (int c = 0; c < NC; c++) M.combo_err[q][c] = ERR_DEFAULT;
         for (int i = 0; i < 4; i++)
