@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
 // whatever NT is (loops only spread independent items), so results do not depend on it.
 
 struct FrontLayout {
-    int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, dml, total;
+    int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, dml, bml, total;
 };
 constexpr int kScratchPerWarp = 144 * 4 + 64 * 4 + 16 * 4 + 16 * 20;
 
@@ -370,8 +370,19 @@ struct FrontMisc {
     uint8_t combo_fmt[21][13][4];
     int top[kNumCand];
     int ncand;
+    int nlive;  // block modes in the proposal search's list
 };
 
+// pass07's buffer in floats: one-thread-per-mode weights (max_w x nt), the proposal
+// search's groups (at least one mode: max_w + Tp), and before pass02 the texel
+// channels and projections, then pass08's error terms (5 x Tp); Tp = T rounded up to 4
+__host__ __device__ inline int front_layout_qf_floats(int T, int max_w, int nt) {
+    const int Tp = (T + 3) & ~3;
+    int f = max_w * nt;
+    if (f < 5 * Tp) f = 5 * Tp;
+    if (f < max_w + Tp) f = max_w + Tp;
+    return f;
+}
 __host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
 __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w, int nt) {
     FrontLayout f;
@@ -389,11 +400,10 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    // pass07's quantised weights; before pass02 the same bytes hold the texel channels and
-    // projections (5 x T rounded up to 4, floats) and then pass08's error terms (5 x that)
-    f.qf = take16(o, (max_w * nt > 5 * ((T + 3) & ~3) ? max_w * nt : 5 * ((T + 3) & ~3)) * 4);
+    f.qf = take16(o, front_layout_qf_floats(T, max_w, nt) * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.dml = take16(o, 16 + ndm * 2);
+    f.bml = take16(o, nbm * 2);  // the proposal search's block modes, ascending
     f.total = o;
     return f;
 }
@@ -629,9 +639,20 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     int16_t* list = reinterpret_cast<int16_t*>(sm + fl.dml + 16);
     if (bmm && tid < 4) flags[tid] = 0;
     __syncthreads();
+    int16_t* blist = reinterpret_cast<int16_t*>(sm + fl.bml);
     if (bmm) {
         for (int i = tid; i < nbm; i += kFrontThreads)
             if ((bmm[i >> 6] >> (i & 63)) & 1) { const int d = tb.bm(i).dm; atomicOr(&flags[d >> 5], 1u << (d & 31)); }
+        if (warp == 0) {  // the masked block modes in ascending order: each 32-bit half word is its own ballot
+            int n = 0;
+            for (int i0 = 0; i0 < nbm; i0 += 32) {
+                uint32_t b = (uint32_t)(bmm[i0 >> 6] >> (i0 & 63));
+                if (nbm - i0 < 32) b &= (1u << (nbm - i0)) - 1u;
+                if ((b >> lane) & 1u) blist[n + __popc(b & ((1u << lane) - 1u))] = (int16_t)(i0 + lane);
+                n += __popc(b);
+            }
+            if (lane == 0) M.nlive = n;
+        }
     }
     // pass08 error terms of every texel against its partition's axes
     for (int t = tid; t < Tp; t += kFrontThreads) {
@@ -852,27 +873,30 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     __syncthreads();
 
     // ---------------- pass07: weight quantisation error per block mode
-    for (int j = tid; j < nbm; j += kFrontThreads) {
-        const int i = tb.bm_order(j);  // neighbouring threads get modes of the same decimation
-        if (bmm && !((bmm[i >> 6] >> (i & 63)) & 1)) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
-        const DevBm bm = tb.bm(i);
-        const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
-        if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
-        const DevDm dmi = tb.dm(bm.dm);
-        const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
-        const float* dw = dec + bm.dm * 64;
-        for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
-        float err = 0.0f;
-        for (int t = 0; t < T; t++) {
-            const uint64_t e4 = tb.tw4(bm.dm, t);
-            float v = 0.0f;
+    const int nlist = bmm ? M.nlive : nbm;  // block modes evaluated: the list, or all of them
+    if (!bmm) {
+        // one thread per mode; neighbouring threads get modes of the same decimation
+        for (int j = tid; j < nbm; j += kFrontThreads) {
+            const int i = tb.bm_order(j);
+            const DevBm bm = tb.bm(i);
+            const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+            if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
+            const DevDm dmi = tb.dm(bm.dm);
+            const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
+            const float* dw = dec + bm.dm * 64;
+            for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
+            float err = 0.0f;
+            for (int t = 0; t < T; t++) {
+                const uint64_t e4 = tb.tw4(bm.dm, t);
+                float v = 0.0f;
 #pragma unroll
-            for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
-            const float d = v - iw[t];
-            err = err + (d * d) * wes[is_const ? 0 : t];
+                for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+                const float d = v - iw[t];
+                err = err + (d * d) * wes[is_const ? 0 : t];
+            }
+            bm_err[i] = err;
+            bm_bits[i] = bc;
         }
-        bm_err[i] = err;
-        bm_bits[i] = bc;
     }
     // ---------------- pass10: best format combination per quant level and integer total
     // (role q - 4; beside pass07, which does not read it)
@@ -918,9 +942,67 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
                 }
             }
     }
+    if (bmm) {
+        // The proposal search's few block modes, in groups that fit the buffer: the quantised
+        // weights (one thread per mode and weight), the error terms (one per mode and
+        // texel), then each mode's sum in texel order (padding texels add +0.0f to a sum of
+        // non-negative terms).  Each value is the one-thread-per-mode loop's.
+        const int mw = a.L.max_w;
+        const int qf_floats = front_layout_qf_floats(T, mw, kFrontThreads);
+        const int G = qf_floats / (mw + Tp);
+        float* qw = qfs;           // [G][mw]
+        float* et = qfs + G * mw;  // [G][Tp]
+        for (int g0 = 0; g0 < nlist; g0 += G) {
+            const int g = min(G, nlist - g0);
+            for (int it = tid; it < g * mw; it += kFrontThreads) {
+                const int k = it / mw, w = it - k * mw;
+                const DevBm bm = tb.bm(blist[g0 + k]);
+                const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+                if (bm.quant > 11 || bc <= 0 || w >= (int)tb.dm(bm.dm).W) continue;
+                const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
+                float qf;
+                bm_quant_weight(tb, s, dec[bm.dm * 64 + w], &qf);
+                qw[k * mw + w] = qf;
+            }
+            __syncthreads();
+            for (int it = tid; it < g * Tp; it += kFrontThreads) {
+                const int k = it / Tp, t = it - k * Tp;
+                const DevBm bm = tb.bm(blist[g0 + k]);
+                const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+                float term = 0.0f;
+                if (t < T && !(bm.quant > 11 || bc <= 0)) {
+                    const uint64_t e4 = tb.tw4(bm.dm, t);
+                    const float* qk = qw + k * mw;
+                    float v = 0.0f;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qk[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+                    const float d = v - iw[t];
+                    term = (d * d) * wes[is_const ? 0 : t];
+                }
+                et[k * Tp + t] = term;
+            }
+            __syncthreads();
+            // (the next group's first phase writes only qw, which this one does not read)
+            for (int k = tid; k < g; k += kFrontThreads) {
+                const int i = blist[g0 + k];
+                const DevBm bm = tb.bm(i);
+                const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+                if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
+                const float* x = et + k * Tp;
+                float err = 0.0f;
+                for (int t = 0; t < Tp; t += 4) {
+                    const float4 y = *reinterpret_cast<const float4*>(x + t);
+                    err = err + y.x; err = err + y.y; err = err + y.z; err = err + y.w;
+                }
+                bm_err[i] = err;
+                bm_bits[i] = bc;
+            }
+        }
+    }
     __syncthreads();
     // ---------------- pass11: best colour combination per block mode
-    for (int i = tid; i < nbm; i += kFrontThreads) {
+    for (int k = tid; k < nlist; k += kFrontThreads) {
+        const int i = bmm ? blist[k] : k;
         const float werr = bm_err[i];
         uint8_t* fm = ccr_fmt + i * 4;
         if (werr >= ERR_DEFAULT) { ccr_tot[i] = ERR_DEFAULT; ccr_q[i * 2] = ccr_q[i * 2 + 1] = 0; fm[0] = fm[1] = fm[2] = fm[3] = 0; continue; }
@@ -957,13 +1039,29 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     // warp 0 picks them in order: each round the (error, index)-smallest mode after the
     // previous pick -- the order in which counting, for every mode, the modes ranked
     // before it would place them
-    if (warp == 0) {
+    if (warp == 0 && bmm && nlist <= 32) {
+        // up to 32 listed modes, one per lane: a usable mode's pick position is the number
+        // of usable modes before it in (error, index) order
+        const int i = lane < nlist ? blist[lane] : 0x7FFFFFFF;
+        const float e = lane < nlist ? ccr_tot[i] : ERR_DEFAULT;
+        const bool ok = e < ERR_DEFAULT;
+        int rank = 0;
+        for (int j = 0; j < nlist; j++) {
+            const float ej = __shfl_sync(FULL, e, j);
+            const int ij = __shfl_sync(FULL, i, j);
+            rank += (ej < ERR_DEFAULT && (ej < e || (ej == e && ij < i))) ? 1 : 0;
+        }
+        const int nok = __popc(__ballot_sync(FULL, ok));
+        if (ok && rank < kNumCand) M.top[rank] = i;
+        if (lane >= nok && lane < kNumCand) M.top[lane] = -1;
+    } else if (warp == 0) {
         float pv = 0.0f;
         int pi = -1;
         for (int r = 0; r < kNumCand; r++) {
             float be = 3.4e38f;
             int bi = 0x7FFFFFFF;
-            for (int i = lane; i < nbm; i += 32) {
+            for (int k = lane; k < nlist; k += 32) {
+                const int i = bmm ? blist[k] : k;
                 const float e = ccr_tot[i];
                 if (!(e < ERR_DEFAULT)) continue;
                 if (r > 0 && !(e > pv || (e == pv && i > pi))) continue;
