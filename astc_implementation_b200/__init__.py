@@ -111,6 +111,7 @@ def load_library():
         "astcb200_set_pruning": (I32, [P, ctypes.POINTER(Pruning)]),
         "astcb200_pruning_stats": (I32, [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
         "astcb200_proposal_logits": (I32, [P, P, P, SZ]),
+        "astcb200_proposal_selection": (I32, [P, P, P, P, P, SZ]),
         "astcb200_train_gemm": (I32, [P, P, P, I32, I32, I32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                       P, I32, I32, P]),
         "astcb200_train_xent": (I32, [P, U32, P, P, U32, U32, U32, P, P, P, P]),
@@ -276,6 +277,19 @@ class ASTCEncoder:
         z = np.empty((self.numBlocks, outputs), np.float32)
         _check(load_library().astcb200_proposal_logits(self._ctx, _ptr(img), _ptr(z), z.size), self._ctx)
         return z
+
+    def proposal_selection(self, imageData):
+        """The proposal search's selection for an image (test hook): route (numBlocks,) with
+        0 = proposal search, 1 = full search; picks (numBlocks, 18) = count, flags, then the
+        partitionings (P - 2) << 10 | entry; masks (numBlocks, 16) = block-mode bits per P."""
+        img = self._image(imageData)
+        n = self.numBlocks
+        route = np.empty(n, np.uint8)
+        picks = np.empty((n, 18), np.uint16)
+        masks = np.empty((n, 16), np.uint64)
+        _check(load_library().astcb200_proposal_selection(self._ctx, _ptr(img), _ptr(route), _ptr(picks), _ptr(masks), n),
+               self._ctx)
+        return route, picks, masks
 
     def stage_times(self):
         """(ms[4], launches[4]) per kernel for the last encode (needs stage_timing=True)."""

@@ -318,4 +318,79 @@ int astcb200_proposal_logits(astcb200_ctx* ctx, const uint8_t* rgba8, float* log
     return ASTCB200_OK;
 }
 
+int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* route, uint16_t* picks,
+                                uint64_t* masks, size_t nblocks) {
+    if (!ctx || !rgba8 || !route || !picks || !masks) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    if (nblocks < ctx->nblocks) return ASTCB200_BAD_ARG;
+    const NetDev* nd = nullptr;
+    for (const NetDev* x : ctx->nets)
+        if (x->bx == (int)ctx->bx && x->by == (int)ctx->by) nd = x;
+    if (!nd) { ctx->err = "no network for this footprint"; return ASTCB200_BAD_ARG; }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t in_bytes = (size_t)ctx->width * ctx->height * 4;
+    const size_t chunk = std::min<size_t>(ctx->chunk, ctx->nblocks);
+    const size_t nchunks = (ctx->nblocks + chunk - 1) / chunk;
+    Scratch& sc = ctx->scratch;
+    int rc;
+    if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.logits, sc.cap_logits, chunk * nd->net.s.nout * sizeof(float), "cudaMalloc logits"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.lists, sc.cap_lists, chunk * 2 * sizeof(int), "cudaMalloc block lists"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.prop, sc.cap_prop, chunk * sizeof(PropPicks), "cudaMalloc proposals"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.masks, sc.cap_masks, chunk * 4 * kMaskWords * sizeof(uint64_t), "cudaMalloc block-mode masks"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.full_err, sc.cap_ferr, chunk * sizeof(float), "cudaMalloc full-search errors"))) return rc;
+    if ((rc = ensure_buf(ctx, sc.pbl, sc.cap_pbl, chunk * 4 * kMaxProposals * sizeof(uint32_t), "cudaMalloc work lists"))) return rc;
+    if ((rc = begin_routes(ctx, nchunks))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
+    KernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.img = ctx->d_img;
+    a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
+    a.tables = ctx->cur->d;
+    a.L = ctx->cur->L;
+    const Pruning& pr = ctx->pruning;
+    mlp::Select sel;
+    sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
+    sel.p1_floor = pr.p1_floor;
+    for (int i = 0; i < 3; i++) sel.sel[i] = (int)ctx->cur->L.count_selected[i + 1];
+    std::memset(route, 1, ctx->nblocks);
+    std::memset(picks, 0, ctx->nblocks * 18 * sizeof(uint16_t));
+    std::memset(masks, 0, ctx->nblocks * 4 * kMaskWords * sizeof(uint64_t));
+    std::vector<int> lst(chunk);
+    std::vector<PropPicks> pp(chunk);
+    std::vector<uint64_t> mk(chunk * 4 * kMaskWords);
+    int counts[mlp::kRouteCounters];
+    for (uint32_t first = 0; first < ctx->nblocks; first += (uint32_t)chunk) {
+        a.block_first = (int)first;
+        a.nblocks = (int)std::min<size_t>(chunk, ctx->nblocks - first);
+        mlp::Routes r;
+        r.counts = ctx->d_counts + mlp::kRouteCounters * ctx->counts_used++;
+        r.pruned = sc.lists; r.full = sc.lists + chunk; r.full_err = sc.full_err;
+        r.prop = sc.prop; r.masks = sc.masks; r.confidence = nullptr;
+        r.pb_list = sc.pbl; r.pb_stride = (int)(chunk * kMaxProposals);
+        CK(cudaMemsetAsync(r.counts, 0, mlp::kRouteCounters * sizeof(int), ctx->stream), "reset route counters");
+        CK(mlp::launch_mlp_logits(a, nd->net, sc.logits, ctx->d_mlp_error, ctx->stream), "k_mlp_logits");
+        CK(mlp::launch_select(a, nd->net, sc.logits, sel, r, ctx->stream), "k_select");
+        CK(cudaMemcpyAsync(counts, r.counts, sizeof(counts), cudaMemcpyDeviceToHost, ctx->stream), "D2H route counters");
+        CK(cudaMemcpyAsync(lst.data(), sc.lists, (size_t)a.nblocks * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H list");
+        CK(cudaMemcpyAsync(pp.data(), sc.prop, (size_t)a.nblocks * sizeof(PropPicks), cudaMemcpyDeviceToHost, ctx->stream), "D2H picks");
+        CK(cudaMemcpyAsync(mk.data(), sc.masks, (size_t)a.nblocks * 4 * kMaskWords * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                           ctx->stream), "D2H masks");
+        if ((rc = wait_stream(ctx, ctx->stream))) return rc;
+        for (int pos = 0; pos < counts[0] && pos < a.nblocks; pos++) {
+            const int blk = lst[pos];
+            if (blk < 0 || (uint32_t)blk >= ctx->nblocks) { ctx->err = "selection list out of range"; return ASTCB200_CUDA_ERROR; }
+            route[blk] = 0;
+            uint16_t* o = picks + (size_t)blk * 18;
+            o[0] = pp[pos].n; o[1] = pp[pos].flags;
+            for (int j = 0; j < 16; j++) o[2 + j] = pp[pos].v[j];
+            std::memcpy(masks + (size_t)blk * 4 * kMaskWords, mk.data() + (size_t)pos * 4 * kMaskWords, 4 * kMaskWords * sizeof(uint64_t));
+        }
+    }
+    int err = 0;
+    CK(cudaMemcpy(&err, ctx->d_mlp_error, sizeof(int), cudaMemcpyDeviceToHost), "read error flag");
+    if (err) { ctx->err = "a network inference CTA gave up waiting for its copies or MMAs"; return ASTCB200_TIMEOUT; }
+    return ASTCB200_OK;
+}
+
 }  // extern "C"

@@ -193,6 +193,14 @@ int astcb200_pruning_stats(astcb200_ctx* ctx, uint64_t* proposal_blocks, uint64_
 /* Test hook: the network's logits (blocks x outputs, FP32) for the image set by
  * astcb200_set_image, from host RGBA8. */
 int astcb200_proposal_logits(astcb200_ctx* ctx, const uint8_t* rgba8, float* logits, size_t logits_len);
+/* Test hook (no reference counterpart): the selection the proposal search makes for the
+ * image set by astcb200_set_image, from host RGBA8, with the current pruning settings.
+ * Per block (raster order, nblocks >= the image's block count): route[i] = 0 proposal
+ * search, 1 full search; picks[i * 18 ...] = count n, flags (bit 0: P = 1 skipped), then
+ * n partitionings (P - 2) << 10 | table entry; masks[i * 16 ...] = for P = 1..4, four
+ * words of block-mode bits (valid block-mode order).  Full-search blocks get zeros. */
+int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* route, uint16_t* picks,
+                                uint64_t* masks, size_t nblocks);
 
 /* Training primitives of the proposal network (device pointers, FP32, queued on
  * cuda_stream, deterministic).  C[i][j] = sum_l A[i*sa_i + l*sa_l] * B[l*sb_l + j*sb_j]

@@ -656,6 +656,17 @@ void flags_from_texels(InputBlock& b, int T) {
 inline float dist_sq(v4 a, v4 b) { v4 d = a - b; return dot4(d * d, {CW[0], CW[1], CW[2], CW[3]}); }
 const v4 CWV = {0.30f * 2.25f, 0.59f * 2.25f, 0.11f * 2.25f, 1.0f};
 
+// The partitioned block of table entry `entry` (0..1023) for P = 2..4, as pass007
+// emits it (compression_pipeline.cpp passes 001-007 output).
+void make_pb(const Footprint& f, const InputBlock& blk, int P, int entry, InputBlock& nb) {
+    const PartInfo& pi = f.pinfo[(P - 2) * 1024 + entry];
+    std::memcpy(nb.px, blk.px, sizeof(nb.px));
+    nb.gray = blk.gray; nb.calpha = blk.calpha;
+    nb.pidx = pi.index;
+    for (int p = 0; p < 4; p++) nb.pcount[p] = pi.texel_count[p];
+    for (int t = 0; t < MAX_TEXELS; t++) nb.tp[t] = pi.of_texel[t];
+}
+
 // ---------------------------------------------------------------- partition search, passes 001-007
 // Returns the number of partitioned blocks written to out[].
 int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBlock* out, uint32_t* entries_out) {
@@ -847,15 +858,8 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
         if (!written) { fin[emitted++] = idx; if (emitted >= req) break; }
     }
     for (int i = 0; i < emitted; i++) {
-        uint32_t entry = (P - 2) * 1024 + fin[i];  // REF-BUG-4: rank used as table index
-        const PartInfo& pi = f.pinfo[entry];
-        InputBlock& nb = out[i];
-        std::memcpy(nb.px, blk.px, sizeof(nb.px));
-        nb.gray = blk.gray; nb.calpha = blk.calpha;
-        nb.pidx = pi.index;
-        for (int p = 0; p < 4; p++) nb.pcount[p] = pi.texel_count[p];
-        for (int t = 0; t < MAX_TEXELS; t++) nb.tp[t] = pi.of_texel[t];
-        if (entries_out) entries_out[i] = entry;
+        make_pb(f, blk, P, (int)fin[i], out[i]);  // REF-BUG-4: rank used as table index
+        if (entries_out) entries_out[i] = (P - 2) * 1024 + fin[i];
     }
     return emitted;
 }
@@ -1741,7 +1745,11 @@ void pass17(const Footprint& f, const InputBlock& b, int P, Cand& c, Cand& top, 
     if (total < top.total_error) top = c;
 }
 
-Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w) {
+// mask (optional): the block modes to evaluate, one bit per valid block mode (4 words);
+// the others get pass07's "unusable" error and never become candidates.  topn: how many
+// of the 8 best trials are refined; iters: refinement iterations (the reference: 8, 6).
+Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w, const uint64_t* mask = nullptr,
+               int topn = NUM_CAND, int iters = 6) {
     pass01(f, b, w.ei);
     const int ndm = (int)f.valid_dms.size(), nbm = (int)f.valid_bms.size();
     for (int m = 0; m < ndm; m++) {
@@ -1752,7 +1760,15 @@ Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w) {
         pass05(di, w.lh[m], w.ang[m], w.lowv[m], w.highv[m]);
     }
     w.qr.resize(nbm); w.ccr.resize(nbm);
-    for (int i = 0; i < nbm; i++) pass07(f, b, w, P, i);
+    for (int i = 0; i < nbm; i++) {
+        if (mask && !((mask[i >> 6] >> (i & 63)) & 1)) {
+            QuantRes& r = w.qr[i];
+            std::memset(r.qw, 0, sizeof(r.qw));
+            r.error = 1e38f; r.bitcount = 0;
+            continue;
+        }
+        pass07(f, b, w, P, i);
+    }
     pass08(f, b, w.ei, P, w.ece);
     pass09(b, w.ei, w.ece, P, w.cerr, w.cfmt);
     if (P > 1) pass10(P, w.cerr, w.cfmt, w.combo);
@@ -1782,9 +1798,9 @@ Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w) {
         ncand = k + 1;
     }
     // compression_pipeline.cpp:473-484 refinement loop, one candidate at a time
-    for (int k = 0; k < ncand; k++) {
+    for (int k = 0; k < std::min(ncand, topn); k++) {
         Cand& c = w.cand[k];
-        for (int a = 0; a < 6; a++) {
+        for (int a = 0; a < iters; a++) {
             pass13(f, b, P, c, w.rgbs[k]);
             pass14(P, c, w.rgbs[k]);
             pass15(P, c, w.ue0[k], w.ue1[k]);
@@ -1823,6 +1839,31 @@ Sym encode_block(const Footprint& f, const InputBlock& blk, PBWork& w) {
             if (bc == nullptr || cur[i].err < bc->err) bc = &cur[i];
         }
         if (bc && bc->err < best.err) best = *bc;
+    }
+    return best;
+}
+
+// The search restricted to given candidates (no counterpart in the reference; the
+// checker of the learned proposal search): P = 1 unless flags bit 0 is set, then the
+// proposed partitionings in the given order, each with its partition count's block-mode
+// mask, `topn` trials refined `iters` times; the first minimum over that order wins, and
+// only errors below 1e30 count (`found` = 0: none, the block goes to the full search).
+Sym encode_block_restricted(const Footprint& f, const InputBlock& blk, PBWork& w, const uint16_t* picks,
+                            const uint64_t* masks, int topn, int iters, bool& found) {
+    Sym best; std::memset(&best, 0, sizeof(best)); best.err = 1e30f;
+    found = false;
+    const int n = picks[0], flags = picks[1];
+    for (int s = (flags & 1) ? 1 : 0; s <= n; s++) {
+        int P = 1;
+        InputBlock pb;
+        if (s == 0) pb = blk;
+        else {
+            const int v = picks[2 + s - 1];
+            P = 2 + (v >> 10);
+            make_pb(f, blk, P, v & 1023, pb);
+        }
+        const Sym cur = process_pb(f, pb, P, w, masks + (P - 1) * 4, topn, iters);
+        if (cur.err < best.err) { best = cur; found = true; }
     }
     return best;
 }
@@ -2004,6 +2045,42 @@ int orc_encode_blocks(const float* texels, int nblocks, int bx, int by, int thre
         uint32_t words[ORC_SYMBOLIC_WORDS]; sym_to_words(s, words);
         if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
         if (out_blocks) sym_to_phys(f, words, out_blocks + (size_t)i * 16);
+    });
+    return 0;
+}
+
+int orc_encode_restricted(const uint8_t* rgba, int width, int height, int bx, int by, int threads,
+                          const uint16_t* picks, const uint64_t* masks, int topn, int refine_iters,
+                          uint8_t* out_blocks, uint32_t* symbolic, uint8_t* found) {
+    if (!rgba || width <= 0 || height <= 0 || !valid_footprint(bx, by) || !picks || !masks || !found ||
+        topn < 1 || topn > NUM_CAND || refine_iters < 1)
+        return -1;
+    const Footprint& f = *get_fp(bx, by);
+    if (f.valid_bms.size() > 256) return -1;  // masks hold 256 block modes
+    CT();
+    int nbx = (width + bx - 1) / bx, nby = (height + by - 1) / by, n = nbx * nby;
+    for (int i = 0; i < n; i++) {
+        const uint16_t* pk = picks + (size_t)i * ORC_PICK_WORDS;
+        if (pk[0] > 16) return -1;
+        for (int j = 0; j < pk[0]; j++) {
+            const int P = 2 + (pk[2 + j] >> 10), e = pk[2 + j] & 1023;
+            if (P > 4 || e >= (int)f.count_selected[P - 1]) return -1;
+        }
+    }
+    run_parallel(n, threads, [&](int i, PBWork& w) {
+        InputBlock b; make_block(rgba, width, height, bx, by, i % nbx, i / nbx, b);
+        bool ok = false;
+        Sym s = encode_block_restricted(f, b, w, picks + (size_t)i * ORC_PICK_WORDS, masks + (size_t)i * 16, topn,
+                                        refine_iters, ok);
+        found[i] = ok ? 1 : 0;
+        uint32_t words[ORC_SYMBOLIC_WORDS];
+        if (ok) sym_to_words(s, words);
+        else std::memset(words, 0, sizeof(words));  // no block to describe
+        if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
+        if (out_blocks) {
+            if (ok) sym_to_phys(f, words, out_blocks + (size_t)i * 16);
+            else std::memset(out_blocks + (size_t)i * 16, 0, 16);
+        }
     });
     return 0;
 }

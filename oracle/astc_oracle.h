@@ -37,6 +37,18 @@ int orc_encode(const uint8_t* rgba, int width, int height, int bx, int by, int t
 int orc_encode_blocks(const float* texels, int nblocks, int bx, int by, int threads,
                       uint32_t* symbolic, uint8_t* out_blocks);
 
+// The search restricted to given candidates, the checker of the learned proposal
+// search (no counterpart in the reference).  Per block: picks[ORC_PICK_WORDS] = count n
+// (<= 16), flags (bit 0: skip P = 1), then n partitionings (P - 2) << 10 | table entry;
+// masks[16] = for P = 1..4, 4 words of block-mode bits (valid block-mode order).  The
+// first `topn` (1..8) trials are refined `refine_iters` times.  found[i] = 0 when no
+// candidate reached an error below 1e30 (that block's outputs are then zero).
+// Footprints with more than 256 valid block modes are rejected (-1).
+#define ORC_PICK_WORDS 18
+int orc_encode_restricted(const uint8_t* rgba, int width, int height, int bx, int by, int threads,
+                          const uint16_t* picks, const uint64_t* masks, int topn, int refine_iters,
+                          uint8_t* out_blocks, uint32_t* symbolic, uint8_t* found);
+
 // Packs one SymbolicBlock into a physical block (restatement of
 // code/physical_compression.cpp:843).
 int orc_symbolic_to_physical(int bx, int by, const uint32_t* symbolic, uint8_t* out16);

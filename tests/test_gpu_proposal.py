@@ -154,6 +154,64 @@ def test_proposal_search_obeys_the_selection(bx, by):
     assert ab.psnr(dec, img) > ab.psnr(ab.decode(bx, by, 90, 61, full), img) - 3.0
 
 
+def restricted_oracle(img, bx, by, picks, masks, topn, iters):
+    h, w = img.shape[:2]
+    n = picks.shape[0]
+    out = np.zeros((n, 16), np.uint8)
+    sym = np.zeros((n, 108), np.uint32)
+    found = np.zeros(n, np.uint8)
+    rc = _libs.oracle().orc_encode_restricted(_libs.ptr(np.ascontiguousarray(img)), w, h, bx, by, 0,
+                                              _libs.ptr(np.ascontiguousarray(picks)), _libs.ptr(np.ascontiguousarray(masks)),
+                                              topn, iters, _libs.ptr(out), _libs.ptr(sym), _libs.ptr(found))
+    assert rc == 0
+    return out, sym, found.astype(bool)
+
+
+def full_oracle(img, bx, by):
+    h, w = img.shape[:2]
+    n = ((w + bx - 1) // bx) * ((h + by - 1) // by)
+    out = np.zeros((n, 16), np.uint8)
+    sym = np.zeros((n, 108), np.uint32)
+    assert _libs.oracle().orc_encode(_libs.ptr(np.ascontiguousarray(img)), w, h, bx, by, 0, _libs.ptr(out), _libs.ptr(sym)) == 0
+    return out, sym
+
+
+@pytest.mark.parametrize("bx,by,net_kind,prune", [
+    (4, 4, "shipped", dict(topn=2, iters=3)),
+    (6, 6, "shipped", dict(topn=2, iters=3)),
+    (4, 4, "random", dict(max_partitionings=6, block_modes=8, refine_candidates=4, refine_iterations=6,
+                          coverage=0.999, threshold=1e-4, single_partition_floor=0.3, topn=4, iters=6)),
+    (6, 6, "random", dict(max_partitionings=3, block_modes=40, refine_candidates=1, refine_iterations=2,
+                          coverage=0.95, threshold=1e-3, topn=1, iters=2)),
+])
+def test_proposal_search_bit_exact_against_restricted_oracle(bx, by, net_kind, prune):
+    """Given the selection the GPU made (routes, partitionings, block-mode masks), every
+    block equals the CPU oracle's search restricted to those candidates; blocks routed to
+    the full search, or left without a candidate, equal the oracle's full search."""
+    prune = dict(prune)
+    topn, iters = prune.pop("topn"), prune.pop("iters")
+    lay = proposal.Layout(bx, by)
+    net = proposal.load_weights(bx, by) if net_kind == "shipped" else random_net(lay, 11)
+    w, h = 11 * bx + 3, 7 * by + 2  # ragged edges
+    img = synth.make_texture(w, h, 90 + bx)
+    enc = ab.ASTCEncoder(device=0)
+    enc.secondaryInit(w, h, bx, by)
+    enc.set_proposal_net(net)
+    enc.set_pruning(True, reroute_error=0.0, **prune)
+    sym = enc.encode_symbolic(img)
+    blocks = enc.encode(img)
+    route, picks, masks = enc.proposal_selection(img)
+    enc.close()
+    r_out, r_sym, found = restricted_oracle(img, bx, by, picks, masks, topn, iters)
+    f_out, f_sym = full_oracle(img, bx, by)
+    prop = (route == 0) & found
+    assert prop.sum() > 0.5 * len(route)
+    assert np.array_equal(sym[prop], r_sym[prop]) and np.array_equal(blocks.reshape(-1, 16)[prop], r_out[prop])
+    assert np.array_equal(sym[~prop], f_sym[~prop]) and np.array_equal(blocks.reshape(-1, 16)[~prop], f_out[~prop])
+    if net_kind == "random" and prune.get("single_partition_floor"):
+        assert ((picks[:, 1] & 1) == 1)[route == 0].any()  # the P = 1 skip is exercised
+
+
 @pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
 def test_reroute_keeps_the_better_of_both_searches(bx, by):
     """With every proposal-search block also sent to the full search, each block ends

@@ -59,3 +59,66 @@ def test_partition_search_returns_reference_rank_entries():
         assert 1 <= n <= 4
         # the rank among the first 128 ordered candidates is used as the table entry
         assert all((P - 2) * 1024 <= e < (P - 2) * 1024 + 128 for e in ent[:n])
+
+
+def _restricted(img, bx, by, picks, masks, topn, iters):
+    h, w = img.shape[:2]
+    n = picks.shape[0]
+    out = np.zeros((n, 16), np.uint8)
+    sym = np.zeros((n, 108), np.uint32)
+    found = np.zeros(n, np.uint8)
+    rc = _libs.oracle().orc_encode_restricted(_libs.ptr(np.ascontiguousarray(img)), w, h, bx, by, 0, _libs.ptr(picks),
+                                              _libs.ptr(masks), topn, iters, _libs.ptr(out), _libs.ptr(sym), _libs.ptr(found))
+    assert rc == 0
+    return out, sym, found.astype(bool)
+
+
+@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
+def test_restricted_search_with_every_candidate_is_the_full_search(bx, by):
+    """The proposal search's checker, given P = 1, every partitioning the partition search
+    emits (in partition-count order), all block modes, 8 trials and 6 iterations, is the
+    full search block for block."""
+    img = synth.make_texture(3 * bx + 1, 2 * by + 3, 23)
+    tex = synth.texel_blocks(img, bx, by)
+    n = tex.shape[0]
+    picks = np.zeros((n, 18), np.uint16)
+    for i in range(n):
+        v = []
+        for P in (2, 3, 4):
+            ent = np.zeros(4, np.uint32)
+            k = _libs.oracle().orc_partition_search(bx, by, _libs.ptr(np.ascontiguousarray(tex[i])), P, _libs.ptr(ent))
+            v += [int(e) for e in ent[:k]]
+        picks[i, 0] = len(v)
+        picks[i, 2:2 + len(v)] = v
+    masks = np.full((n, 16), np.iinfo(np.uint64).max, np.uint64)
+    full_out, full_sym = _encode(img, bx, by)
+    out, sym, found = _restricted(img, bx, by, picks, masks, 8, 6)
+    assert found.all()
+    assert np.array_equal(sym, full_sym) and np.array_equal(out, full_out.reshape(n, 16))
+    # fewer candidates never beat the full search; with none at all nothing is found
+    picks_p1 = np.zeros_like(picks)
+    _, sym1, found1 = _restricted(img, bx, by, picks_p1, masks, 2, 3)
+    assert found1.all() and (sym1[:, 0].view(np.float32) >= full_sym[:, 0].view(np.float32)).all()
+    picks_none = picks_p1.copy()
+    picks_none[:, 1] = 1
+    _, _, found0 = _restricted(img, bx, by, picks_none, masks, 2, 3)
+    assert not found0.any()
+
+
+def test_restricted_search_rejects_bad_candidates():
+    img = synth.make_texture(8, 8, 1)
+    picks = np.zeros((4, 18), np.uint16)
+    masks = np.zeros((4, 16), np.uint64)
+    out = np.zeros((4, 16), np.uint8)
+    found = np.zeros(4, np.uint8)
+    orc = _libs.oracle()
+    args = lambda pk, topn, iters, bx=4: (_libs.ptr(img), 8, 8, bx, bx, 1, _libs.ptr(pk), _libs.ptr(masks), topn, iters,
+                                          _libs.ptr(out), None, _libs.ptr(found))
+    assert orc.orc_encode_restricted(*args(picks, 9, 3)) == -1       # topn above 8
+    assert orc.orc_encode_restricted(*args(picks, 2, 0)) == -1       # no refinement
+    bad = picks.copy()
+    bad[0, 0], bad[0, 2] = 1, (3 << 10)                               # P = 5
+    assert orc.orc_encode_restricted(*args(bad, 2, 3)) == -1
+    bad[0, 2] = 1023                                                  # entry beyond the selected ones
+    assert orc.orc_encode_restricted(*args(bad, 2, 3)) == -1
+    assert orc.orc_encode_restricted(*args(picks, 2, 3, bx=12)) == -1  # more than 256 block modes
