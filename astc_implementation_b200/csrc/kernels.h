@@ -180,7 +180,7 @@ __device__ __forceinline__ uint4* block_dst(const KernelArgs& a, int blk) {
 #endif
 
 // Shared-memory sizes the launches need for one footprint.
-size_t front_smem_bytes(const TableLayout& L, int threads = 128);
+size_t front_smem_bytes(const TableLayout& L, int threads = 128, bool list = false);
 size_t refine_smem_bytes(const TableLayout& L);
 size_t search_smem_bytes(const TableLayout& L);
 

@@ -373,18 +373,20 @@ struct FrontMisc {
     int nlive;  // block modes in the proposal search's list
 };
 
-// pass07's buffer in floats: one-thread-per-mode weights (max_w x nt), the proposal
-// search's groups (at least one mode: max_w + Tp), and before pass02 the texel
-// channels and projections, then pass08's error terms (5 x Tp); Tp = T rounded up to 4
-__host__ __device__ inline int front_layout_qf_floats(int T, int max_w, int nt) {
+// pass07's buffer in floats, before pass02 also the texel channels and projections,
+// then pass08's error terms (5 x Tp; Tp = T rounded up to 4).  The full search's
+// pass07 takes one thread per mode (max_w x nt); the proposal search's (`list`) works on
+// groups of kListGroup modes (max_w + Tp each), so its launches need less shared memory
+// and more of its CTAs fit on an SM.
+constexpr int kListGroup = 16;
+__host__ __device__ inline int front_layout_qf_floats(int T, int max_w, int nt, bool list) {
     const int Tp = (T + 3) & ~3;
-    int f = max_w * nt;
+    int f = list ? kListGroup * (max_w + Tp) : max_w * nt;
     if (f < 5 * Tp) f = 5 * Tp;
-    if (f < max_w + Tp) f = max_w + Tp;
     return f;
 }
 __host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
-__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w, int nt) {
+__host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int max_w, int nt, bool list) {
     FrontLayout f;
     int o = 0;
     f.px = take16(o, T * 16);
@@ -400,7 +402,7 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.ccr_tot = take16(o, nbm * 4);
     f.ccr_q = take16(o, nbm * 2);
     f.ccr_fmt = take16(o, nbm * 4);
-    f.qf = take16(o, front_layout_qf_floats(T, max_w, nt) * 4);
+    f.qf = take16(o, front_layout_qf_floats(T, max_w, nt, list) * 4);
     f.misc = take16(o, (int)sizeof(FrontMisc));
     f.dml = take16(o, 16 + ndm * 2);
     f.bml = take16(o, nbm * 2);  // the proposal search's block modes, ascending
@@ -448,7 +450,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     const Tabs tb{a.tables, &a.L};
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w, NT);
+    const FrontLayout fl = front_layout(T, ndm, nbm, a.L.max_w, NT, a.bm_mask != nullptr);
     float4* px = reinterpret_cast<float4*>(sm + fl.px);
     float* iw = reinterpret_cast<float*>(sm + fl.w);
     float* wes = reinterpret_cast<float*>(sm + fl.wes);
@@ -948,7 +950,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         // texel), then each mode's sum in texel order (padding texels add +0.0f to a sum of
         // non-negative terms).  Each value is the one-thread-per-mode loop's.
         const int mw = a.L.max_w;
-        const int qf_floats = front_layout_qf_floats(T, mw, kFrontThreads);
+        const int qf_floats = front_layout_qf_floats(T, mw, kFrontThreads, true);
         const int G = qf_floats / (mw + Tp);
         float* qw = qfs;           // [G][mw]
         float* et = qfs + G * mw;  // [G][Tp]
@@ -1128,8 +1130,11 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     }
 }
 
+// Resident CTAs of 128 threads the register budget is sized for (the proposal search's
+// compact layout lets that many fit in shared memory for the small footprints).
+constexpr int kFrontMinBlocks128 = 8;
 template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_front(const __grid_constant__ KernelArgs a) {
+__global__ void __launch_bounds__(NT, kFrontMinBlocks128 * 128 / NT > 32 ? 32 : kFrontMinBlocks128 * 128 / NT) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     // Items: every slot of every block in slot-major order (co-resident CTAs work on the
     // same partition count), or the proposal pass's work list grouped by partition count.
@@ -1166,7 +1171,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_front(const __grid_constant__
 }  // namespace
 
 size_t search_smem_bytes(const TableLayout&) { return (size_t)kSearchWarps * kSearchWarpBytes; }
-size_t front_smem_bytes(const TableLayout& L, int nt) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w, nt).total; }
+size_t front_smem_bytes(const TableLayout& L, int nt, bool list) { return (size_t)front_layout(L.T, L.ndm, L.nbm, L.max_w, nt, list).total; }
 
 // front_bytes: the 128-thread layout, the largest of the three.
 cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
@@ -1174,6 +1179,10 @@ cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+    // the largest shared-memory carveout: occupancy of the front is bounded by shared memory
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<128>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<32>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     return e;
 }
 
@@ -1189,7 +1198,7 @@ cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
     const int nt = a.front_threads == 32 || a.front_threads == 64 ? a.front_threads : 128;
     int grid = a.nblocks * a.slots;
     if (a.block_list) grid = std::min(grid, kListGridFront * (128 / nt));
-    const size_t smem = front_smem_bytes(a.L, nt);
+    const size_t smem = front_smem_bytes(a.L, nt, a.bm_mask != nullptr);
     if (nt == 32) k_front<32><<<grid, 32, smem, s>>>(a);
     else if (nt == 64) k_front<64><<<grid, 64, smem, s>>>(a);
     else k_front<128><<<grid, 128, smem, s>>>(a);
