@@ -13,6 +13,7 @@
 //                  written straight to the 16-byte output block.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 #include "device_math.cuh"
 #include "kernels.h"
@@ -297,7 +298,7 @@ constexpr int kRefineThreads = 128;
 __host__ __device__ inline int refine_cpb(int topn) { return topn <= 1 ? 1 : topn <= 2 ? 2 : topn <= 4 ? 4 : 8; }
 __host__ __device__ inline int refine_pbs(int T, int topn) {
     const int by_threads = kRefineThreads / refine_cpb(topn);
-    const int by_smem = 40960 / (T * 16);
+    const int by_smem = 40960 / (T * (T > 16 ? 4 : 16));
     return by_threads < by_smem ? by_threads : (by_smem > 16 ? by_smem : 16);
 }
 
@@ -341,9 +342,28 @@ __device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const uin
     return v;
 }
 
-constexpr int kUwCacheTexels = 36;  // footprints up to 6x6 keep each thread's infilled weights in shared memory
+constexpr int kUwCacheTexels = 16;  // footprints up to 4x4 keep each thread's infilled weights in shared memory
 
-__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const float4* px, const uint8_t* tp,
+// A partitioned block's staged texels.  Up to 16 texels they are floats; larger blocks
+// stage RGBA8 (4 bytes a texel, so more CTAs fit on an SM) read back through the CTA's
+// table of (v / 255) * 65536, the value src_texel computes.
+__host__ __device__ inline bool refine_u8(int T) { return T > 16; }
+template <bool U8> struct TexelRow;
+template <> struct TexelRow<true> {
+    const uchar4* c;
+    const float* lut;
+    __device__ __forceinline__ float4 operator[](int t) const {
+        const uchar4 v = c[t];
+        return make_float4(lut[v.x], lut[v.y], lut[v.z], lut[v.w]);
+    }
+};
+template <> struct TexelRow<false> {
+    const float4* c;
+    __device__ __forceinline__ float4 operator[](int t) const { return c[t]; }
+};
+
+template <class Row>
+__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const Row px, const uint8_t* tp,
                                  CandSmem& cs, float* uwc, Snap* snap) {
     const RTabs tb{a.tables, &a.L};
     const int T = a.L.T;
@@ -558,14 +578,17 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
 
 // CPB: candidate threads per partitioned block (refine_cpb of the launch's top-N), a
 // template parameter so that the full search's instance (8) keeps constant indexing.
-template <int CPB>
+// U8: texels staged as RGBA8 (refine_u8).
+template <int CPB, bool U8>
 __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int T = a.L.T;
     constexpr int cpb = CPB;
     const int pbs = CPB == 8 ? kRefineThreads / 8 : refine_pbs(T, CPB);
     CandSmem* cs = reinterpret_cast<CandSmem*>(smem);
-    float4* pxs = reinterpret_cast<float4*>(smem + sizeof(CandSmem) * kRefineThreads);
+    float* lut = reinterpret_cast<float*>(smem + sizeof(CandSmem) * kRefineThreads);
+    using Px = typename std::conditional<U8, uchar4, float4>::type;
+    Px* pxs = reinterpret_cast<Px*>(U8 ? smem + sizeof(CandSmem) * kRefineThreads + 256 * 4 : smem + sizeof(CandSmem) * kRefineThreads);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + pbs * T);
     int* keys = reinterpret_cast<int*>(tps + ((pbs * T + 15) & ~15));
     float* uwc_all = reinterpret_cast<float*>(keys + kRefineThreads);
@@ -578,6 +601,9 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
     const int ngroups = (npb + pbs - 1) / pbs;
     __shared__ unsigned int refined[4];  // candidates refined by this CTA, by P (work counters)
     if (tid < 4) refined[tid] = 0;
+    if (U8)
+        for (int v = tid; v < 256; v += kRefineThreads) lut[v] = ((float)v / 255.0f) * 65536.0f;  // as src_texel
+    // (the first group's barrier below orders these writes before any read)
     for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
         int my_lb = -1, my_slot = 0;  // this thread's partitioned block in the staging order
         {
@@ -596,7 +622,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
                     const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
                     const BlockSrc src = block_src(a, chunk_block(a, lb));
                     for (int t = k; t < T; t += cpb) {
-                        pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
+                        if constexpr (U8) pxs[pbl * T + t] = src_rgba8(src, a.L.bx, t);
+                        else pxs[pbl * T + t] = src_texel(src, a.L.bx, t);
                         tps[pbl * T + t] = P > 1 ? prow[t] : 0;
                     }
                 }
@@ -628,7 +655,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
             snap->err = ERR_DEFAULT;  // inert slot unless refined below
             if (k < (int)rec.ncand) {
                 float* uwc = T <= kUwCacheTexels ? uwc_all + tid : nullptr;
-                refine_candidate(a, rec, (int)rec.P, k, pxs + pbl * T, tps + pbl * T, cs[tid], uwc, snap);
+                if constexpr (U8) refine_candidate(a, rec, (int)rec.P, k, TexelRow<true>{pxs + pbl * T, lut}, tps + pbl * T, cs[tid], uwc, snap);
+                else refine_candidate(a, rec, (int)rec.P, k, TexelRow<false>{pxs + pbl * T}, tps + pbl * T, cs[tid], uwc, snap);
                 if (a.work) atomicAdd(&refined[rec.P - 1], 1u);
             }
         }
@@ -815,7 +843,9 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
 
 size_t refine_smem_bytes(const TableLayout& L, int topn) {
     const size_t pbs = (size_t)refine_pbs(L.T, topn);
-    return sizeof(CandSmem) * kRefineThreads + pbs * L.T * 16 + ((pbs * L.T + 15) & ~(size_t)15) + kRefineThreads * 4 +
+    const bool u8 = refine_u8(L.T);
+    return sizeof(CandSmem) * kRefineThreads + (u8 ? 256 * 4 : 0) + pbs * L.T * (u8 ? 4 : 16) + ((pbs * L.T + 15) & ~(size_t)15) +
+           kRefineThreads * 4 +
            (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
 }
 
@@ -845,7 +875,8 @@ cudaError_t configure_kernels(const TableLayout& L) {
     for (int i = 0; i < 3; i++) m[i] = std::max(m[i], need[i]);
     e = configure_search_kernels(m[0], m[1]);
     if (e != cudaSuccess) return e;
-    for (auto f : {k_refine<1>, k_refine<2>, k_refine<4>, k_refine<8>})
+    for (auto f : {k_refine<1, false>, k_refine<2, false>, k_refine<4, false>, k_refine<8, false>, k_refine<1, true>,
+                   k_refine<2, true>, k_refine<4, true>, k_refine<8, true>})
         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m[2])) != cudaSuccess) return e;
     return cudaSuccess;
 }
@@ -856,10 +887,17 @@ cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
     int grid = (npb + pbs - 1) / pbs;
     if (a.block_list) grid = std::min(grid, kListGridRefine);
     const size_t smem = refine_smem_bytes(a.L, cpb);
-    if (cpb == 1) k_refine<1><<<grid, kRefineThreads, smem, s>>>(a);
-    else if (cpb == 2) k_refine<2><<<grid, kRefineThreads, smem, s>>>(a);
-    else if (cpb == 4) k_refine<4><<<grid, kRefineThreads, smem, s>>>(a);
-    else k_refine<8><<<grid, kRefineThreads, smem, s>>>(a);
+    if (refine_u8(a.L.T)) {
+        if (cpb == 1) k_refine<1, true><<<grid, kRefineThreads, smem, s>>>(a);
+        else if (cpb == 2) k_refine<2, true><<<grid, kRefineThreads, smem, s>>>(a);
+        else if (cpb == 4) k_refine<4, true><<<grid, kRefineThreads, smem, s>>>(a);
+        else k_refine<8, true><<<grid, kRefineThreads, smem, s>>>(a);
+    } else {
+        if (cpb == 1) k_refine<1, false><<<grid, kRefineThreads, smem, s>>>(a);
+        else if (cpb == 2) k_refine<2, false><<<grid, kRefineThreads, smem, s>>>(a);
+        else if (cpb == 4) k_refine<4, false><<<grid, kRefineThreads, smem, s>>>(a);
+        else k_refine<8, false><<<grid, kRefineThreads, smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
