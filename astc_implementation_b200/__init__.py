@@ -73,7 +73,8 @@ class Pruning(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("enable", ctypes.c_uint32), ("max_partitionings", ctypes.c_uint32),
                 ("block_modes", ctypes.c_uint32), ("refine_candidates", ctypes.c_uint32), ("coverage", ctypes.c_float),
                 ("threshold", ctypes.c_float), ("reroute_error", ctypes.c_float), ("front_threads", ctypes.c_uint32),
-                ("refine_iterations", ctypes.c_uint32), ("single_partition_floor", ctypes.c_float)]
+                ("refine_iterations", ctypes.c_uint32), ("single_partition_floor", ctypes.c_float),
+                ("fallback_iterations", ctypes.c_uint32)]
 
 
 def load_library():
@@ -259,10 +260,11 @@ class ASTCEncoder:
 
     def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98,
                     threshold=0.5, reroute_error=8.0, front_threads=128, refine_iterations=3,
-                    single_partition_floor=0.0):
+                    single_partition_floor=0.0, fallback_iterations=3):
         """Proposal-search settings for later encodes of footprints with a network."""
         cfg = Pruning(ctypes.sizeof(Pruning), 1 if enable else 0, max_partitionings, block_modes, refine_candidates,
-                      coverage, threshold, reroute_error, front_threads, refine_iterations, single_partition_floor)
+                      coverage, threshold, reroute_error, front_threads, refine_iterations, single_partition_floor,
+                      fallback_iterations)
         _check(load_library().astcb200_set_pruning(self._ctx, ctypes.byref(cfg)), self._ctx)
 
     def pruning_stats(self):

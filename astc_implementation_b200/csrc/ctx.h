@@ -52,6 +52,7 @@ struct Pruning {
     float reroute_error = 8.0f;
     int front_threads = 128;
     int refine_iters = 3;
+    int fallback_iters = 3;  // refinement iterations of the full-search pass over the fallback list
     float p1_floor = 0.0f;  // per-texel weighted squared error (8-bit units) above which
                                  // a proposal-search block also takes the full search; 0: off
 };

@@ -129,6 +129,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     af.block_list = r.full; af.block_count = counts + 1;
     af.prev_err = r.full_err;
     af.slots = kSlotsPerBlock; af.topn = kNumCand;
+    af.refine_iters = pr.fallback_iters;  // the candidates' serial refinement chain sets this pass's duration
     af.pbrec = sc.pbrec + n * kMaxSlots;
     af.snaps = sc.snaps + n * kMaxSlots * kNumCand;
 
@@ -246,7 +247,7 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
                         cfg->refine_candidates == 0 || cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
                         !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f) ||
                         (cfg->front_threads && cfg->front_threads != 32 && cfg->front_threads != 64 && cfg->front_threads != 128) ||
-                        cfg->refine_iterations > 6 || !(cfg->single_partition_floor >= 0.0f)))
+                        cfg->refine_iterations > 6 || !(cfg->single_partition_floor >= 0.0f) || cfg->fallback_iterations > 6))
         return ASTCB200_BAD_ARG;
     Pruning& p = ctx->pruning;
     p.enable = cfg->enable != 0;
@@ -259,6 +260,7 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.front_threads = cfg->front_threads ? (int)cfg->front_threads : 128;
     p.refine_iters = cfg->struct_size >= sizeof(astcb200_pruning) && cfg->refine_iterations ? (int)cfg->refine_iterations : 3;
     p.p1_floor = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->single_partition_floor : 0.0f;
+    p.fallback_iters = cfg->fallback_iterations ? (int)cfg->fallback_iterations : 3;
     release_batches(ctx);  // captured graphs hold the previous settings
     return ASTCB200_OK;
 }

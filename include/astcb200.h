@@ -185,6 +185,9 @@ typedef struct astcb200_pruning {
                                    reference and the full-search pass run 6) */
     float single_partition_floor; /* blocks with proposed partitionings skip the single-partition
                                    candidate when its probability is below this (0 = never) */
+    uint32_t fallback_iterations; /* refinement iterations of the full-search pass over the
+                                   low-confidence and rerouted blocks, 1..6 (0 = 3; 6 makes that
+                                   pass the reference's full search) */
 } astcb200_pruning;
 /* Applies to later encodes of footprints that have a network (the others use the full search). */
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);

@@ -1825,8 +1825,9 @@ Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w, const 
     return s;
 }
 
-// compression_pipeline.cpp:359-519, for one block: P = 1..4, best candidate, best P.
-Sym encode_block(const Footprint& f, const InputBlock& blk, PBWork& w) {
+// compression_pipeline.cpp:359-519, for one block: P = 1..4, best candidate, best P
+// (iters: refinement iterations, 6 in the reference).
+Sym encode_block(const Footprint& f, const InputBlock& blk, PBWork& w, int iters = 6) {
     Sym best; std::memset(&best, 0, sizeof(best)); best.err = 1e30f;  // ERROR_CALC_DEFAULT (astc.h:77)
     InputBlock pbs[4];
     for (int P = 1; P <= 4; P++) {
@@ -1835,7 +1836,7 @@ Sym encode_block(const Footprint& f, const InputBlock& blk, PBWork& w) {
         else n = partition_search(f, blk, P, pbs, nullptr);
         const Sym* bc = nullptr; Sym cur[4];
         for (int i = 0; i < n; i++) {
-            cur[i] = process_pb(f, pbs[i], P, w);
+            cur[i] = process_pb(f, pbs[i], P, w, nullptr, NUM_CAND, iters);
             if (bc == nullptr || cur[i].err < bc->err) bc = &cur[i];
         }
         if (bc && bc->err < best.err) best = *bc;
@@ -2025,6 +2026,22 @@ int orc_encode(const uint8_t* rgba, int width, int height, int bx, int by, int t
     run_parallel(n, threads, [&](int i, PBWork& w) {
         InputBlock b; make_block(rgba, width, height, bx, by, i % nbx, i / nbx, b);
         Sym s = encode_block(f, b, w);
+        uint32_t words[ORC_SYMBOLIC_WORDS]; sym_to_words(s, words);
+        if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
+        sym_to_phys(f, words, out_blocks + (size_t)i * 16);
+    });
+    return 0;
+}
+
+int orc_encode_iters(const uint8_t* rgba, int width, int height, int bx, int by, int threads, int refine_iters,
+                     uint8_t* out_blocks, uint32_t* symbolic) {
+    if (!rgba || width <= 0 || height <= 0 || !valid_footprint(bx, by) || !out_blocks || refine_iters < 1) return -1;
+    const Footprint& f = *get_fp(bx, by);
+    CT();
+    int nbx = (width + bx - 1) / bx, nby = (height + by - 1) / by, n = nbx * nby;
+    run_parallel(n, threads, [&](int i, PBWork& w) {
+        InputBlock b; make_block(rgba, width, height, bx, by, i % nbx, i / nbx, b);
+        Sym s = encode_block(f, b, w, refine_iters);
         uint32_t words[ORC_SYMBOLIC_WORDS]; sym_to_words(s, words);
         if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
         sym_to_phys(f, words, out_blocks + (size_t)i * 16);

@@ -32,6 +32,11 @@ extern "C" {
 int orc_encode(const uint8_t* rgba, int width, int height, int bx, int by, int threads,
                uint8_t* out_blocks, uint32_t* symbolic);
 
+// orc_encode with `refine_iters` refinement iterations instead of the reference's 6 (the
+// proposal search's full-search pass over its fallback blocks runs fewer).
+int orc_encode_iters(const uint8_t* rgba, int width, int height, int bx, int by, int threads, int refine_iters,
+                     uint8_t* out_blocks, uint32_t* symbolic);
+
 // Runs the search for a list of blocks given as pre-split texel data (T texels of
 // 4 floats each, already scaled to 0..65536) and returns symbolic results.
 int orc_encode_blocks(const float* texels, int nblocks, int bx, int by, int threads,

@@ -115,7 +115,8 @@ def full_and_pruned(img, bx, by, net, **prune):
 def test_everything_routed_to_full_search_is_bit_exact():
     lay = proposal.Layout(4, 4)
     img = synth.make_texture(80, 52, 12)
-    full, full_sym, blocks, sym, stats = full_and_pruned(img, 4, 4, random_net(lay, 1), threshold=2.0, reroute_error=0.0)
+    full, full_sym, blocks, sym, stats = full_and_pruned(img, 4, 4, random_net(lay, 1), threshold=2.0, reroute_error=0.0,
+                                                         fallback_iterations=6)
     assert stats == (0, 20 * 13)
     assert np.array_equal(blocks, full) and np.array_equal(sym, full_sym)
 
@@ -167,29 +168,31 @@ def restricted_oracle(img, bx, by, picks, masks, topn, iters):
     return out, sym, found.astype(bool)
 
 
-def full_oracle(img, bx, by):
+def full_oracle(img, bx, by, iters=6):
     h, w = img.shape[:2]
     n = ((w + bx - 1) // bx) * ((h + by - 1) // by)
     out = np.zeros((n, 16), np.uint8)
     sym = np.zeros((n, 108), np.uint32)
-    assert _libs.oracle().orc_encode(_libs.ptr(np.ascontiguousarray(img)), w, h, bx, by, 0, _libs.ptr(out), _libs.ptr(sym)) == 0
+    assert _libs.oracle().orc_encode_iters(_libs.ptr(np.ascontiguousarray(img)), w, h, bx, by, 0, iters, _libs.ptr(out),
+                                           _libs.ptr(sym)) == 0
     return out, sym
 
 
 @pytest.mark.parametrize("bx,by,net_kind,prune", [
-    (4, 4, "shipped", dict(topn=2, iters=3)),
-    (6, 6, "shipped", dict(topn=2, iters=3)),
+    (4, 4, "shipped", dict(topn=2, iters=3, fb=3)),
+    (6, 6, "shipped", dict(topn=2, iters=3, fb=3)),
     (4, 4, "random", dict(max_partitionings=6, block_modes=8, refine_candidates=4, refine_iterations=6,
-                          coverage=0.999, threshold=1e-4, single_partition_floor=0.3, topn=4, iters=6)),
+                          coverage=0.999, threshold=1e-4, single_partition_floor=0.3, topn=4, iters=6,
+                          fallback_iterations=6, fb=6)),
     (6, 6, "random", dict(max_partitionings=3, block_modes=40, refine_candidates=1, refine_iterations=2,
-                          coverage=0.95, threshold=1e-3, topn=1, iters=2)),
+                          coverage=0.95, threshold=1e-3, fallback_iterations=1, topn=1, iters=2, fb=1)),
 ])
 def test_proposal_search_bit_exact_against_restricted_oracle(bx, by, net_kind, prune):
     """Given the selection the GPU made (routes, partitionings, block-mode masks), every
     block equals the CPU oracle's search restricted to those candidates; blocks routed to
     the full search, or left without a candidate, equal the oracle's full search."""
     prune = dict(prune)
-    topn, iters = prune.pop("topn"), prune.pop("iters")
+    topn, iters, fb = prune.pop("topn"), prune.pop("iters"), prune.pop("fb")
     lay = proposal.Layout(bx, by)
     net = proposal.load_weights(bx, by) if net_kind == "shipped" else random_net(lay, 11)
     w, h = 11 * bx + 3, 7 * by + 2  # ragged edges
@@ -203,7 +206,7 @@ def test_proposal_search_bit_exact_against_restricted_oracle(bx, by, net_kind, p
     route, picks, masks = enc.proposal_selection(img)
     enc.close()
     r_out, r_sym, found = restricted_oracle(img, bx, by, picks, masks, topn, iters)
-    f_out, f_sym = full_oracle(img, bx, by)
+    f_out, f_sym = full_oracle(img, bx, by, fb)  # the fallback's full search, fb refinement iterations
     prop = (route == 0) & found
     assert prop.sum() > 0.5 * len(route)
     assert np.array_equal(sym[prop], r_sym[prop]) and np.array_equal(blocks.reshape(-1, 16)[prop], r_out[prop])
@@ -218,7 +221,7 @@ def test_reroute_keeps_the_better_of_both_searches(bx, by):
     with the lower of the two errors, bit-identical to the search that produced it."""
     net = proposal.load_weights(bx, by)
     img = synth.make_texture(96, 72, 61)
-    prune = dict(max_partitionings=2, block_modes=8, refine_candidates=2, coverage=0.9, threshold=0.0)
+    prune = dict(max_partitionings=2, block_modes=8, refine_candidates=2, coverage=0.9, threshold=0.0, fallback_iterations=6)
     _, full_sym, _, prop_sym, stats0 = full_and_pruned(img, bx, by, net, reroute_error=0.0, **prune)
     _, _, blocks, both_sym, stats = full_and_pruned(img, bx, by, net, reroute_error=1e-9, **prune)
     n = full_sym.shape[0]
@@ -296,6 +299,8 @@ def test_pruning_settings_are_checked_and_applied():
         enc.set_pruning(True, refine_iterations=7)
     with pytest.raises(ab.ASTCError):
         enc.set_pruning(True, front_threads=48)
+    with pytest.raises(ab.ASTCError):
+        enc.set_pruning(True, fallback_iterations=7)
     enc.set_pruning(True, max_partitionings=4, coverage=1.01, threshold=0.0, reroute_error=0.0, single_partition_floor=2.0)
     sym = enc.encode_symbolic(img)
     stats = enc.pruning_stats()

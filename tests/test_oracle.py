@@ -122,3 +122,21 @@ def test_restricted_search_rejects_bad_candidates():
     bad[0, 2] = 1023                                                  # entry beyond the selected ones
     assert orc.orc_encode_restricted(*args(bad, 2, 3)) == -1
     assert orc.orc_encode_restricted(*args(picks, 2, 3, bx=12)) == -1  # more than 256 block modes
+
+
+def test_full_search_iteration_count():
+    """orc_encode_iters with the reference's 6 iterations is orc_encode; with fewer, every block's
+    error is at least the 6-iteration one (the first iterations are the same, and each candidate
+    keeps its best-so-far)."""
+    img = synth.make_texture(21, 14, 41)
+    h, w = img.shape[:2]
+    full_out, full_sym = _encode(img, 4, 4)
+    n = full_sym.shape[0]
+    for iters in (6, 3, 1):
+        out = np.zeros((n, 16), np.uint8)
+        sym = np.zeros((n, 108), np.uint32)
+        assert _libs.oracle().orc_encode_iters(_libs.ptr(img), w, h, 4, 4, 0, iters, _libs.ptr(out), _libs.ptr(sym)) == 0
+        if iters == 6:
+            assert np.array_equal(sym, full_sym) and np.array_equal(out, full_out.reshape(n, 16))
+        else:
+            assert (sym[:, 0].view(np.float32) >= full_sym[:, 0].view(np.float32)).all()
