@@ -365,9 +365,6 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
     return v;
 }
-__device__ __forceinline__ bool part_valid(int c, const Select& sel) {
-    return c == kClassP1 || (c < kPartClasses && (c & 1023) < sel.sel[c >> 10]);
-}
 
 // Monotone map of a finite float to an unsigned key (larger value, larger key).
 __device__ __forceinline__ uint32_t okey(float v) {
@@ -397,11 +394,10 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     int lc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) { lv[k] = -3.0e38f; lc[k] = 0x7FFFFFFF; }
-    for (int c = lane; c <= kClassP1; c += 32) {
-        if (!part_valid(c, sel)) continue;
+    for (int c = lane; c <= S.p1; c += 32) {
         const float v = z[c];
         mx = fmaxf(mx, v);
-        if (c < kPartClasses && v > lv[K - 1]) {  // a lane sees its classes in increasing order
+        if (c < S.p1 && v > lv[K - 1]) {  // a lane sees its classes in increasing order
             lv[K - 1] = v; lc[K - 1] = c;
 #pragma unroll
             for (int k = K - 1; k > 0; k--)
@@ -413,10 +409,9 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     }
     mx = warp_max(mx);
     float se = 0.0f;
-    for (int c = lane; c <= kClassP1; c += 32)
-        if (part_valid(c, sel)) se += __expf(z[c] - mx);
+    for (int c = lane; c <= S.p1; c += 32) se += __expf(z[c] - mx);
     se = warp_sum(se);
-    const float p1 = __expf(z[kClassP1] - mx) / se;
+    const float p1 = __expf(z[S.p1] - mx) / se;
     // the kmax best partitionings, merged from the lanes' lists
     uint16_t picks[kMaxProposals];
     float mass[kMaxProposals];
@@ -432,7 +427,7 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
             for (int j = 0; j < K - 1; j++) { lv[j] = lv[j + 1]; lc[j] = lc[j + 1]; }
             lv[K - 1] = -3.0e38f; lc[K - 1] = 0x7FFFFFFF;
         }
-        picks[n] = (uint16_t)ci;
+        picks[n] = (uint16_t)pick_of_class(S, (int)ci);
         acc += __expf(okey_value(best) - mx) / se;
         mass[n] = acc;
         n++;
@@ -471,7 +466,7 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     uint64_t* mk = r.masks + (size_t)pos * 4 * kMaskWords;
     for (int p = 0; p < 4; p++) {
         if (!((heads >> p) & 1)) continue;
-        const float* h = z + kHeadBase + p * S.nbm_pad;
+        const float* h = z + S.head_base + p * S.nbm_pad;
         float hv[2 * kMaskWords];
         uint32_t picked = 0;
 #pragma unroll

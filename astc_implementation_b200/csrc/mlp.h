@@ -4,11 +4,13 @@
 // The network maps one block's texels, normalised to [0,1] (RGBA8 / 255) and
 // rounded to bf16, through two hidden layers of 256 ReLU units to one logit
 // per class:
-//   [0, 3072)            partitionings: table entry e of P = 2, 3, 4 at (P-2)*1024 + e
-//                        (only entries below the footprint's selected count are classes)
-//   3072                 the single-partition block
-//   [3200 + p*nbm_pad, +nbm)  block modes (trial indices) for P = p + 1 partitions
-// padded to a multiple of 128 outputs.  Inputs are padded to a multiple of 16.
+//   [0, p1)              partitionings: the selected table entries e < sel[P-2] of P = 2, 3, 4
+//                        one count after another, entry e of P at part_base[P-2] + e
+//   p1                   the single-partition block (p1 = sel[0] + sel[1] + sel[2])
+//   [head_base + p*nbm_pad, +nbm)  block modes (trial indices) for P = p + 1 partitions,
+//                        head_base = p1 + 1 rounded up to a multiple of 32
+// padded to a multiple of 128 outputs.  Inputs are padded to a multiple of 16.  Outside
+// the network a partitioning is named (P - 2) << 10 | e (pick_of_class).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -19,9 +21,6 @@ namespace astcb200 {
 namespace mlp {
 
 constexpr int kHidden = 256;
-constexpr int kPartClasses = 3072;
-constexpr int kClassP1 = 3072;
-constexpr int kHeadBase = 3200;
 constexpr int kTileRows = 128;   // blocks per CTA of the inference kernel
 constexpr int kChunkN = 64;      // output columns per layer-3 MMA chunk
 constexpr int kOutAlign = 128;   // outputs are padded to a multiple of this
@@ -29,17 +28,36 @@ constexpr int kOutAlign = 128;   // outputs are padded to a multiple of this
 struct Shape {
     int k0, k0p;        // inputs (4 * texels) and padded to a multiple of 16
     int nbm, nbm_pad;   // block-mode classes per head and the head stride
+    int sel[3];         // selected table entries of P = 2, 3, 4
+    int part_base[3];   // their first classes
+    int p1;             // the single-partition class
+    int head_base;      // the first block-mode class
     int nout;           // outputs, padded to a multiple of kOutAlign
 };
 
-inline Shape shape_for(int texels, int nbm) {
+// sel3: the footprint's selected table entries of P = 2, 3, 4 (TableLayout::count_selected[1..3])
+inline Shape shape_for(int texels, int nbm, const uint32_t* sel3) {
     Shape s;
     s.k0 = 4 * texels;
     s.k0p = (s.k0 + 15) & ~15;
     s.nbm = nbm;
     s.nbm_pad = (nbm + 31) & ~31;
-    s.nout = (kHeadBase + 4 * s.nbm_pad + kOutAlign - 1) / kOutAlign * kOutAlign;
+    int o = 0;
+    for (int i = 0; i < 3; i++) { s.sel[i] = (int)sel3[i]; s.part_base[i] = o; o += s.sel[i]; }
+    s.p1 = o;
+    s.head_base = (s.p1 + 1 + 31) & ~31;
+    s.nout = (s.head_base + 4 * s.nbm_pad + kOutAlign - 1) / kOutAlign * kOutAlign;
     return s;
+}
+
+// The partitioning of class c < p1 as (P - 2) << 10 | table entry.
+__host__ __device__ inline int pick_of_class(const Shape& s, int c) {
+    const int q = c >= s.part_base[2] ? 2 : c >= s.part_base[1] ? 1 : 0;
+    return (q << 10) | (c - s.part_base[q]);
+}
+// Block-mode head (0..3 for P = 1..4) of partition class c <= p1.
+__host__ __device__ inline int head_of_class(const Shape& s, int c) {
+    return c == s.p1 ? 0 : 1 + (c >= s.part_base[2] ? 2 : c >= s.part_base[1] ? 1 : 0);
 }
 
 // Element index of (row n, column k) in the no-swizzle K-major layout the
@@ -68,7 +86,6 @@ struct Select {
     float threshold;   // the block takes the full search when P=1 plus the kmax best mass is below this
     int kbm;           // block modes per partition count in the masks (<= 64)
     float p1_floor;    // with proposals, P = 1 is searched only when its probability reaches this
-    int sel[3];        // selected table entries for P = 2, 3, 4 (valid classes)
 };
 
 // Output of the selection kernel for one chunk.

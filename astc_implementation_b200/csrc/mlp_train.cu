@@ -74,12 +74,8 @@ __global__ void __launch_bounds__(256) k_gemm(const float* __restrict__ A, const
 
 struct XentShape {
     int nout, nbm, head_stride, batch;
-    int sel[3];
+    mlp::Shape cls;  // class plan (p1, part_base, head_base)
 };
-
-__device__ __forceinline__ bool part_class(int c, const XentShape& s) {
-    return c == mlp::kClassP1 || (c < mlp::kPartClasses && (c & 1023) < s.sel[c >> 10]);
-}
 __device__ __forceinline__ float wmax(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
     return v;
@@ -101,28 +97,27 @@ __global__ void __launch_bounds__(128) k_xent(const float* __restrict__ Z, const
     const int pl = part_label[b], bl = bm_label[b];
     // partition head
     float mx = -3.0e38f;
-    for (int c = lane; c <= mlp::kClassP1; c += 32)
-        if (part_class(c, s)) mx = fmaxf(mx, z[c]);
+    const int p1 = s.cls.p1, hb = s.cls.head_base;
+    for (int c = lane; c <= p1; c += 32) mx = fmaxf(mx, z[c]);
     mx = wmax(mx);
     float se = 0.0f;
-    for (int c = lane; c <= mlp::kClassP1; c += 32)
-        if (part_class(c, s)) se += expf(z[c] - mx);
+    for (int c = lane; c <= p1; c += 32) se += expf(z[c] - mx);
     se = wsum(se);
-    for (int c = lane; c < mlp::kHeadBase; c += 32) {
+    for (int c = lane; c < hb; c += 32) {
         float v = 0.0f;
-        if (part_class(c, s)) v = (expf(z[c] - mx) / se - (c == pl ? 1.0f : 0.0f)) * inv_b;
+        if (c <= p1) v = (expf(z[c] - mx) / se - (c == pl ? 1.0f : 0.0f)) * inv_b;
         g[c] = v;
     }
     // block-mode head of the label's partition count
-    const int head = pl == mlp::kClassP1 ? 0 : (pl >> 10) + 1;
-    const int h0 = mlp::kHeadBase + head * s.head_stride;
+    const int head = mlp::head_of_class(s.cls, pl);
+    const int h0 = hb + head * s.head_stride;
     float hm = -3.0e38f;
     for (int c = lane; c < s.nbm; c += 32) hm = fmaxf(hm, z[h0 + c]);
     hm = wmax(hm);
     float hs = 0.0f;
     for (int c = lane; c < s.nbm; c += 32) hs += expf(z[h0 + c] - hm);
     hs = wsum(hs);
-    for (int c = mlp::kHeadBase + lane; c < s.nout; c += 32) {
+    for (int c = hb + lane; c < s.nout; c += 32) {
         float v = 0.0f;
         const int k = c - h0;
         if (k >= 0 && k < s.nbm) v = (expf(z[c] - hm) / hs - (k == bl ? 1.0f : 0.0f)) * inv_b;
@@ -179,10 +174,10 @@ int astcb200_train_gemm(const float* A, const float* B, float* C, int M, int N, 
 int astcb200_train_xent(const float* Z, uint32_t nout, const int32_t* part_label, const int32_t* bm_label, uint32_t batch,
                         uint32_t nbm, uint32_t head_stride, const uint32_t* sel3, float* dZ, float* loss_rows, void* stream) {
     if (!Z || !part_label || !bm_label || !sel3 || !dZ || !loss_rows || batch == 0) return ASTCB200_BAD_ARG;
-    if (nout < (uint32_t)mlp::kHeadBase + 4 * head_stride || nbm > head_stride) return ASTCB200_BAD_ARG;
     XentShape s;
+    s.cls = mlp::shape_for(0, (int)nbm, sel3);
+    if (nbm > head_stride || nout < (uint32_t)s.cls.head_base + 4 * head_stride) return ASTCB200_BAD_ARG;
     s.nout = (int)nout; s.nbm = (int)nbm; s.head_stride = (int)head_stride; s.batch = (int)batch;
-    for (int i = 0; i < 3; i++) s.sel[i] = (int)sel3[i];
     k_xent<<<(batch + 3) / 4, 128, 0, (cudaStream_t)stream>>>(Z, part_label, bm_label, s, dZ, loss_rows);
     return launch_status();
 }

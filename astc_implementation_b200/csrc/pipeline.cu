@@ -98,7 +98,6 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     mlp::Select sel;
     sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
     sel.p1_floor = pr.p1_floor;
-    for (int i = 0; i < 3; i++) sel.sel[i] = (int)ft->L.count_selected[i + 1];
     mlp::Routes r;
     r.counts = counts;
     r.pruned = sc.lists;
@@ -170,12 +169,12 @@ int astcb200_proposal_layout(uint8_t bx, uint8_t by, uint32_t* inputs, uint32_t*
     TableLayout L;
     std::vector<uint8_t> blob;
     if (!build_tables(bx, by, L, blob)) return ASTCB200_INVALID_FOOTPRINT;
-    const mlp::Shape s = mlp::shape_for(L.T, L.nbm);
+    const mlp::Shape s = mlp::shape_for(L.T, L.nbm, L.count_selected + 1);
     if (inputs) *inputs = s.k0;
     if (inputs_padded) *inputs_padded = s.k0p;
     if (outputs) *outputs = s.nout;
     if (block_modes) *block_modes = s.nbm;
-    if (head_base) *head_base = mlp::kHeadBase;
+    if (head_base) *head_base = s.head_base;
     if (head_stride) *head_stride = s.nbm_pad;
     if (sel3) for (int i = 0; i < 3; i++) sel3[i] = L.count_selected[i + 1];
     return ASTCB200_OK;
@@ -188,7 +187,7 @@ int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* w)
     const FootTables* ft = nullptr;
     int rc = get_tables(ctx, w->block_x, w->block_y, &ft);
     if (rc) return rc;
-    const mlp::Shape s = mlp::shape_for(ft->L.T, ft->L.nbm);
+    const mlp::Shape s = mlp::shape_for(ft->L.T, ft->L.nbm, ft->L.count_selected + 1);
     if (w->inputs != (uint32_t)s.k0 || w->hidden != (uint32_t)mlp::kHidden || w->outputs != (uint32_t)s.nout) {
         ctx->err = "network shape does not match astcb200_proposal_layout";
         return ASTCB200_BAD_ARG;
@@ -354,7 +353,6 @@ int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t
     mlp::Select sel;
     sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
     sel.p1_floor = pr.p1_floor;
-    for (int i = 0; i < 3; i++) sel.sel[i] = (int)ctx->cur->L.count_selected[i + 1];
     std::memset(route, 1, ctx->nblocks);
     std::memset(picks, 0, ctx->nblocks * 18 * sizeof(uint16_t));
     std::memset(masks, 0, ctx->nblocks * 4 * kMaskWords * sizeof(uint64_t));

@@ -25,7 +25,6 @@ import numpy as np
 from . import ASTCEncoder, _check, load_library
 
 HIDDEN = 256
-P1_CLASS = 3072
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 
 
@@ -38,6 +37,25 @@ class Layout:
         self.bx, self.by = bx, by
         self.inputs, self.inputs_padded, self.outputs, self.nbm, self.head_base, self.head_stride = (x.value for x in u)
         self.sel3 = tuple(int(v) for v in sel)
+        # classes: the selected partitionings of P = 2, 3, 4 one count after another, then the
+        # single-partition class p1, then the block-mode heads from head_base
+        self.part_base = (0, self.sel3[0], self.sel3[0] + self.sel3[1])
+        self.p1 = sum(self.sel3)
+
+    def part_class(self, P, entry):
+        """Class of table entry `entry` of partition count P = 2..4."""
+        return np.asarray(self.part_base)[np.asarray(P) - 2] + entry
+
+    def pick_of(self, c):
+        """(P - 2) << 10 | entry of partition class c < p1 (the encoder's name of a partitioning)."""
+        c = np.asarray(c)
+        q = (c >= self.part_base[1]).astype(np.int64) + (c >= self.part_base[2])
+        return (q << 10) | (c - np.asarray(self.part_base)[q])
+
+    def head_of(self, part):
+        """Block-mode head (0..3 for P = 1..4) of partition classes."""
+        part = np.asarray(part)
+        return np.where(part == self.p1, 0, 1 + (part >= self.part_base[1]).astype(np.int64) + (part >= self.part_base[2]))
 
 
 def bf16_round(x):
@@ -90,13 +108,15 @@ def _seed_to_entry(bx, by):
 def labels_from_symbolic(sym, bx, by):
     """(partition class, block-mode class, usable) per block from SymbolicBlock records
     (108 u32: [1] block mode, [2] partition count, [3] partition seed)."""
+    lay = Layout(bx, by)
     modes = _trial_modes(bx, by)
     trial_of_mode = np.full(2048, -1, np.int64)
     trial_of_mode[modes.astype(np.int64)] = np.arange(len(modes))
     pidx = _seed_to_entry(bx, by).astype(np.int64)
     pc = sym[:, 2].astype(np.int64)
     seed = sym[:, 3].astype(np.int64) & 1023
-    part = np.where(pc <= 1, P1_CLASS, (np.clip(pc, 2, 4) - 2) * 1024 + pidx[np.clip(pc, 2, 4) - 2, seed])
+    q = np.clip(pc, 2, 4) - 2
+    part = np.where(pc <= 1, lay.p1, np.asarray(lay.part_base)[q] + pidx[q, seed])
     bm = trial_of_mode[sym[:, 1].astype(np.int64) & 2047]
     usable = (sym[:, 0].view(np.float32) < 1e29) & (bm >= 0) & (pc >= 1) & (pc <= 4)
     return part.astype(np.int32), np.maximum(bm, 0).astype(np.int32), usable
@@ -266,15 +286,11 @@ class Trainer:
 
 
 def _accuracy_counts(z, part, bm, lay, topk):
-    valid = np.zeros(P1_CLASS + 1, bool)
-    for p in range(3):
-        valid[p * 1024: p * 1024 + lay.sel3[p]] = True
-    valid[P1_CLASS] = True
-    zp = np.where(valid[None, :], z[:, : P1_CLASS + 1], -np.inf)
+    zp = z[:, : lay.p1 + 1]
     top1 = zp.argmax(axis=1) == part
-    topk_idx = np.argsort(-zp[:, :P1_CLASS], axis=1)[:, :topk]
-    recall = (topk_idx == part[:, None]).any(axis=1) | (part == P1_CLASS)
-    heads = np.where(part == P1_CLASS, 0, (part >> 10) + 1)
+    topk_idx = np.argsort(-zp[:, : lay.p1], axis=1)[:, :topk]
+    recall = (topk_idx == part[:, None]).any(axis=1) | (part == lay.p1)
+    heads = lay.head_of(part)
     hz = np.stack([z[np.arange(len(z)), lay.head_base + heads * lay.head_stride + c] for c in range(lay.nbm)], axis=1)
     bm1 = hz.argmax(axis=1) == bm
     return np.array([top1.sum(), recall.sum(), bm1.sum()], np.float64)

@@ -12,18 +12,32 @@ mathematics of the network:
   training:  everything FP32/FP64, loss = CE(partition head) + CE(block-mode head of the
              label's partition count), gradients by backpropagation
 
-Output classes: [0, 3072) partitionings (P-2)*1024 + table entry (entries below the
-footprint's selected count only), 3072 the single-partition block, and from 3200 one
-head of `nbm` block modes per partition count P = 1..4, `head_stride` apart.
+Output classes (sel3 = the footprint's selected table entries of P = 2, 3, 4): the
+partitionings of P = 2, 3, 4 one count after another (entry e of P at part_base[P-2] + e),
+then the single-partition block p1 = sum(sel3), then from head_base (p1 + 1 rounded up to a
+multiple of 32) one head of `nbm` block modes per partition count P = 1..4, `head_stride`
+apart.
 
 Only tests/ may import this module; the product never does.
 """
 import numpy as np
 
 HIDDEN = 256
-PART = 3072
-P1 = 3072
-HEAD = 3200
+
+
+class Classes:
+    """The class plan of a footprint with selected table entries sel3 (P = 2, 3, 4)."""
+
+    def __init__(self, sel3):
+        s = [int(v) for v in sel3]
+        self.part_base = (0, s[0], s[0] + s[1])
+        self.p1 = s[0] + s[1] + s[2]
+        self.head_base = (self.p1 + 1 + 31) & ~31
+
+    def head_of(self, part):
+        """Block-mode head (0..3 for P = 1..4) of partition classes."""
+        part = np.asarray(part)
+        return np.where(part == self.p1, 0, 1 + (part >= self.part_base[1]).astype(np.int64) + (part >= self.part_base[2]))
 
 
 def bf16_round(x):
@@ -67,21 +81,6 @@ def infer(x, w):
     return (h2 @ w3.T + w["b3"]).astype(np.float32)
 
 
-def part_valid(sel3):
-    """Boolean mask over classes [0, 3073): valid partition classes."""
-    m = np.zeros(P1 + 1, bool)
-    for p in range(3):
-        m[p * 1024: p * 1024 + int(sel3[p])] = True
-    m[P1] = True
-    return m
-
-
-def head_of(part_label):
-    """Block-mode head (0..3 for P = 1..4) of a partition label."""
-    part_label = np.asarray(part_label)
-    return np.where(part_label == P1, 0, (part_label >> 10) + 1)
-
-
 def loss_and_grads(x, w, part_label, bm_label, nbm, head_stride, sel3):
     """FP64 forward and backward pass of the training loss (mean over the batch).
     Returns (loss_part, loss_bm, grads, dz) with grads keyed like w."""
@@ -96,19 +95,19 @@ def loss_and_grads(x, w, part_label, bm_label, nbm, head_stride, sel3):
     z = h2 @ W["w3"].T + W["b3"]
     B = x.shape[0]
     dz = np.zeros_like(z)
-    valid = part_valid(sel3)
-    zp = np.where(valid[None, :], z[:, : P1 + 1], -np.inf)
+    cl = Classes(sel3)
+    zp = z[:, : cl.p1 + 1]
     mx = zp.max(axis=1, keepdims=True)
     e = np.exp(zp - mx)
     se = e.sum(axis=1, keepdims=True)
     lp = np.log(se[:, 0]) + mx[:, 0] - z[np.arange(B), part_label]
     sp = e / se
     sp[np.arange(B), part_label] -= 1.0
-    dz[:, : P1 + 1] = sp / B
-    heads = head_of(part_label)
+    dz[:, : cl.p1 + 1] = sp / B
+    heads = cl.head_of(part_label)
     lb = np.zeros(B)
     for i in range(B):
-        h0 = HEAD + heads[i] * head_stride
+        h0 = cl.head_base + heads[i] * head_stride
         zh = z[i, h0: h0 + nbm]
         m = zh.max()
         eh = np.exp(zh - m)
@@ -131,23 +130,23 @@ def select(z, sel3, kmax, coverage, threshold, kbm, nbm, head_stride):
     """Selection rule of the proposal search for one block's logits z: returns
     (confident, proposed partition classes best first, block-mode sets per head)."""
     z = np.asarray(z, np.float64)
-    valid = part_valid(sel3)
-    zp = np.where(valid, z[: P1 + 1], -np.inf)
+    cl = Classes(sel3)
+    zp = z[: cl.p1 + 1]
     mx = zp.max()
     p = np.exp(zp - mx)
     p /= p.sum()
-    order = sorted((c for c in range(PART) if valid[c]), key=lambda c: (-z[c], c))[:kmax]
-    mass = p[P1] + np.cumsum([p[c] for c in order]) if order else np.array([])
-    confident = (p[P1] + sum(p[c] for c in order)) >= threshold
+    order = sorted(range(cl.p1), key=lambda c: (-z[c], c))[:kmax]
+    mass = p[cl.p1] + np.cumsum([p[c] for c in order]) if order else np.array([])
+    confident = (p[cl.p1] + sum(p[c] for c in order)) >= threshold
     used = len(order)
     for k, m in enumerate(mass):
         if m >= coverage:
             used = k + 1
             break
-    if p[P1] >= coverage:
+    if p[cl.p1] >= coverage:
         used = 0
     modes = []
     for h in range(4):
-        zh = z[HEAD + h * head_stride: HEAD + h * head_stride + nbm]
+        zh = z[cl.head_base + h * head_stride: cl.head_base + h * head_stride + nbm]
         modes.append(set(sorted(range(nbm), key=lambda c: (-zh[c], c))[: min(kbm, nbm)]))
     return bool(confident), order[:used], modes

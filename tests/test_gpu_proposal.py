@@ -44,7 +44,7 @@ def test_tensor_core_logits_match_oracle(bx, by, w, h):
     # rounding of the hidden layers to bf16 give differences of a few bf16 ulps
     assert err.max() <= 2e-2 * scale, err.max()
     assert err.mean() <= 1e-3 * scale, err.mean()
-    top = lambda a: np.argsort(-a[:, : mo.P1], axis=1)[:, :4]
+    top = lambda a: np.argsort(-a[:, : lay.p1], axis=1)[:, :4]
     assert (top(z) == top(ref)).mean() > 0.95
 
 
@@ -55,8 +55,8 @@ def test_training_gradients_match_oracle():
     img = synth.make_texture(64, 64, 77)
     X = mo.inputs(mo.block_rgba8(img, 4, 4), lay.inputs_padded)[:64]
     rng = np.random.default_rng(5)
-    part = np.concatenate([rng.integers(0, lay.sel3[0], 20), 1024 + rng.integers(0, lay.sel3[1], 20),
-                           2048 + rng.integers(0, lay.sel3[2], 20), np.full(4, mo.P1)]).astype(np.int32)
+    part = np.concatenate([rng.integers(0, lay.sel3[0], 20), lay.part_base[1] + rng.integers(0, lay.sel3[1], 20),
+                           lay.part_base[2] + rng.integers(0, lay.sel3[2], 20), np.full(4, lay.p1)]).astype(np.int32)
     bm = rng.integers(0, lay.nbm, 64).astype(np.int32)
     tr = proposal.Trainer(lay, {k: w[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3")}, batch=64)
     with torch.cuda.stream(tr.stream):
@@ -145,8 +145,8 @@ def test_proposal_search_obeys_the_selection(bx, by):
         if not conf:
             assert np.array_equal(sym[i], full_sym[i])
             continue
-        head = 0 if part[i] == mo.P1 else (part[i] >> 10) + 1
-        if part[i] != mo.P1 and part[i] not in picks:
+        head = int(lay.head_of(part[i]))
+        if part[i] != lay.p1 and part[i] not in picks:
             continue  # near-tied logits can order differently than the checker's float64 sort
         assert bm[i] in modes[head] or np.array_equal(sym[i], full_sym[i])
         n_checked += 1
