@@ -609,14 +609,19 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
         {
             const int pbl = tid / cpb, k = tid % cpb;
             const int li = grp * pbs + pbl;
-            int key = 0xFFFF;  // empty slots sort last (decimation modes are < 128)
+            int key = 0x3FFFFF;  // empty slots sort last
             if (pbl < pbs && li < npb) {
                 int slot, lb;
                 if (a.pb_list) pb_item(a, li, lb, slot);
                 else { slot = li / nb; lb = li % nb; }
                 my_lb = lb; my_slot = slot;
                 const PBRec& r = a.pbrec[lb * a.slots + slot];
-                if (k < (int)r.ncand) key = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
+                if (k < (int)r.ncand) {
+                    const int dm = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
+                    int fk = 0;
+                    for (int q = 0; q < 4; q++) { const int f = r.c[k].fmt[q]; fk = fk * 8 + (f == 0 ? 0 : f == 4 ? 1 : f == 6 ? 2 : f == 8 ? 3 : f == 10 ? 4 : f == 12 ? 5 : 6); }
+                    key = ((((int)r.P - 1) << 12 | fk) << 7) | dm;  // partition count, formats, decimation mode
+                }
                 if (r.ncand > 0) {
                     const int P = r.P;
                     const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
@@ -628,12 +633,13 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant
                     }
                 }
             }
-            keys[tid] = key * kRefineThreads + tid;  // unique keys: decimation mode, then position
+            keys[tid] = key * kRefineThreads + tid;  // unique keys: P, formats, decimation mode, then position
             cs[tid].pad = (uint32_t)(my_lb + 1) | ((uint32_t)my_slot << 27);  // item of staging position tid
         }
         __syncthreads();
-        // Thread tid takes the candidate of rank tid in decimation-mode order, so a
-        // warp's candidates mostly share loop bounds and table rows.
+        // Thread tid takes the candidate of rank tid in (partition count, endpoint formats,
+        // decimation mode) order, so a warp's candidates mostly take the same packing path
+        // and share loop bounds and table rows.
         int mine = 0;
         {
             const int kk = keys[tid];
