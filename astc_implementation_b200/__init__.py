@@ -259,7 +259,7 @@ class ASTCEncoder:
         _check(load_library().astcb200_set_proposal_net(self._ctx, ctypes.byref(net)), self._ctx)
 
     def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98,
-                    threshold=0.5, reroute_error=8.0, front_threads=128, refine_iterations=3,
+                    threshold=0.5, reroute_error=8.0, front_threads=0, refine_iterations=3,
                     single_partition_floor=0.0, fallback_iterations=3):
         """Proposal-search settings for later encodes of footprints with a network."""
         cfg = Pruning(ctypes.sizeof(Pruning), 1 if enable else 0, max_partitionings, block_modes, refine_candidates,

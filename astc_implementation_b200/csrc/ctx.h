@@ -50,7 +50,7 @@ struct Pruning {
     int kmax = 4, kbm = 16, topn = 2;
     float coverage = 0.98f, threshold = 0.5f;
     float reroute_error = 8.0f;
-    int front_threads = 128;
+    int front_threads = 0;  // 0: by footprint (64 up to 16 texels, else 128)
     int refine_iters = 3;
     int fallback_iters = 3;  // refinement iterations of the full-search pass over the fallback list
     float p1_floor = 0.0f;  // per-texel weighted squared error (8-bit units) above which

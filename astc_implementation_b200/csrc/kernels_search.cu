@@ -29,6 +29,19 @@ constexpr float ERR_DEFAULT = 1e37f;
 __constant__ int c_levels[21] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256};
 __constant__ int c_steps_for_quant[12] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32};
 __constant__ int c_free_bits[4] = {111, 97, 94, 91};  // pass07:5
+// pass10's format-class combinations (i | j << 2 | k << 4 | l << 6) for P = 2, 3, 4: every
+// tuple of classes 0..3 whose classes lie within one of each other (the pass's i, j, k, l
+// loops with their skips), grouped by the total i + j + k + l and, inside a total, in loop
+// order; c_combo_off[P - 2][c] .. [c + 1] delimits total c.
+__constant__ uint8_t c_combo[78] = {
+    0, 4, 1, 5, 9, 6, 10, 14, 11, 15,                                                      // P = 2
+    0, 16, 4, 1, 20, 17, 5, 21, 37, 25, 22, 41, 38, 26, 42, 58, 46, 43, 62, 59, 47, 63,     // P = 3
+    0, 64, 16, 4, 1, 80, 68, 20, 65, 17, 5, 84, 81, 69, 21, 85, 149, 101, 89, 86, 165, 153,  // P = 4
+    105, 150, 102, 90, 169, 166, 154, 106, 170, 234, 186, 174, 171, 250, 238, 190, 235, 187, 175,
+    254, 251, 239, 191, 255};
+__constant__ uint8_t c_combo_off[3][14] = {{0, 1, 3, 4, 6, 7, 9, 10, 10, 10, 10, 10, 10, 10},
+                                           {10, 11, 14, 17, 18, 21, 24, 25, 28, 31, 32, 32, 32, 32},
+                                           {32, 33, 37, 43, 47, 48, 52, 58, 62, 63, 67, 73, 77, 78}};
 
 enum { FMT_LUMINANCE = 0, FMT_LUMINANCE_ALPHA = 4, FMT_RGB_SCALE = 6, FMT_RGB = 8, FMT_RGB_SCALE_ALPHA = 10, FMT_RGBA = 12 };
 
@@ -678,16 +691,19 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         terms[t] = t0; terms[Tp + t] = t1; terms[2 * Tp + t] = t2; terms[3 * Tp + t] = t3; terms[4 * Tp + t] = t4;
     }
     __syncthreads();
-    // the decimation modes to run, in ascending order (warp 0); pass08 sums (role 5p + k)
+    // the decimation modes to run (warp 0): the decimated ones first, whose pass02 makes them
+    // the longest, so that the warps taking them in turn finish closer together; pass08
+    // sums (role 5p + k)
     if (bmm && warp == 0) {
         int n = 0;
-        for (int d0 = 0; d0 < ndm; d0 += 32) {
-            const int d = d0 + lane;
-            const bool f = d < ndm && ((flags[d >> 5] >> (d & 31)) & 1);
-            const uint32_t b = __ballot_sync(FULL, f);
-            if (f) list[n + __popc(b & ((1u << lane) - 1))] = (int16_t)d;
-            n += __popc(b);
-        }
+        for (int pass = 0; pass < 2; pass++)
+            for (int d0 = 0; d0 < ndm; d0 += 32) {
+                const int d = d0 + lane;
+                const bool f = d < ndm && ((flags[d >> 5] >> (d & 31)) & 1) && ((tb.dm(d).W == T) == (pass == 1));
+                const uint32_t b = __ballot_sync(FULL, f);
+                if (f) list[n + __popc(b & ((1u << lane) - 1))] = (int16_t)d;
+                n += __popc(b);
+            }
         __syncwarp();
         if (lane == 0) flags[0] = n;  // the flags are no longer needed
     }
@@ -901,48 +917,30 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
         }
     }
     // ---------------- pass10: best format combination per quant level and integer total
-    // (role q - 4; beside pass07, which does not read it)
-    if (P > 1 && role < 17) {
-        const int q = role + 4;
+    // One item per (quant level, integer total), beside pass07 (role-indexed): the format
+    // combinations with that total, in the order the one-thread loops visit them (i, j, k, l
+    // ascending, each format class within one of the others), so the first minimum is the same.
+    if (P > 1) {
         const int NC = P == 2 ? 7 : P == 3 ? 10 : 13;
-        for (int c = 0; c < NC; c++) M.combo_err[q][c] = ERR_DEFAULT;
-        for (int i = 0; i < 4; i++)
-            for (int j = 0; j < 4; j++) {
-                const int lo2 = min(i, j), hi2 = max(i, j);
-                if (hi2 - lo2 > 1) continue;
-                if (P == 2) {
-                    const float e = fminf(M.cerr[0][q][i] + M.cerr[1][q][j], 1e10f);
-                    if (e < M.combo_err[q][i + j]) {
-                        M.combo_err[q][i + j] = e;
-                        uint8_t* f = M.combo_fmt[q][i + j];
-                        f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = 0; f[3] = 0;
-                    }
-                    continue;
-                }
-                for (int k = 0; k < 4; k++) {
-                    const int lo3 = min(k, lo2), hi3 = max(k, hi2);
-                    if (hi3 - lo3 > 1) continue;
-                    if (P == 3) {
-                        const float e = fminf((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k], 1e10f);
-                        if (e < M.combo_err[q][i + j + k]) {
-                            M.combo_err[q][i + j + k] = e;
-                            uint8_t* f = M.combo_fmt[q][i + j + k];
-                            f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = M.cfmt[2][q][k]; f[3] = 0;
-                        }
-                        continue;
-                    }
-                    for (int l = 0; l < 4; l++) {
-                        const int lo4 = min(l, lo3), hi4 = max(l, hi3);
-                        if (hi4 - lo4 > 1) continue;
-                        const float e = fminf(((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k]) + M.cerr[3][q][l], 1e10f);
-                        if (e < M.combo_err[q][i + j + k + l]) {
-                            M.combo_err[q][i + j + k + l] = e;
-                            uint8_t* f = M.combo_fmt[q][i + j + k + l];
-                            f[0] = M.cfmt[0][q][i]; f[1] = M.cfmt[1][q][j]; f[2] = M.cfmt[2][q][k]; f[3] = M.cfmt[3][q][l];
-                        }
-                    }
-                }
+        for (int it = role; it < 17 * NC; it += kFrontThreads) {
+            const int q = 4 + it / NC, c = it - (it / NC) * NC;
+            float be = ERR_DEFAULT;
+            uint32_t bf = 0;
+            for (int o = c_combo_off[P - 2][c]; o < c_combo_off[P - 2][c + 1]; o++) {
+                const uint32_t cb = c_combo[o];
+                const int i = cb & 3, j = (cb >> 2) & 3, k = (cb >> 4) & 3, l = cb >> 6;
+                float e;
+                if (P == 2) e = fminf(M.cerr[0][q][i] + M.cerr[1][q][j], 1e10f);
+                else if (P == 3) e = fminf((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k], 1e10f);
+                else e = fminf(((M.cerr[0][q][i] + M.cerr[1][q][j]) + M.cerr[2][q][k]) + M.cerr[3][q][l], 1e10f);
+                if (e < be) { be = e; bf = cb; }
             }
+            M.combo_err[q][c] = be;
+            uint8_t* f = M.combo_fmt[q][c];
+            f[0] = M.cfmt[0][q][bf & 3]; f[1] = M.cfmt[1][q][(bf >> 2) & 3];
+            f[2] = P > 2 ? M.cfmt[2][q][(bf >> 4) & 3] : 0;
+            f[3] = P > 3 ? M.cfmt[3][q][bf >> 6] : 0;
+        }
     }
     if (bmm) {
         // The proposal search's few block modes, in groups that fit the buffer: the quantised

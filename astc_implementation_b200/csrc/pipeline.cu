@@ -114,7 +114,8 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     ap.block_list = r.pruned; ap.block_count = counts;
     ap.prop = r.prop; ap.bm_mask = r.masks;
     ap.slots = 1 + pr.kmax; ap.topn = pr.topn;
-    ap.front_threads = pr.front_threads;
+    // small blocks: two warps per partitioned block keep twice as many of them resident
+    ap.front_threads = pr.front_threads ? pr.front_threads : (ft->L.T <= 16 ? 64 : 128);
     ap.refine_iters = pr.refine_iters;
     ap.reroute_list = r.full; ap.reroute_count = counts + 1;  // blocks left without a candidate
     ap.pb_list = r.pb_list; ap.pb_count = counts + 2; ap.pb_stride = r.pb_stride;
@@ -256,7 +257,7 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.coverage = cfg->coverage;
     p.threshold = cfg->threshold;
     p.reroute_error = cfg->reroute_error;
-    p.front_threads = cfg->front_threads ? (int)cfg->front_threads : 128;
+    p.front_threads = (int)cfg->front_threads;
     p.refine_iters = cfg->struct_size >= sizeof(astcb200_pruning) && cfg->refine_iterations ? (int)cfg->refine_iterations : 3;
     p.p1_floor = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->single_partition_floor : 0.0f;
     p.fallback_iters = cfg->fallback_iterations ? (int)cfg->fallback_iterations : 3;

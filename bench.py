@@ -9,7 +9,8 @@ search.  The metric is Mtexel/s over both encodes.
               stream around exactly K steps, max over ranks; the L2 is flushed
               (512 MiB memset) before every step inside the timed region.
   e2e         the same steps through the public host API (ASTCEncoder.encode:
-              host RGBA8 in, host blocks out, copies inside the timed region).
+              host RGBA8 in, host blocks out, from and to pinned host memory,
+              copies inside the timed region).
   roofline    the dominant kernel's modelled FP32 operations (flop_model.py)
               over its CUDA-event time, against this GPU's FP32 FMA peak
               measured by astcb200_fp32_peak.
@@ -485,12 +486,14 @@ def main():
     prop_psnr = psnrs() if use_prop and full_psnr else None
     routes = [e.pruning_stats() for e in encs] if use_prop else None
 
-    # e2e through the public host API, same method
+    # e2e through the public host API, same method: inputs from and outputs to pinned host memory
     host_steps = max(1, min(args.steps, 3))
+    pin_imgs = [torch.from_numpy(im.reshape(-1)).pin_memory().numpy() for im in imgs]
+    pin_outs = [torch.empty(e.numBlocks * 16, dtype=torch.uint8).pin_memory().numpy() for e in encs]
     t_e2e = time.perf_counter()
     for i in range(host_steps):
-        for e in encs:
-            e.encode(imgs[i % 4])
+        for k, e in enumerate(encs):
+            e.encode(pin_imgs[i % 4], pin_outs[k])
     e2e, _ = job_rate(texels_per_step() * host_steps, 1000.0 * (time.perf_counter() - t_e2e), dist, "cuda")
     h2d = SIZE * SIZE * 4 * len(FOOTPRINTS)
     d2h = sum(blocks_of(bx, by) * 16 for bx, by in FOOTPRINTS)

@@ -180,7 +180,8 @@ typedef struct astcb200_pruning {
                                    B 0.2475, A 1) also takes the full search, and the better of
                                    the two results is kept; 0 disables */
     uint32_t front_threads;     /* threads per CTA of the proposal pass's front kernel: 32, 64 or
-                                   128 (0 = 128); results do not depend on it */
+                                   128 (0 = 64 for blocks of up to 16 texels, else 128); results
+                                   do not depend on it */
     uint32_t refine_iterations; /* refinement iterations of the proposal pass, 1..6 (0 = 3; the
                                    reference and the full-search pass run 6) */
     float single_partition_floor; /* blocks with proposed partitionings skip the single-partition
