@@ -111,6 +111,8 @@ def load_library():
         "astcb200_set_proposal_net": (I32, [P, ctypes.POINTER(ProposalNet)]),
         "astcb200_set_pruning": (I32, [P, ctypes.POINTER(Pruning)]),
         "astcb200_pruning_stats": (I32, [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+        "astcb200_decode_device": (I32, [U32, U32, U32, U32, P, P, P]),
+        "astcb200_decode_error_device": (I32, [U32, U32, U32, U32, P, P, P, P]),
         "astcb200_proposal_logits": (I32, [P, P, P, SZ]),
         "astcb200_proposal_selection": (I32, [P, P, P, P, P, SZ]),
         "astcb200_train_gemm": (I32, [P, P, P, I32, I32, I32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
@@ -339,6 +341,24 @@ def decode(block_x, block_y, dim_x, dim_y, blocks):
     out = np.empty((dim_y, dim_x, 4), np.uint8)
     _check(lib.astcb200_decode(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, _ptr(out)))
     return out
+
+
+def decode_device(block_x, block_y, dim_x, dim_y, d_blocks, d_rgba8, stream=0):
+    """GPU decode between device buffers (pointers as integers), queued on `stream`;
+    the same texels as decode()."""
+    _check(load_library().astcb200_decode_device(block_x, block_y, dim_x, dim_y, d_blocks, d_rgba8, stream))
+
+
+def decode_error_device(block_x, block_y, dim_x, dim_y, d_blocks, d_ref_rgba8, d_sse, stream=0):
+    """GPU decode compared with a reference image: writes the per-channel sums of squared
+    differences (4 x uint64) to device memory d_sse, queued on `stream`."""
+    _check(load_library().astcb200_decode_error_device(block_x, block_y, dim_x, dim_y, d_blocks, d_ref_rgba8, d_sse, stream))
+
+
+def psnr_from_sse(sse, dim_x, dim_y):
+    """PSNR over all RGBA channels from decode_error_device's four sums (same as psnr())."""
+    tot = float(sum(int(v) for v in sse))
+    return float("inf") if tot == 0 else 10.0 * np.log10(255.0 * 255.0 * 4.0 * dim_x * dim_y / tot)
 
 
 def encode_noalloc(device, d_rgba8, width, height, block_x, block_y, d_out_blocks, stream=0):

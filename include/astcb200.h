@@ -239,6 +239,19 @@ int astcb200_store_image(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uin
  * (dim_x*dim_y*4 bytes, UNORM8 with round-to-nearest from the 16-bit result). */
 int astcb200_decode(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
                     const uint8_t* blocks, size_t blocks_len, uint8_t* rgba8_out);
+/* The same decoder on the GPU (no reference counterpart), between device buffers on the
+ * current device, queued on cuda_stream: d_blocks holds the image's blocks in raster
+ * order, d_rgba8 (4-byte aligned) receives dim_x*dim_y RGBA8 texels, exactly the texels
+ * astcb200_decode gives. */
+int astcb200_decode_device(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
+                           const uint8_t* d_blocks, uint8_t* d_rgba8, void* cuda_stream);
+/* Decode and compare on the GPU without writing the image: d_sse[0..3] (device) receives,
+ * per channel R, G, B, A, the sum over texels of the squared difference between the
+ * decoded texels and the reference image d_ref_rgba8 (4-byte aligned).  PSNR over all
+ * channels is 10 log10(255^2 * 4 * dim_x * dim_y / (d_sse[0] + ... + d_sse[3])). */
+int astcb200_decode_error_device(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
+                                 const uint8_t* d_blocks, const uint8_t* d_ref_rgba8, uint64_t* d_sse,
+                                 void* cuda_stream);
 
 /* Device milliseconds spent in each of the four kernels (partition search, front,
  * refine, select/pack) by the last encode call, summed over chunks; needs
