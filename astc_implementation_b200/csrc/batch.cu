@@ -44,6 +44,7 @@ namespace {
 struct Group {
     const FootTables* ft;
     uint32_t first_seg, nsegs, nblocks;
+    bool full_only;  // textures below mlp::kMinProposalTexels: the full search
 };
 
 struct Plan {
@@ -75,14 +76,17 @@ int make_plan(astcb200_ctx* ctx, const astcb200_texture* tex, uint32_t n, bool d
         const std::pair<int, int> fp(t.block_x, t.block_y);
         if (std::find(feet.begin(), feet.end(), fp) == feet.end()) feet.push_back(fp);
     }
-    for (const auto& fp : feet) {
-        Group g{nullptr, (uint32_t)p.segs.size(), 0, 0};
+    // one queue per footprint and texture class (small textures take the full search)
+    for (const auto& fp : feet)
+      for (int small = 0; small < 2; small++) {
+        Group g{nullptr, (uint32_t)p.segs.size(), 0, 0, small == 1};
         int rc = get_tables(ctx, fp.first, fp.second, &g.ft);
         if (rc) return rc;
         uint64_t base = 0;
         for (uint32_t i = 0; i < n; i++) {
             const astcb200_texture& t = tex[i];
             if (t.block_x != fp.first || t.block_y != fp.second) continue;
+            if (((uint64_t)t.width * t.height < (uint64_t)mlp::kMinProposalTexels) != (small == 1)) continue;
             TexSeg s;
             s.img = t.rgba8; s.out = t.out_blocks;
             s.width = (int)t.width; s.height = (int)t.height;
@@ -94,10 +98,11 @@ int make_plan(astcb200_ctx* ctx, const astcb200_texture* tex, uint32_t n, bool d
             p.tex_of.push_back(i);
         }
         g.nsegs = (uint32_t)p.segs.size() - g.first_seg;
+        if (g.nsegs == 0) continue;
         g.nblocks = (uint32_t)base;
         p.max_group_blocks = std::max(p.max_group_blocks, g.nblocks);
         p.groups.push_back(g);
-    }
+      }
     return ASTCB200_OK;
 }
 
@@ -161,7 +166,7 @@ int enqueue(astcb200_ctx* ctx, const Plan& p, cudaStream_t s, uint32_t chunk, ui
             a.nsegs = (int)g.nsegs;
             a.block_first = (int)first;
             a.nblocks = (int)std::min<uint32_t>(chunk, g.nblocks - first);
-            int rc = enqueue_chunk(ctx, a, g.ft, ctx->bscratch[k], st[k], nullptr, nullptr, &n);
+            int rc = enqueue_chunk(ctx, a, g.ft, ctx->bscratch[k], st[k], nullptr, nullptr, &n, g.full_only);
             if (rc) return rc;
         }
     }

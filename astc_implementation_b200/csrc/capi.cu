@@ -105,7 +105,8 @@ int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t
         a.block_first = (int)first;
         a.nblocks = (int)std::min<uint32_t>(ctx->chunk, ctx->nblocks - first);
         if ((rc = enqueue_chunk(ctx, a, ctx->cur, ctx->scratch, s, timing ? &ctx->stage_ev[(size_t)E * c] : nullptr,
-                                timing ? &ctx->stage_kind[(size_t)kStageIntervals * c] : nullptr, &n)))
+                                timing ? &ctx->stage_kind[(size_t)kStageIntervals * c] : nullptr, &n,
+                                (uint64_t)ctx->width * ctx->height < (uint64_t)mlp::kMinProposalTexels)))
             return rc;
     }
     if (launches) *launches = n;

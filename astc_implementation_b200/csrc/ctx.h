@@ -135,8 +135,9 @@ int begin_routes(astcb200_ctx* ctx, size_t chunks);
 constexpr int kStageIntervals = 9;
 // Queues the search of one chunk (base: addressing, block_first, nblocks) on s; ev and
 // kinds, when not null, receive kStageIntervals + 1 events and the launches' stages.
+// full_only: the full search even when the footprint has a network (small textures).
 int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* ft, Scratch& sc, cudaStream_t s,
-                  cudaEvent_t* ev, int8_t* kinds, uint32_t* launches);
+                  cudaEvent_t* ev, int8_t* kinds, uint32_t* launches, bool full_only = false);
 void free_scratch(Scratch& sc);
 void release_batches(astcb200_ctx* ctx);
 

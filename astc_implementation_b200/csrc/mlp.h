@@ -103,6 +103,10 @@ struct Routes {
 };
 
 constexpr int kRouteCounters = 8;  // ints per chunk: routes, then partitioned-block counts, padding
+// Textures of fewer texels take the (reference's) full search even with a network: their
+// blocks are mostly edge-clamped copies of a few texels, unlike what the networks learned
+// from, and searching them fully costs next to nothing.
+constexpr int kMinProposalTexels = 1024;
 
 constexpr int kMlpSmemBytes = 200704 + 1024 + 1024;  // operands and staging, barriers, alignment slack
 

@@ -55,7 +55,7 @@ int begin_routes(astcb200_ctx* ctx, size_t chunks) {
 }
 
 int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* ft, Scratch& sc, cudaStream_t s,
-                  cudaEvent_t* ev, int8_t* kinds, uint32_t* launches) {
+                  cudaEvent_t* ev, int8_t* kinds, uint32_t* launches, bool full_only) {
     KernelArgs a = base;
     a.tables = ft->d;
     a.L = ft->L;
@@ -77,7 +77,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         return ASTCB200_OK;
     };
     int rc;
-    const NetDev* nd = net_for(ctx, ft);
+    const NetDev* nd = full_only ? nullptr : net_for(ctx, ft);
     if (!nd) {
         a.slots = kSlotsPerBlock;
         a.topn = kNumCand;
@@ -357,6 +357,7 @@ int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t
     std::memset(route, 1, ctx->nblocks);
     std::memset(picks, 0, ctx->nblocks * 18 * sizeof(uint16_t));
     std::memset(masks, 0, ctx->nblocks * 4 * kMaskWords * sizeof(uint64_t));
+    if ((uint64_t)ctx->width * ctx->height < (uint64_t)mlp::kMinProposalTexels) return ASTCB200_OK;  // full search
     std::vector<int> lst(chunk);
     std::vector<PropPicks> pp(chunk);
     std::vector<uint64_t> mk(chunk * 4 * kMaskWords);

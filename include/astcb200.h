@@ -174,7 +174,9 @@ typedef struct astcb200_pruning {
     uint32_t block_modes;       /* block modes evaluated per partition count, at most 64 */
     uint32_t refine_candidates; /* refinement candidates per partitioned block, at most 8 */
     float coverage;             /* stop proposing once P=1 plus the proposed probability reaches this */
-    float threshold;            /* full search when P=1 plus the best max_partitionings carry less */
+    float threshold;            /* full search when P=1 plus the best max_partitionings carry less
+                                   (textures of fewer than 1024 texels always take the full search,
+                                   with the reference's 6 refinement iterations) */
     float reroute_error;        /* a block whose proposal-search result has a larger per-texel error
                                    (weighted squared, 8-bit units; weights R 0.675, G 1.3275,
                                    B 0.2475, A 1) also takes the full search, and the better of

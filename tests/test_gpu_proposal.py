@@ -215,6 +215,30 @@ def test_proposal_search_bit_exact_against_restricted_oracle(bx, by, net_kind, p
         assert ((picks[:, 1] & 1) == 1)[route == 0].any()  # the P = 1 skip is exercised
 
 
+def test_small_textures_take_the_full_search():
+    """Textures of fewer than 1024 texels are encoded by the reference's full search (6
+    refinement iterations) even with a network and pruning enabled, alone or in a batch."""
+    tex = [(synth.make_texture(w, h, 70 + w), bx) for (w, h), bx in [((3, 2), 4), ((1, 3), 6), ((31, 30), 4), ((20, 17), 6)]]
+    big = (synth.make_texture(40, 30, 9), 4)  # 1200 texels: the proposal search
+    enc = ab.ASTCEncoder(device=0)
+    for bx in (4, 6):
+        enc.set_proposal_net(proposal.load_weights(bx, bx))
+    enc.set_pruning(True)
+    outs = enc.encode_batch([(img, bx, bx) for img, bx in tex + [big]])
+    for (img, bx), out in zip(tex, outs):
+        h, w = img.shape[:2]
+        ref, _ = full_oracle(img, bx, bx, 6)
+        enc.secondaryInit(w, h, bx, bx)
+        assert np.array_equal(enc.encode(img).reshape(-1, 16), ref)
+        assert np.array_equal(out.reshape(-1, 16), ref)
+        assert enc.pruning_stats() == (0, 0)  # no proposal pass ran
+    img, bx = big
+    enc.secondaryInit(40, 30, bx, bx)
+    enc.encode(img)
+    assert enc.pruning_stats()[0] > 0
+    enc.close()
+
+
 @pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
 def test_reroute_keeps_the_better_of_both_searches(bx, by):
     """With every proposal-search block also sent to the full search, each block ends
