@@ -302,13 +302,15 @@ def run_combined(args):
         torch.cuda.synchronize()
         return t0.elapsed_time(t1) / steps
 
-    def quality():
+    sse = torch.zeros(4, dtype=torch.int64, device="cuda")
+
+    def quality():  # decoded and compared on the GPU (astcb200_decode_error_device)
         q = []
         k = 0
         for fp in (6, 4):
             for d, w, h in levels:
-                img = d.cpu().numpy().reshape(h, w, 4)
-                q.append(ab.psnr(ab.decode(fp, fp, w, h, outs[k].cpu().numpy()), img))
+                ab.decode_error_device(fp, fp, w, h, outs[k].data_ptr(), d.data_ptr(), sse.data_ptr(), stream.cuda_stream)
+                q.append(ab.psnr_from_sse(sse.cpu().numpy().astype(np.uint64), w, h))
                 k += 1
         return np.array(q)
 
@@ -459,11 +461,16 @@ def main():
         torch.cuda.synchronize()
         return t0.elapsed_time(t1), stage_ms, stage_n, work
 
-    def psnrs():
+    sse = torch.zeros(4, dtype=torch.int64, device="cuda")
+
+    def psnrs():  # encoded, decoded and compared on the GPU (astcb200_decode_error_device)
         out = []
         for k, (bx, by) in enumerate(FOOTPRINTS):
-            for im in imgs:
-                out.append(ab.psnr(ab.decode(bx, by, SIZE, SIZE, encs[k].encode(im)), im))
+            for i in range(len(imgs)):
+                encs[k].encode_device(d_imgs[i].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
+                ab.decode_error_device(bx, by, SIZE, SIZE, outs[k].data_ptr(), d_imgs[i].data_ptr(), sse.data_ptr(),
+                                       stream.cuda_stream)
+                out.append(ab.psnr_from_sse(sse.cpu().numpy().astype(np.uint64), SIZE, SIZE))
         return out
 
     # the full search on the same images: its speed and quality are the reference point
