@@ -40,7 +40,7 @@ __device__ __forceinline__ int32_t shl1(int32_t v) { return (int32_t)((uint32_t)
 
 // ------------------------------------------------------------ pass14 colour endpoint packing
 struct Packer {
-    const uint8_t* cu2u;  // [17][512]
+    const uint8_t* cu2u;  // [17][512], then [17] deviation bounds
     __device__ int32_t tab(uint32_t q, int32_t idx) const { return cu2u[(q - 4) * 512 + idx]; }
     __device__ float enc_err(float4 u0, float4 u1, I4 q0, I4 q1) const {
         const float4 e0 = u0 - make_float4((float)q0.x, (float)q0.y, (float)q0.z, (float)q0.w);
@@ -121,10 +121,26 @@ struct Packer {
         o0 = c1i; o1 = c0i;
         return true;
     }
+    // The reference's loop nudges the endpoints 0.2 apart per step until their quantised
+    // channel sums no longer cross.  A quantised channel is at most dev(q) from its rounded
+    // input (the table's bound), so while the rounded sums are more than 6 * dev(q) apart
+    // no step can end the loop; those sums only move towards each other, so the steps
+    // before the first one that can end it only move the endpoints (the same float
+    // operations in the same order), and the lookups start there.
     __device__ void quant_rgb(float4 c0, float4 c1, I4& o0, I4& o1, uint32_t q) const {
         I4 c0i, c1i;
         const float4 nudge = mk(0.2f);
-        for (int it = 0; it < 4096; it++) {  // ends once c0 <= 0 and c1 >= 255 at the latest (< 1300 steps)
+        const int lim = 6 * (int)cu2u[17 * 512 + (q - 4)];
+        int it = 0;
+#pragma unroll 1
+        for (; it < 4095; it++) {
+            const int s0 = (max(f2i(rintf(c0.x)), 0) + max(f2i(rintf(c0.y)), 0)) + max(f2i(rintf(c0.z)), 0);
+            const int s1 = (min(f2i(rintf(c1.x)), 255) + min(f2i(rintf(c1.y)), 255)) + min(f2i(rintf(c1.z)), 255);
+            if (s0 - s1 <= lim) break;
+            c0 = c0 - nudge;
+            c1 = c1 + nudge;
+        }
+        for (; it < 4096; it++) {  // ends once c0 <= 0 and c1 >= 255 at the latest (< 1300 steps)
             I4 c0q = ivec(rnev(c0));
             c0q = {max(c0q.x, 0), max(c0q.y, 0), max(c0q.z, 0), max(c0q.w, 0)};
             c0i = q3flt(q, c0q, c0);
@@ -578,9 +594,10 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
 
 // CPB: candidate threads per partitioned block (refine_cpb of the launch's top-N), a
 // template parameter so that the full search's instance (8) keeps constant indexing.
-// U8: texels staged as RGBA8 (refine_u8).
+// U8: texels staged as RGBA8 (refine_u8).  Registers are capped for five resident CTAs
+// (the packer's call would otherwise raise the whole kernel's allocation).
 template <int CPB, bool U8>
-__global__ void __launch_bounds__(kRefineThreads) k_refine(const __grid_constant__ KernelArgs a) {
+__global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int T = a.L.T;
     constexpr int cpb = CPB;
