@@ -365,11 +365,12 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_partition_search(const __
 struct FrontLayout {
     int px, w, wes, tp, dec, lo, hi, scratch, bm_err, bm_bits, ccr_tot, ccr_q, ccr_fmt, qf, misc, dml, bml, total;
 };
-constexpr int kScratchPerWarp = 144 * 4 + 64 * 4 + 16 * 4 + 16 * 20;
-// passes 02-05 with a half-warp per decimation mode (up to 16 texels): inf[16], smp[16],
-// ang[16], then the pass05 keys and minidx as in the warp layout
-constexpr int kScratchPerHalf = 448;
-static_assert(2 * kScratchPerHalf <= kScratchPerWarp && 48 * 4 + 16 * 8 + 16 * 4 <= kScratchPerHalf, "half-warp scratch");
+
+// Scratch of passes 02-05 per half-warp: the pass03 table indices [64], angular offsets
+// [16], pass05 keys [16] (u64) and minidx [16].  pass02's infilled weights (T floats per
+// half-warp) go to pass07's buffer, unused between pass08's sums and pass07.
+constexpr int kDmScratchHalf = 64 * 4 + 16 * 4 + 16 * 8 + 16 * 4;
+constexpr int kDmScratchPerWarp = 2 * kDmScratchHalf;
 
 struct FrontMisc {
     float4 avg[4], dir[4], ep0[4], ep1[4];
@@ -400,6 +401,7 @@ __host__ __device__ inline int front_layout_qf_floats(int T, int max_w, int nt, 
     const int Tp = (T + 3) & ~3;
     int f = list ? kListGroup * (max_w + Tp) : max_w * nt;
     if (f < 5 * Tp) f = 5 * Tp;
+    if (f < (nt / 32) * 2 * T) f = (nt / 32) * 2 * T;  // pass02's infill, two modes per warp
     return f;
 }
 __host__ __device__ inline int take16(int& o, int bytes) { const int r = o; o = (o + bytes + 15) & ~15; return r; }
@@ -413,7 +415,7 @@ __host__ __device__ inline FrontLayout front_layout(int T, int ndm, int nbm, int
     f.dec = take16(o, ndm * 64 * 4);
     f.lo = take16(o, ndm * 8 * 4);
     f.hi = take16(o, ndm * 8 * 4);
-    f.scratch = take16(o, (nt / 32) * kScratchPerWarp);
+    f.scratch = take16(o, (nt / 32) * kDmScratchPerWarp);
     f.bm_err = take16(o, nbm * 4);
     f.bm_bits = take16(o, nbm * 4);
     f.ccr_tot = take16(o, nbm * 4);
@@ -461,161 +463,164 @@ __device__ __forceinline__ int bm_quant_weight(const Tabs& tb, const BmQuant& s,
     return v;
 }
 
-// Passes 02-05 for the decimation modes of a partitioned block, one group of G lanes per
-// mode.  Blocks of up to 16 texels (and so up to 16 weights and 12 angular steps) take a
-// half-warp per mode (G = 16), each half with its own scratch; larger blocks a warp.
-// Every lane of a warp runs the same number of loop trips (a half without a mode idles),
-// so the warp-wide __syncwarp()s are reached by all of its lanes.
-template <int G, int kFrontWarps>
+// pass02 of one decimation mode by a half-warp (lane gl of 16): the ideal decimated
+// weights dw, then for decimated modes the infill and the one-step correction.  Every lane
+// of the warp takes the syncs (both halves run this together, each on its own mode).
+__device__ __forceinline__ void pass02_mode(const Tabs& tb, int T, int m, const DevDm& dmi, int W, bool act, int gl, float* inf,
+                                            const float* iw, const float* wes, bool is_const, float* dw) {
+    if (W == T || !act) {
+        for (int w = gl; w < W; w += 16) dw[w] = iw[w];
+    } else {
+        for (int w = gl; w < W; w += 16) {
+            const int n = tb.wt_count(m, w);
+            float v = 0.0f;
+            if (n) {
+                const int base = dmi.wt_base + tb.wt_start(m, w);
+                float ws = 0.0f, tc = 1e-10f;
+                for (int j = 0; j < n; j++) {
+                    const uint32_t e = tb.w2t(base + j);
+                    const int t = e & 0xFF;
+                    const float cwt = ((float)(e >> 8) * (1.0f / 16.0f)) * wes[is_const ? 0 : t];
+                    ws = ws + iw[t] * cwt;
+                    tc = tc + cwt;
+                }
+                v = ws / tc;
+            }
+            dw[w] = v;
+        }
+    }
+    const bool decim = act && W != T;
+    __syncwarp();
+    if (decim) {
+        for (int t = gl; t < T; t += 16) {
+            // the texel's entries in list order; padding entries add dw[0] * 0, which never changes v
+            const uint64_t e4 = tb.tw4(m, t);
+            float v = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + dw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+            inf[t] = v;
+        }
+    }
+    __syncwarp();
+    if (decim) {
+        for (int w = gl; w < W; w += 16) {
+            const int n = tb.wt_count(m, w), base = dmi.wt_base + tb.wt_start(m, w);
+            float e0 = 1e-10f, e1 = 0.0f;
+            for (int j = 0; j < n; j++) {
+                const uint32_t e = tb.w2t(base + j);
+                const int t = e & 0xFF;
+                const float c = (float)(e >> 8) * (1.0f / 16.0f);
+                const float sc = wes[is_const ? 0 : t] * c;
+                e0 = e0 + c * sc;
+                e1 = e1 + (inf[t] - iw[t]) * sc;
+            }
+            dw[w] = dw[w] + clampf((e1 * -16.0f) / e0, -0.25f, 0.25f);
+        }
+    }
+}
+
+// Passes 02-05 for the decimation modes of a partitioned block, a half-warp per mode, two
+// modes per warp at a time (passes 03-05 need at most 16 lanes: 16 angular steps at most,
+// 12 for every valid mode).  Every lane of a warp runs the same number of loop trips (a
+// half without a mode idles), so the warp-wide __syncwarp()s are reached by all of its
+// lanes.
+template <int kFrontWarps>
 __device__ __forceinline__ void dm_passes(const Tabs& tb, int T, const FrontLayout& fl, uint8_t* sm, int ndm_run,
                                           const int16_t* dm_run, const float* iw, const float* wes, bool is_const,
-                                          float* dec, float* lov, float* hiv) {
-    {
-        constexpr int gpw = 32 / G;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        const int grp = lane / G, gl = lane % G;
-        uint8_t* scr = sm + fl.scratch + warp * kScratchPerWarp + grp * kScratchPerHalf;
-        float* inf = reinterpret_cast<float*>(scr);
-        uint32_t* smp = reinterpret_cast<uint32_t*>(scr + (G == 32 ? 144 * 4 : 16 * 4));
-        float* ang = reinterpret_cast<float*>(scr + (G == 32 ? 144 * 4 + 64 * 4 : 32 * 4));
-        float* lh = reinterpret_cast<float*>(scr + (G == 32 ? 144 * 4 + 64 * 4 + 16 * 4 : 48 * 4));  // pass05 keys [16] (u64), minidx [16]
-        for (int mb = warp * gpw; mb < ndm_run; mb += kFrontWarps * gpw) {
-            const int mi = mb + grp;
-            const bool act = mi < ndm_run;
-            const int m = act ? (dm_run ? dm_run[mi] : mi) : 0;
-            const DevDm dmi = tb.dm(m);
-            const int W = act ? (int)dmi.W : 0;
-            float* dw = dec + m * 64;
-            if (W == T || !act) {
-                for (int w = gl; w < W; w += G) dw[w] = iw[w];
-            } else {
-                for (int w = gl; w < W; w += G) {
-                    const int n = tb.wt_count(m, w);
-                    float v = 0.0f;
-                    if (n) {
-                        const int base = dmi.wt_base + tb.wt_start(m, w);
-                        float ws = 0.0f, tc = 1e-10f;
-                        for (int j = 0; j < n; j++) {
-                            const uint32_t e = tb.w2t(base + j);
-                            const int t = e & 0xFF;
-                            const float cwt = ((float)(e >> 8) * (1.0f / 16.0f)) * wes[is_const ? 0 : t];
-                            ws = ws + iw[t] * cwt;
-                            tc = tc + cwt;
-                        }
-                        v = ws / tc;
-                    }
-                    dw[w] = v;
-                }
-            }
-            // with half-warps every lane takes these syncs (a half with a direct or no mode
-            // skips the work between them); a whole warp shares its mode
-            const bool decim = act && W != T;
-            if (G == 16 || decim) __syncwarp();
-            if (decim) {
-                for (int t = gl; t < T; t += G) {
-                    // the texel's entries in list order; padding entries add dw[0] * 0, which never changes v
-                    const uint64_t e4 = tb.tw4(m, t);
-                    float v = 0.0f;
+                                          float* dec, float* lov, float* hiv, float* infbuf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int half = lane >> 4, hl = lane & 15;
+    float* inf = infbuf + (warp * 2 + half) * T;
+    uint8_t* hs = sm + fl.scratch + warp * kDmScratchPerWarp + half * kDmScratchHalf;
+    uint32_t* smp = reinterpret_cast<uint32_t*>(hs);
+    float* ang = reinterpret_cast<float*>(hs + 64 * 4);
+    float* lh = reinterpret_cast<float*>(hs + 64 * 4 + 16 * 4);  // pass05 keys [16] (u64), minidx [16]
+    for (int mb = warp * 2; mb < ndm_run; mb += kFrontWarps * 2) {
+        const int mi = mb + half;
+        const bool act = mi < ndm_run;
+        const int m = act ? (dm_run ? dm_run[mi] : mi) : 0;
+        const DevDm dmi = tb.dm(m);
+        const int W = act ? (int)dmi.W : 0;
+        float* dw = dec + m * 64;
+        pass02_mode(tb, T, m, dmi, W, act, hl, inf, iw, wes, is_const, dw);
+        __syncwarp();
+        for (int w = hl; w < W; w += 16) smp[w] = f2u(rintf(clampf(dw[w], 0.0f, 1.0f) * (1024.0f - 1.0f)));
+        __syncwarp();
+        // pass03: angular offsets
+        if (act) {
+            // table values fetched four at a time, then summed in weight order
+            float ax = 0.0f, ay = 0.0f;
+            int j = 0;
+            for (; j + 4 <= W; j += 4) {
+                float c[4], sn[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + dw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f)); }
-                    inf[t] = v;
-                }
-            }
-            if (G == 16 || decim) __syncwarp();
-            if (decim) {
-                for (int w = gl; w < W; w += G) {
-                    const int n = tb.wt_count(m, w), base = dmi.wt_base + tb.wt_start(m, w);
-                    float e0 = 1e-10f, e1 = 0.0f;
-                    for (int j = 0; j < n; j++) {
-                        const uint32_t e = tb.w2t(base + j);
-                        const int t = e & 0xFF;
-                        const float c = (float)(e >> 8) * (1.0f / 16.0f);
-                        const float sc = wes[is_const ? 0 : t] * c;
-                        e0 = e0 + c * sc;
-                        e1 = e1 + (inf[t] - iw[t]) * sc;
-                    }
-                    dw[w] = dw[w] + clampf((e1 * -16.0f) / e0, -0.25f, 0.25f);
-                }
-            }
-            __syncwarp();
-            // pass03: angular offsets
-            for (int w = gl; w < W; w += G) smp[w] = f2u(rintf(clampf(dw[w], 0.0f, 1.0f) * (1024.0f - 1.0f)));
-            __syncwarp();
-            if (act && gl < 16) {
-                // table values fetched four at a time, then summed in weight order
-                float ax = 0.0f, ay = 0.0f;
-                int j = 0;
-                for (; j + 4 <= W; j += 4) {
-                    float c[4], sn[4];
+                for (int u = 0; u < 4; u++) { const int k = smp[j + u] * 16 + hl; c[u] = tb.cos_t(k); sn[u] = tb.sin_t(k); }
 #pragma unroll
-                    for (int u = 0; u < 4; u++) { const int k = smp[j + u] * 16 + gl; c[u] = tb.cos_t(k); sn[u] = tb.sin_t(k); }
-#pragma unroll
-                    for (int u = 0; u < 4; u++) { ax = ax + c[u]; ay = ay + sn[u]; }
-                }
-                for (; j < W; j++) { const int k = smp[j] * 16 + gl; ax = ax + tb.cos_t(k); ay = ay + tb.sin_t(k); }
-                ang[gl] = atan2_search(ay, ax) * (1.0f / (2.0f * 3.14159265358979323846f));
+                for (int u = 0; u < 4; u++) { ax = ax + c[u]; ay = ay + sn[u]; }
             }
-            __syncwarp();
-            // pass04 + pass05: lane i < S evaluates angular step i (rounding error and cut
-            // errors over the weights) and offers its candidates to the weight spans the
-            // sequential scan of pass05 would update with them: span sp takes e, sp - 1 takes
-            // e + cl and then e + ch, sp - 2 takes e + cl + ch, each only when strictly below the
-            // span's best so far (initially 1e37), steps in ascending order.  That scan keeps,
-            // per span, the first minimum in this order, which is the smallest key
-            //   error bits << 32 | step << 2 | order within the step << 1 | low-cut flag:
-            // errors are sums of non-negative products (never -0.0f, NaN or 1e37), so their
-            // bit patterns order like their values.  Only spans 0..15 are read (q <= 7 needs
-            // span c_steps_for_quant[q] <= 12; S <= 12 for every valid decimation mode).
-            const int S = act ? (int)dmi.max_angular_steps : 0;
-            unsigned long long* best = reinterpret_cast<unsigned long long*>(lh);  // [16]
-            float* lmin = lh + 32;                                                 // [16] minidx per step
-            if (gl < 16) best[gl] = ~0ull;
-            __syncwarp();
-            if (gl < S) {
-                float mnw = 3.4e38f, mxw = -3.4e38f;
-                for (int j = 0; j < W; j++) { const float v = dw[j]; if (v < mnw) mnw = v; if (v > mxw) mxw = v; }
-                const float rcp = (float)(gl + 1), off = ang[gl];
-                const float minidx = rintf(mnw * rcp - off), maxidx = rintf(mxw * rcp - off);
-                float ev = 0.0f, cl = 0.0f, ch = 0.0f;
-                for (int j = 0; j < W; j++) {
-                    const float sv = dw[j] * rcp - off, r = rintf(sv), d = sv - r;
-                    ev = ev + d * d;
-                    cl = cl + (r == minidx ? 1.0f - (2.0f * d) : 0.0f);
-                    ch = ch + (r == maxidx ? 1.0f + (2.0f * d) : 0.0f);
-                }
-                const int sp = min(max(f2i((maxidx - minidx) + 1.0f), 2), (int)dmi.max_quant_steps + 3);
-                const float ss = 1.0f / rcp, esc = ss * ss;
-                const float e = ev * esc, ecl0 = cl * esc, ech0 = ch * esc;
-                const float ecl = e + ecl0, ech = e + ech0, eclh = (e + ecl0) + ech0;
-                lmin[gl] = minidx;
-                const unsigned long long ik = (unsigned long long)gl << 2;
-                if (sp < 16 && e < 1e37f) atomicMin(&best[sp], ((unsigned long long)__float_as_uint(e) << 32) | ik);
-                if (sp - 1 < 16 && ecl < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ecl) << 32) | ik | 1ull);
-                if (sp - 1 < 16 && ech < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ech) << 32) | ik | 2ull);
-                if (sp - 2 < 16 && eclh < 1e37f) atomicMin(&best[sp - 2], ((unsigned long long)__float_as_uint(eclh) << 32) | ik | 1ull);
-            }
-            __syncwarp();
-            // pass05: low/high value per quant level from the best step of its span (step 0
-            // and no low cut when no candidate got below 1e37)
-            if (act && gl < 8) {
-                const int q = gl;
-                float lo_v = 0.0f, hi_v = 0.0f;
-                if (q <= (int)dmi.max_quant_level) {
-                    const int qs = c_steps_for_quant[q];
-                    const unsigned long long k = best[qs];
-                    const int bsi = k == ~0ull ? 0 : (int)(((uint32_t)k) >> 2);
-                    const float lwi = lmin[bsi] + ((k != ~0ull && (k & 1ull)) ? 1.0f : 0.0f);
-                    const float hwi = (lwi + (float)qs) - 1.0f;
-                    const float step = 1.0f / (1.0f + (float)bsi);
-                    const float off = ang[bsi];
-                    lo_v = (off + lwi) * step;
-                    hi_v = (off + hwi) * step;
-                }
-                lov[m * 8 + q] = lo_v;
-                hiv[m * 8 + q] = hi_v;
-            }
-            __syncwarp();
+            for (; j < W; j++) { const int k = smp[j] * 16 + hl; ax = ax + tb.cos_t(k); ay = ay + tb.sin_t(k); }
+            ang[hl] = atan2_search(ay, ax) * (1.0f / (2.0f * 3.14159265358979323846f));
         }
+        __syncwarp();
+        // pass04 + pass05: lane i < S evaluates angular step i (rounding error and cut
+        // errors over the weights) and offers its candidates to the weight spans the
+        // sequential scan of pass05 would update with them: span sp takes e, sp - 1 takes
+        // e + cl and then e + ch, sp - 2 takes e + cl + ch, each only when strictly below the
+        // span's best so far (initially 1e37), steps in ascending order.  That scan keeps,
+        // per span, the first minimum in this order, which is the smallest key
+        //   error bits << 32 | step << 2 | order within the step << 1 | low-cut flag:
+        // errors are sums of non-negative products (never -0.0f, NaN or 1e37), so their
+        // bit patterns order like their values.  Only spans 0..15 are read (q <= 7 needs
+        // span c_steps_for_quant[q] <= 12; S <= 12 for every valid decimation mode).
+        const int S = act ? (int)dmi.max_angular_steps : 0;
+        unsigned long long* best = reinterpret_cast<unsigned long long*>(lh);  // [16]
+        float* lmin = lh + 32;                                                 // [16] minidx per step
+        best[hl] = ~0ull;
+        __syncwarp();
+        if (hl < S) {
+            float mnw = 3.4e38f, mxw = -3.4e38f;
+            for (int j = 0; j < W; j++) { const float v = dw[j]; if (v < mnw) mnw = v; if (v > mxw) mxw = v; }
+            const float rcp = (float)(hl + 1), off = ang[hl];
+            const float minidx = rintf(mnw * rcp - off), maxidx = rintf(mxw * rcp - off);
+            float ev = 0.0f, cl = 0.0f, ch = 0.0f;
+            for (int j = 0; j < W; j++) {
+                const float sv = dw[j] * rcp - off, r = rintf(sv), d = sv - r;
+                ev = ev + d * d;
+                cl = cl + (r == minidx ? 1.0f - (2.0f * d) : 0.0f);
+                ch = ch + (r == maxidx ? 1.0f + (2.0f * d) : 0.0f);
+            }
+            const int sp = min(max(f2i((maxidx - minidx) + 1.0f), 2), (int)dmi.max_quant_steps + 3);
+            const float ss = 1.0f / rcp, esc = ss * ss;
+            const float e = ev * esc, ecl0 = cl * esc, ech0 = ch * esc;
+            const float ecl = e + ecl0, ech = e + ech0, eclh = (e + ecl0) + ech0;
+            lmin[hl] = minidx;
+            const unsigned long long ik = (unsigned long long)hl << 2;
+            if (sp < 16 && e < 1e37f) atomicMin(&best[sp], ((unsigned long long)__float_as_uint(e) << 32) | ik);
+            if (sp - 1 < 16 && ecl < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ecl) << 32) | ik | 1ull);
+            if (sp - 1 < 16 && ech < 1e37f) atomicMin(&best[sp - 1], ((unsigned long long)__float_as_uint(ech) << 32) | ik | 2ull);
+            if (sp - 2 < 16 && eclh < 1e37f) atomicMin(&best[sp - 2], ((unsigned long long)__float_as_uint(eclh) << 32) | ik | 1ull);
+        }
+        __syncwarp();
+        // pass05: low/high value per quant level from the best step of its span (step 0
+        // and no low cut when no candidate got below 1e37)
+        if (act && hl < 8) {
+            const int q = hl;
+            float lo_v = 0.0f, hi_v = 0.0f;
+            if (q <= (int)dmi.max_quant_level) {
+                const int qs = c_steps_for_quant[q];
+                const unsigned long long k = best[qs];
+                const int bsi = k == ~0ull ? 0 : (int)(((uint32_t)k) >> 2);
+                const float lwi = lmin[bsi] + ((k != ~0ull && (k & 1ull)) ? 1.0f : 0.0f);
+                const float hwi = (lwi + (float)qs) - 1.0f;
+                const float step = 1.0f / (1.0f + (float)bsi);
+                const float off = ang[bsi];
+                lo_v = (off + lwi) * step;
+                hi_v = (off + hwi) * step;
+            }
+            lov[m * 8 + q] = lo_v;
+            hiv[m * 8 + q] = hi_v;
+        }
+        __syncwarp();
     }
 }
 
@@ -915,8 +920,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     }
 
     // ---------------- passes 02-05
-    if (T <= 16) dm_passes<16, kFrontWarps>(tb, T, fl, sm, ndm_run, dm_run, iw, wes, is_const, dec, lov, hiv);
-    else dm_passes<32, kFrontWarps>(tb, T, fl, sm, ndm_run, dm_run, iw, wes, is_const, dec, lov, hiv);
+    dm_passes<kFrontWarps>(tb, T, fl, sm, ndm_run, dm_run, iw, wes, is_const, dec, lov, hiv, qfs);
     __syncthreads();
 
     // ---------------- pass07: weight quantisation error per block mode
