@@ -358,7 +358,6 @@ __device__ __forceinline__ float undec_weight(const RTabs& tb, int dm, const uin
     return v;
 }
 
-constexpr int kUwCacheTexels = 16;  // footprints up to 4x4 keep each thread's infilled weights in shared memory
 
 // A partitioned block's staged texels.  Up to 16 texels they are floats; larger blocks
 // stage RGBA8 (4 bytes a texel, so more CTAs fit on an SM) read back through the CTA's
@@ -380,7 +379,7 @@ template <> struct TexelRow<false> {
 
 template <class Row>
 __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const Row px, const uint8_t* tp,
-                                 CandSmem& cs, float* uwc, Snap* snap) {
+                                 CandSmem& cs, Snap* snap) {
     const RTabs tb{a.tables, &a.L};
     const int T = a.L.T;
     const CandInit& ci = rec.c[k];
@@ -397,11 +396,9 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
     float top_err = ERR_DEFAULT;
     uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
-    // uwc (when non-null) caches this thread's infilled weights, stride kRefineThreads
-    auto fill_uw = [&]() {
-        if (uwc) for (int t = 0; t < T; t++) uwc[t * kRefineThreads] = undec_weight(tb, bm.dm, cs.qw, t, direct);
-    };
-    auto UW = [&](int t) { return uwc ? uwc[t * kRefineThreads] : undec_weight(tb, bm.dm, cs.qw, t, direct); };
+    // infilled weights are recomputed where read: caching them per thread in shared memory
+    // costs more resident CTAs than the recomputation
+    auto UW = [&](int t) { return undec_weight(tb, bm.dm, cs.qw, t, direct); };
 
     auto final_error = [&]() {
         float total = 0.0f;
@@ -430,7 +427,6 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
 
     const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
     for (int it = 0; it < iters; it++) {
-        fill_uw();
         // ---------------- pass13: least-squares endpoints from the current weights
 #pragma unroll 1
         for (int q = 0; q < P; q++) {
@@ -587,7 +583,6 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 else if ((ed < eb) && (uqw > 0)) cs.qw[we] = (uint8_t)dn;
             }
         }
-        fill_uw();
         final_error();
     }
 }
@@ -608,7 +603,6 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
     Px* pxs = reinterpret_cast<Px*>(U8 ? smem + sizeof(CandSmem) * kRefineThreads + 256 * 4 : smem + sizeof(CandSmem) * kRefineThreads);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + pbs * T);
     int* keys = reinterpret_cast<int*>(tps + ((pbs * T + 15) & ~15));
-    float* uwc_all = reinterpret_cast<float*>(keys + kRefineThreads);
     const int tid = threadIdx.x;
     // Items: every slot of every block in slot-major order (consecutive CTAs hold
     // partitioned blocks of the same slot, hence the same partition count, so
@@ -677,9 +671,8 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
             Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
             snap->err = ERR_DEFAULT;  // inert slot unless refined below
             if (k < (int)rec.ncand) {
-                float* uwc = T <= kUwCacheTexels ? uwc_all + tid : nullptr;
-                if constexpr (U8) refine_candidate(a, rec, (int)rec.P, k, TexelRow<true>{pxs + pbl * T, lut}, tps + pbl * T, cs[tid], uwc, snap);
-                else refine_candidate(a, rec, (int)rec.P, k, TexelRow<false>{pxs + pbl * T}, tps + pbl * T, cs[tid], uwc, snap);
+                if constexpr (U8) refine_candidate(a, rec, (int)rec.P, k, TexelRow<true>{pxs + pbl * T, lut}, tps + pbl * T, cs[tid], snap);
+                else refine_candidate(a, rec, (int)rec.P, k, TexelRow<false>{pxs + pbl * T}, tps + pbl * T, cs[tid], snap);
                 if (a.work) atomicAdd(&refined[rec.P - 1], 1u);
             }
         }
@@ -868,8 +861,7 @@ size_t refine_smem_bytes(const TableLayout& L, int topn) {
     const size_t pbs = (size_t)refine_pbs(L.T, topn);
     const bool u8 = refine_u8(L.T);
     return sizeof(CandSmem) * kRefineThreads + (u8 ? 256 * 4 : 0) + pbs * L.T * (u8 ? 4 : 16) + ((pbs * L.T + 15) & ~(size_t)15) +
-           kRefineThreads * 4 +
-           (L.T <= kUwCacheTexels ? (size_t)L.T * kRefineThreads * 4 : 0);
+           kRefineThreads * 4;
 }
 
 size_t refine_smem_bytes(const TableLayout& L) {  // the largest over the refinement top-N
