@@ -40,7 +40,7 @@ __device__ __forceinline__ int32_t shl1(int32_t v) { return (int32_t)((uint32_t)
 
 // ------------------------------------------------------------ pass14 colour endpoint packing
 struct Packer {
-    const uint8_t* cu2u;  // [17][512], then [17] deviation bounds
+    const uint8_t* cu2u;  // [17][512]
     __device__ int32_t tab(uint32_t q, int32_t idx) const { return cu2u[(q - 4) * 512 + idx]; }
     __device__ float enc_err(float4 u0, float4 u1, I4 q0, I4 q1) const {
         const float4 e0 = u0 - make_float4((float)q0.x, (float)q0.y, (float)q0.z, (float)q0.w);
@@ -121,35 +121,52 @@ struct Packer {
         o0 = c1i; o1 = c0i;
         return true;
     }
-    // The reference's loop nudges the endpoints 0.2 apart per step until their quantised
-    // channel sums no longer cross.  A quantised channel is at most dev(q) from its rounded
-    // input (the table's bound), so while the rounded sums are more than 6 * dev(q) apart
-    // no step can end the loop; those sums only move towards each other, so the steps
-    // before the first one that can end it only move the endpoints (the same float
-    // operations in the same order), and the lookups start there.
+    // Quantised channel sums of the endpoints at one step of the loop below: true when the
+    // step ends it (the low endpoint's sum no longer above the high one's).
+    __device__ bool qrgb_probe(uint32_t q, float x0, float y0, float z0, float x1, float y1, float z1, I4& c0i, I4& c1i) const {
+        c0i = q3flt(q, I4{max(f2i(rintf(x0)), 0), max(f2i(rintf(y0)), 0), max(f2i(rintf(z0)), 0), 0}, make_float4(x0, y0, z0, 0.0f));
+        c1i = q3flt(q, I4{min(f2i(rintf(x1)), 255), min(f2i(rintf(y1)), 255), min(f2i(rintf(z1)), 255), 0}, make_float4(x1, y1, z1, 0.0f));
+        return (c0i.x + c0i.y + c0i.z) <= (c1i.x + c1i.y + c1i.z);
+    }
+    // The reference's loop nudges the endpoints 0.2 apart per step (at most 4096 steps) and
+    // stops at the first step whose quantised channel sums no longer cross.  A rounded
+    // channel and its half-step bit move monotonically with its endpoint and the table is
+    // monotonic, so the low sum never rises and the high one never falls from step to step:
+    // the stopping test is monotonic in the step.  The stop is found by probing steps 0, 1,
+    // 3, 7, ... and bisecting the last bracket; the endpoints are always brought to a probed
+    // step by the loop's own float subtractions and additions from an earlier probed step,
+    // so each probe sees the values the loop would.
     __device__ void quant_rgb(float4 c0, float4 c1, I4& o0, I4& o1, uint32_t q) const {
+        float x0 = c0.x, y0 = c0.y, z0 = c0.z, x1 = c1.x, y1 = c1.y, z1 = c1.z;  // step lo
         I4 c0i, c1i;
-        const float4 nudge = mk(0.2f);
-        const int lim = 6 * (int)cu2u[17 * 512 + (q - 4)];
-        int it = 0;
-#pragma unroll 1
-        for (; it < 4095; it++) {
-            const int s0 = (max(f2i(rintf(c0.x)), 0) + max(f2i(rintf(c0.y)), 0)) + max(f2i(rintf(c0.z)), 0);
-            const int s1 = (min(f2i(rintf(c1.x)), 255) + min(f2i(rintf(c1.y)), 255)) + min(f2i(rintf(c1.z)), 255);
-            if (s0 - s1 <= lim) break;
-            c0 = c0 - nudge;
-            c1 = c1 + nudge;
-        }
-        for (; it < 4096; it++) {  // ends once c0 <= 0 and c1 >= 255 at the latest (< 1300 steps)
-            I4 c0q = ivec(rnev(c0));
-            c0q = {max(c0q.x, 0), max(c0q.y, 0), max(c0q.z, 0), max(c0q.w, 0)};
-            c0i = q3flt(q, c0q, c0);
-            c0 = c0 - nudge;
-            I4 c1q = ivec(rnev(c1));
-            c1q = {min(c1q.x, 255), min(c1q.y, 255), min(c1q.z, 255), min(c1q.w, 255)};
-            c1i = q3flt(q, c1q, c1);
-            c1 = c1 + nudge;
-            if ((c0i.x + c0i.y + c0i.z) <= (c1i.x + c1i.y + c1i.z)) break;
+        if (!qrgb_probe(q, x0, y0, z0, x1, y1, z1, c0i, c1i)) {
+            auto advance = [](float& a, float& b, float& c, float& d, float& e, float& f, int n) {
+#pragma unroll 4
+                for (int i = 0; i < n; i++) { a = a - 0.2f; b = b - 0.2f; c = c - 0.2f; d = d + 0.2f; e = e + 0.2f; f = f + 0.2f; }
+            };
+            int lo = 0, hi = 0, step = 1;
+            for (;;) {  // the test fails at lo; at most 13 trips
+                hi = min(lo + step, 4095);
+                float a = x0, b = y0, c = z0, d = x1, e = y1, f = z1;
+                advance(a, b, c, d, e, f, hi - lo);
+                if (qrgb_probe(q, a, b, c, d, e, f, c0i, c1i) || hi == 4095) break;
+                x0 = a; y0 = b; z0 = c; x1 = d; y1 = e; z1 = f;
+                lo = hi;
+                step *= 2;
+            }
+            while (hi - lo > 1) {  // the stop is in (lo, hi] (hi = 4095: the last step)
+                const int mid = lo + (hi - lo) / 2;
+                float a = x0, b = y0, c = z0, d = x1, e = y1, f = z1;
+                advance(a, b, c, d, e, f, mid - lo);
+                if (qrgb_probe(q, a, b, c, d, e, f, c0i, c1i)) {
+                    hi = mid;
+                } else {
+                    lo = mid;
+                    x0 = a; y0 = b; z0 = c; x1 = d; y1 = e; z1 = f;
+                }
+            }
+            advance(x0, y0, z0, x1, y1, z1, 1);
+            qrgb_probe(q, x0, y0, z0, x1, y1, z1, c0i, c1i);
         }
         o0 = c0i; o1 = c1i;
     }

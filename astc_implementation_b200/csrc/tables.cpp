@@ -132,7 +132,7 @@ void quints_of(int Q, int q[3]) {
 struct ConstTables {
     uint8_t q2u[142], q2u_start[12];
     int8_t qmt[10][128];
-    uint8_t cu2u[17][512 + 16];  // then the level's largest |entry - idx / 2| (byte 512)
+    uint8_t cu2u[17][512];
     uint16_t prev_next[12][65];
     float bqe[17];
     uint8_t wscr[12][32], cscr[17][256], trits[243], quints[125];
@@ -176,7 +176,6 @@ ConstTables make_const_tables() {
                 if (d < bd || (d == bd && ((idx & 1) ? u > bu : u < bu))) { bd = d; bu = u; }
             }
             c.cu2u[k][idx] = (uint8_t)bu;
-            c.cu2u[k][512] = (uint8_t)std::max<int>(c.cu2u[k][512], std::abs(bu - v));
         }
         for (int v = 0; v < 256; v++) {  // nearest representable value; ties to the higher code
             int bd = 1 << 30, be = 0;
@@ -479,6 +478,11 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
     if (!hp) return false;
     const HostTables& h = *hp;
     const ConstTables& c = const_tables();
+    // the refinement's endpoint quantisation search relies on each level's colour table
+    // being non-decreasing in its index (true by construction: nearest values of idx / 2)
+    for (int k = 0; k < 17; k++)
+        for (int i = 1; i < 512; i++)
+            if (c.cu2u[k][i] < c.cu2u[k][i - 1]) return false;
     std::memset(&L, 0, sizeof(L));
     blob.clear();
     L.bx = bx; L.by = by; L.T = h.T;
@@ -561,14 +565,7 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
     L.off_q2u = put(blob, c.q2u, 142);
     L.off_q2u_start = put(blob, c.q2u_start, 12);
     L.off_qmt = put(blob, &c.qmt[0][0], 1280);
-    {   // u8 [17][512] then the 17 deviation bounds
-        std::vector<uint8_t> cq(17 * 512 + 17);
-        for (int k = 0; k < 17; k++) {
-            std::memcpy(cq.data() + k * 512, c.cu2u[k], 512);
-            cq[17 * 512 + k] = c.cu2u[k][512];
-        }
-        L.off_cu2u = put(blob, cq.data(), cq.size());
-    }
+    L.off_cu2u = put(blob, &c.cu2u[0][0], 17 * 512);
     L.off_prev_next = put(blob, &c.prev_next[0][0], 12 * 65);
     L.off_bqe = put(blob, c.bqe, 17);
     L.off_wscr = put(blob, &c.wscr[0][0], 12 * 32);

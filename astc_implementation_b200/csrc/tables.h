@@ -65,7 +65,7 @@ struct TableLayout {
     uint32_t off_q2u;         // u8 [142]  weight unquant values, sorted (pass07:12-37)
     uint32_t off_q2u_start;   // u8 [12]
     uint32_t off_qmt;         // i8 [10][128] quant mode table (pass11)
-    uint32_t off_cu2u;        // u8 [17][512] colour quantise-unquantise (pass14), then u8 [17] max |entry - idx / 2|
+    uint32_t off_cu2u;        // u8 [17][512] colour quantise-unquantise (pass14), non-decreasing in idx
     uint32_t off_prev_next;   // u16[12][65] (pass16)
     uint32_t off_bqe;         // f32[17]    baseline quant error (pass09)
     uint32_t off_wscr;        // u8 [12][32] weight scramble map
