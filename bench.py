@@ -1,9 +1,11 @@
-"""Throughput benchmark of the ASTC full search on B200.
+"""Throughput benchmark of the ASTC block-compression search on B200.
 
 Workload (one "step"): one 2048x2048 RGBA8 synthetic texture (generator of
 astc_implementation_b200/synth.py, seeds 1-4 in rotation; rank r of a multi-GPU
-run uses seeds 1+4r .. 4+4r) encoded twice, at 4x4 and at 6x6, by the full
-search.  The metric is Mtexel/s over both encodes.
+run uses seeds 1+4r .. 4+4r) encoded twice, at 4x4 and at 6x6, by the learned
+proposal search (the full search, the reference's algorithm, is timed beside it
+on the same textures for the speed-up and PSNR comparison; --method full times
+it alone).  The metric is Mtexel/s over both encodes.
 
   value       device-resident input and output, CUDA events on the launching
               stream around exactly K steps, max over ranks; the L2 is flushed
@@ -529,20 +531,30 @@ def main():
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath) and dom_key in ("front", "refine") and stage_n[:, dom].sum():
-        # DRAM bytes measured by ncu per block of the full search (13 partitioned blocks,
-        # 104 candidates), scaled to the partitioned blocks / candidates this run processed
         kname = "k_front" if dom_key == "front" else "k_refine"
-        per_block = json.load(open(tpath)).get(kname, {}).get("dram_bytes_per_block")
-        if per_block:
-            units = work[:, 0:4].sum() / 13.0 if dom_key == "front" else work[:, 6:10].sum() / 104.0
-            traffic = round(per_block * units / stage_n[:, dom].sum())
+        tj = json.load(open(tpath))
+        if use_prop:
+            # DRAM bytes per launch measured by ncu on this workload (proposal and fallback
+            # launches); other sizes or footprints report none
+            p = tj.get("proposal", {})
+            w = p.get("workload", {})
+            if w.get("size") == SIZE and w.get("footprints") == ["%dx%d" % f for f in FOOTPRINTS] and kname in p:
+                traffic = int(p[kname]["dram_bytes_per_launch"])
+        else:
+            # DRAM bytes measured by ncu per block of the full search (13 partitioned blocks,
+            # 104 candidates), scaled to the partitioned blocks / candidates this run processed
+            per_block = tj.get(kname, {}).get("dram_bytes_per_block")
+            if per_block:
+                units = work[:, 0:4].sum() / 13.0 if dom_key == "front" else work[:, 6:10].sum() / 104.0
+                traffic = round(per_block * units / stage_n[:, dom].sum())
     peaks = measured_peaks()
     cpu = None
     if not args.no_cpu_baseline:
         rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample)
         cpu = {"value": round(rate, 4), "unit": "Mtexel/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": "%dx%d crop of the seed-1 texture at %s, full search (%.1f s of CPU time)"
-                         % (args.cpu_sample, args.cpu_sample, " and ".join("%dx%d" % f for f in FOOTPRINTS), secs)}
+               "sample": "%dx%d crop of the seed-1 texture at %s, full search (%.1f s wall time on %d threads)"
+                         % (args.cpu_sample, args.cpu_sample, " and ".join("%dx%d" % f for f in FOOTPRINTS), secs,
+                            os.cpu_count())}
     fp_names = " and ".join("%dx%d" % f for f in FOOTPRINTS)
     method = ("learned proposal search (%s), full search for low-confidence and poorly encoded blocks"
               % ", ".join("%s=%s" % kv for kv in PRUNING.items())) if use_prop else "full search"
