@@ -93,6 +93,25 @@ def test_degenerate_blocks(enc, kind):
     assert np.array_equal(sym, ref_sym) and np.array_equal(out, ref_out)
 
 
+@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6), (8, 5)])
+@pytest.mark.parametrize("kind", ["noise", "opposed_gradients"])
+def test_endpoint_search_hard_blocks_bit_exact(enc, kind, bx, by):
+    """Blocks whose fitted endpoints come out inverted or far apart make the endpoint
+    packer's nudge loop run for hundreds of steps (found by bisection on the GPU)."""
+    rng = np.random.default_rng(7)
+    h, w = 48, 60
+    if kind == "noise":
+        img = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    else:
+        x = np.linspace(0, 1, w, dtype=np.float32)[None, :].repeat(h, 0)
+        y = np.linspace(0, 1, h, dtype=np.float32)[:, None].repeat(w, 1)
+        img = np.stack([255 * x, 255 * (1 - x), 255 * y, 255 * (1 - y * x)], axis=2)
+        img = (img + rng.normal(0, 12, img.shape)).clip(0, 255).astype(np.uint8)
+    out, sym = gpu_encode(enc, img, bx, by)
+    ref_out, ref_sym = oracle_encode(img, bx, by)
+    assert np.array_equal(sym, ref_sym) and np.array_equal(out, ref_out)
+
+
 def test_full_size_2048_properties():
     """BASELINE config 2 sizes: deterministic, chunking-invariant, decodes well, and a
     sampled set of blocks matches the oracle exactly."""

@@ -71,3 +71,84 @@ def test_oracle_tables_match_live_reference_build():
         pytest.skip("oracle/_ref not built (needs the reference checkout)")
     for bx, by in [(4, 4), (6, 6), (12, 12), (10, 5)]:
         assert _libs.footprint_digests(ref, "astcref_", bx, by) == _libs.footprint_digests(_libs.oracle(), "orc_", bx, by)
+
+
+def test_colour_quant_table_non_decreasing():
+    """The refinement's endpoint quantisation search (k_refine, Packer::quant_rgb) finds the
+    stop of the reference's nudge loop by bisection, which needs every level's colour
+    quantise-unquantise table to be non-decreasing in its index."""
+    cu = _libs.golden_tables()["color_unquant_to_uquant"]
+    assert cu.shape == (17, 512)
+    assert (np.diff(cu.astype(np.int64), axis=1) >= 0).all()
+
+
+def _nudge_stepwise(tab, c0, c1):
+    """The reference's loop (pass14 quantize_rgb): step k uses the endpoints after k nudges."""
+    f32 = np.float32
+    a = b = None
+    for _ in range(4096):
+        a = [tab[2 * max(int(np.rint(v)), 0) + (1 if f32(v - f32(max(int(np.rint(v)), 0))) >= f32(-0.1) else 0)] for v in c0]
+        c0 = [f32(v - f32(0.2)) for v in c0]
+        b = [tab[2 * min(int(np.rint(v)), 255) + (1 if f32(v - f32(min(int(np.rint(v)), 255))) >= f32(-0.1) else 0)] for v in c1]
+        c1 = [f32(v + f32(0.2)) for v in c1]
+        if sum(a) <= sum(b):
+            break
+    return a, b
+
+
+def _nudge_bisect(tab, c0, c1):
+    """The same stop found as k_refine does: probes at steps 0, 1, 3, 7, ... then bisection,
+    endpoints advanced from an earlier probed step by the loop's own float steps."""
+    f32 = np.float32
+
+    def probe(x0, x1):
+        a = [tab[2 * max(int(np.rint(v)), 0) + (1 if f32(v - f32(max(int(np.rint(v)), 0))) >= f32(-0.1) else 0)] for v in x0]
+        b = [tab[2 * min(int(np.rint(v)), 255) + (1 if f32(v - f32(min(int(np.rint(v)), 255))) >= f32(-0.1) else 0)] for v in x1]
+        return sum(a) <= sum(b), a, b
+
+    def advance(x0, x1, n):
+        for _ in range(n):
+            x0 = [f32(v - f32(0.2)) for v in x0]
+            x1 = [f32(v + f32(0.2)) for v in x1]
+        return x0, x1
+
+    ok, a, b = probe(c0, c1)
+    if ok:
+        return a, b
+    lo, step = 0, 1
+    while True:
+        hi = min(lo + step, 4095)
+        t0, t1 = advance(c0, c1, hi - lo)
+        ok, a, b = probe(t0, t1)
+        if ok or hi == 4095:
+            break
+        c0, c1, lo, step = t0, t1, hi, step * 2
+    while hi - lo > 1:
+        mid = lo + (hi - lo) // 2
+        t0, t1 = advance(c0, c1, mid - lo)
+        ok, a, b = probe(t0, t1)
+        if ok:
+            hi = mid
+        else:
+            lo, c0, c1 = mid, t0, t1
+    c0, c1 = advance(c0, c1, 1)
+    _, a, b = probe(c0, c1)
+    return a, b
+
+
+def test_nudge_loop_bisection_matches_stepwise():
+    """The bisection's result equals the reference loop's on random endpoints in [0, 255]
+    at every quant level, inverted pairs (long loops) and half-step values included."""
+    cu = _libs.golden_tables()["color_unquant_to_uquant"]
+    rng = np.random.default_rng(11)
+    f32 = np.float32
+    for i in range(600):
+        tab = [int(v) for v in cu[i % 17]]
+        c0 = [f32(v) for v in rng.uniform(0, 255, 3)]
+        c1 = [f32(v) for v in rng.uniform(0, 255, 3)]
+        if i % 3 == 1:  # bright low endpoint, dark high one: hundreds of steps
+            c0 = [f32(v) for v in rng.uniform(200, 255, 3)]
+            c1 = [f32(v) for v in rng.uniform(0, 40, 3)]
+        if i % 5 == 2:
+            c0 = [f32(np.floor(v) + 0.5) for v in c0]
+        assert _nudge_bisect(tab, c0, c1) == _nudge_stepwise(tab, c0, c1), i
