@@ -624,6 +624,39 @@ __device__ __forceinline__ void dm_passes(const Tabs& tb, int T, const FrontLayo
     }
 }
 
+// Code of the full search only (every block mode) is kept out of line, so that the
+// proposal search's path through the front stays compact in the instruction cache (the
+// front stalls on instruction fetch).
+// pass07 over every block mode, one thread per mode.
+template <int kFrontThreads>
+__device__ __noinline__ void pass07_all_modes(const Tabs& tb, int T, int P, int nbm, const float* lov, const float* hiv,
+                                              float min_cutoff, const float* dec, float* qfs, const float* iw,
+                                              const float* wes, bool is_const, float* bm_err, int* bm_bits) {
+    const int tid = threadIdx.x;
+    // one thread per mode; neighbouring threads get modes of the same decimation
+    for (int j = tid; j < nbm; j += kFrontThreads) {
+        const int i = tb.bm_order(j);
+        const DevBm bm = tb.bm(i);
+        const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
+        if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
+        const DevDm dmi = tb.dm(bm.dm);
+        const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, min_cutoff);
+        const float* dw = dec + bm.dm * 64;
+        for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
+        float err = 0.0f;
+        for (int t = 0; t < T; t++) {
+            const uint64_t e4 = tb.tw4(bm.dm, t);
+            float v = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
+            const float d = v - iw[t];
+            err = err + (d * d) * wes[is_const ? 0 : t];
+        }
+        bm_err[i] = err;
+        bm_bits[i] = bc;
+    }
+}
+
 template <int NT>
 __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, int slot_in_block, uint32_t entry, uint8_t* sm) {
     constexpr int kFrontThreads = NT, kFrontWarps = NT / 32;
@@ -925,30 +958,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
 
     // ---------------- pass07: weight quantisation error per block mode
     const int nlist = bmm ? M.nlive : nbm;  // block modes evaluated: the list, or all of them
-    if (!bmm) {
-        // one thread per mode; neighbouring threads get modes of the same decimation
-        for (int j = tid; j < nbm; j += kFrontThreads) {
-            const int i = tb.bm_order(j);
-            const DevBm bm = tb.bm(i);
-            const int bc = c_free_bits[P - 1] - (int)bm.weight_bits;
-            if (bm.quant > 11 || bc <= 0) { bm_err[i] = 1e38f; bm_bits[i] = 0; continue; }
-            const DevDm dmi = tb.dm(bm.dm);
-            const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
-            const float* dw = dec + bm.dm * 64;
-            for (int w = 0; w < dmi.W; w++) { float qf; bm_quant_weight(tb, s, dw[w], &qf); qfs[w * kFrontThreads + tid] = qf; }
-            float err = 0.0f;
-            for (int t = 0; t < T; t++) {
-                const uint64_t e4 = tb.tw4(bm.dm, t);
-                float v = 0.0f;
-#pragma unroll
-                for (int j = 0; j < 4; j++) { const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF; v = v + qfs[(e & 0xFF) * kFrontThreads + tid] * ((float)(e >> 8) * (1.0f / 16.0f)); }
-                const float d = v - iw[t];
-                err = err + (d * d) * wes[is_const ? 0 : t];
-            }
-            bm_err[i] = err;
-            bm_bits[i] = bc;
-        }
-    }
+    if (!bmm) pass07_all_modes<kFrontThreads>(tb, T, P, nbm, lov, hiv, M.min_cutoff, dec, qfs, iw, wes, is_const, bm_err, bm_bits);
     // ---------------- pass10: best format combination per quant level and integer total
     // One item per (quant level, integer total), beside pass07 (role-indexed): the format
     // combinations with that total, in the order the one-thread loops visit them (i, j, k, l
