@@ -223,6 +223,9 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
     float wie = T <= 20 ? 0.03f : T <= 31 ? 0.04f : T <= 41 ? 0.05f : 0.055f;
     wie = wie * wie;
     const float4 cw = chan_w();
+    uint32_t u_all = 0;  // sum over all texels of f2u(|x|^2 weighted), the line error of a zero direction
+    for (int t = lane; t < T; t += 32) { const float4 x = px[t]; u_all += f2u(dot4(x * x, cw)); }
+    for (int o = 16; o > 0; o >>= 1) u_all += __shfl_xor_sync(FULL, u_all, o);
     for (int r = 0; r < 4; r++) {
         const int cand = lane + 32 * r;
         const int e = (int)(uint32_t)key[cand];
@@ -267,18 +270,23 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
             for (int u = 1; u < 4; u++) { const float pr = dot4(s[u], s[u]); if (pr > mp) { mp = pr; best = s[u]; } }
             tdir[q] = normalize4(best);
         }
-        uint32_t usum = 0, ssum = 0;
+        // Every texel but those t < P of partition t sees a zero average and direction: its
+        // projection is 0, its line error |x|^2 (weighted) and its scale error NaN (the zero
+        // direction's normalisation), so f2u gives 0xFFFFFFFF.  The integer sums take those
+        // terms for every texel at once (u_all, -T) and the loop corrects the few texels
+        // that see their partition's own average and direction; integer sums do not depend
+        // on their order.
+        uint32_t usum = u_all, ssum = 0u - (uint32_t)T;
         int32_t lmin[P], lmax[P];
 #pragma unroll
         for (int q = 0; q < P; q++) { lmin[q] = 2147483647; lmax[q] = -2147483647; }
-        for (int t = 0; t < T; t++) {
-            const int p = row[t];
-            float4 av = mk(0.0f), ud = mk(0.0f);
-            if (t < P && p == t) {
 #pragma unroll
-                for (int q = 0; q < P; q++) if (q == t) { av = tavg[q]; ud = tdir[q]; }
-            }
+        for (int t = 0; t < P; t++) {
+            if (row[t] != t) continue;
+            const float4 av = tavg[t], ud = tdir[t];
             const float4 x = px[t];
+            usum -= f2u(dot4(x * x, cw));
+            ssum += 1u;
             const float up = dot4(x, ud);
             const float4 uproj = av + ud * dot4(x - av, ud);
             const float4 udiff = x - uproj;
@@ -290,9 +298,11 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
             usum += f2u(ud2);
             ssum += f2u(sd2);
             const int32_t upi = f2i(up * 4096.0f);
-#pragma unroll
-            for (int q = 0; q < P; q++) if (p == q) { lmin[q] = min(lmin[q], upi); lmax[q] = max(lmax[q], upi); }
+            lmin[t] = min(lmin[t], upi); lmax[t] = max(lmax[t], upi);
         }
+#pragma unroll
+        for (int q = 0; q < P; q++)  // the partition has a texel of projection 0
+            if (tb.part_count(P, e, q) > (row[q] == q ? 1 : 0)) { lmin[q] = min(lmin[q], 0); lmax[q] = max(lmax[q], 0); }
         float tu = (float)usum, ts = (float)ssum;
 #pragma unroll
         for (int q = 0; q < P; q++) {
