@@ -54,7 +54,8 @@ def test_noalloc_rejects_before_touching_the_device():
     assert lib.astcb200_encode_noalloc(0, None, 64, 64, 4, 4, ctypes.c_void_p(16), None) == ab.BAD_ARG
 
 
-def test_flop_model_matches_survey():
+def test_flop_model_per_block_totals():
+    """The op-count model's totals per block: 4.29 MFLOP at 4x4, 9.61 MFLOP at 6x6."""
     from astc_implementation_b200 import flop_model
     lib = ab.load_library()
     assert abs(flop_model.per_block(lib, 4, 4)["total"] / 1e6 - 4.29) < 0.01
