@@ -1,6 +1,6 @@
 // FP32 throughput probe: each thread runs independent chains of dependent FMAs.
-// Used only to measure the roofline denominator (the driver records HBM and
-// bf16 peaks but no FP32 figure).
+// Used only to measure the roofline denominator for the FP32-bound search kernels
+// (the recorded peaks of this GPU give HBM and bf16 figures but no FP32 one).
 #include <cuda_runtime.h>
 
 #include "astcb200.h"

@@ -5,7 +5,7 @@ and after `oracle/build_ref.sh` has built oracle/_ref/libastcref.so:
 
     python tests/golden/gen_reference_fixtures.py [/path/to/reference]
 
-Outputs (committed; the GPU box never reads the reference itself):
+Outputs (committed; the tests never read the reference itself):
   reference_tables.npz
     * constant tables transcribed from the reference's WGSL source text:
         quant_to_unquant        shaders/pass07_weights_and_error_for_bm.wgsl:12-37
