@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 __all__ = ["ASTCEncoder", "ASTCError", "store_image", "decode", "load_library", "VALID_FOOTPRINTS", "Texture",
-           "downsample_device", "mip_dims"]
+           "downsample_device", "mip_dims", "astc_containers_device"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libastcb200.so")
@@ -51,6 +51,13 @@ class Stats(ctypes.Structure):
 class Texture(ctypes.Structure):
     """astcb200_texture: one texture of a batch."""
     _fields_ = [("rgba8", ctypes.c_void_p), ("out_blocks", ctypes.c_void_p), ("out_len", ctypes.c_size_t),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("block_x", ctypes.c_uint8),
+                ("block_y", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6)]
+
+
+class AstcImage(ctypes.Structure):
+    """astcb200_astc_image: one image of astcb200_astc_containers_device."""
+    _fields_ = [("d_blocks", ctypes.c_void_p), ("host_out", ctypes.c_void_p), ("out_len", ctypes.c_size_t),
                 ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("block_x", ctypes.c_uint8),
                 ("block_y", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6)]
 
@@ -96,6 +103,7 @@ def load_library():
         "astcb200_encode_device": (I32, [P, P, P, P]),
         "astcb200_encode_symbolic": (I32, [P, P, P, SZ]),
         "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
+        "astcb200_astc_containers_device": (I32, [ctypes.POINTER(AstcImage), U32, P]),
         "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
         "astcb200_stage_times": (I32, [P, P, P]),
         "astcb200_stage_times_detail": (I32, [P, P, P]),
@@ -332,6 +340,20 @@ def store_image(block_x, block_y, dim_x, dim_y, data, filename):
     lib = load_library()
     buf = np.ascontiguousarray(data, dtype=np.uint8)
     _check(lib.astcb200_store_image(block_x, block_y, dim_x, dim_y, _ptr(buf), buf.size, os.fsencode(filename)))
+
+
+def astc_containers_device(images, stream=0):
+    """Queues the .astc containers of images whose blocks are in device memory:
+    [(d_blocks, host_out, width, height, block_x, block_y), ...] with integer device
+    addresses and host_out a writable uint8 array (pinned for an asynchronous copy) of at
+    least 16 + 16 * blocks bytes.  Synchronise `stream` before reading host_out."""
+    arr = (AstcImage * len(images))()
+    for i, (d_blocks, host_out, w, h, bx, by) in enumerate(images):
+        if not (isinstance(host_out, np.ndarray) and host_out.dtype == np.uint8 and host_out.flags.c_contiguous
+                and host_out.flags.writeable):
+            raise ASTCError(BAD_ARG, "host_out must be a writable contiguous uint8 array")
+        arr[i] = AstcImage(d_blocks, host_out.ctypes.data, host_out.size, w, h, bx, by)
+    _check(load_library().astcb200_astc_containers_device(arr, len(images), ctypes.c_void_p(stream or None)))
 
 
 def decode(block_x, block_y, dim_x, dim_y, blocks):

@@ -295,19 +295,47 @@ int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16) {
 }
 
 // astc_store.cpp:18-62: magic 0x5CA1AB13, block dims, 24-bit image dims, then the blocks.
+// The .astc header (astc_store.cpp:18-62): magic, block size, image size (24-bit little-endian).
+static void astc_header(uint32_t bx, uint32_t by, uint32_t dx, uint32_t dy, uint8_t* h) {
+    const uint32_t bz = 1, dz = 1, magic = 0x5CA1AB13u;
+    const uint8_t v[16] = {(uint8_t)(magic & 0xFF), (uint8_t)((magic >> 8) & 0xFF), (uint8_t)((magic >> 16) & 0xFF), (uint8_t)(magic >> 24),
+                           (uint8_t)bx, (uint8_t)by, (uint8_t)bz,
+                           (uint8_t)(dx & 0xFF), (uint8_t)((dx >> 8) & 0xFF), (uint8_t)((dx >> 16) & 0xFF),
+                           (uint8_t)(dy & 0xFF), (uint8_t)((dy >> 8) & 0xFF), (uint8_t)((dy >> 16) & 0xFF),
+                           (uint8_t)(dz & 0xFF), (uint8_t)((dz >> 8) & 0xFF), (uint8_t)((dz >> 16) & 0xFF)};
+    std::memcpy(h, v, 16);
+}
+
 int astcb200_store_image(uint32_t bx, uint32_t by, uint32_t dx, uint32_t dy, const uint8_t* data, size_t len, const char* filename) {
     if (!filename || (!data && len)) return ASTCB200_BAD_ARG;
-    const uint32_t bz = 1, dz = 1, magic = 0x5CA1AB13u;
-    uint8_t h[16] = {(uint8_t)(magic & 0xFF), (uint8_t)((magic >> 8) & 0xFF), (uint8_t)((magic >> 16) & 0xFF), (uint8_t)(magic >> 24),
-                     (uint8_t)bx, (uint8_t)by, (uint8_t)bz,
-                     (uint8_t)(dx & 0xFF), (uint8_t)((dx >> 8) & 0xFF), (uint8_t)((dx >> 16) & 0xFF),
-                     (uint8_t)(dy & 0xFF), (uint8_t)((dy >> 8) & 0xFF), (uint8_t)((dy >> 16) & 0xFF),
-                     (uint8_t)(dz & 0xFF), (uint8_t)((dz >> 8) & 0xFF), (uint8_t)((dz >> 16) & 0xFF)};
+    uint8_t h[16];
+    astc_header(bx, by, dx, dy, h);
     FILE* f = std::fopen(filename, "wb");
     if (!f) return ASTCB200_IO_ERROR;
     bool ok = std::fwrite(h, 1, 16, f) == 16 && (len == 0 || std::fwrite(data, 1, len, f) == len);
     ok = (std::fclose(f) == 0) && ok;
     return ok ? ASTCB200_OK : ASTCB200_IO_ERROR;
+}
+
+int astcb200_astc_containers_device(const astcb200_astc_image* images, uint32_t n, void* cuda_stream) {
+    if (!images && n) return ASTCB200_BAD_ARG;
+    for (uint32_t i = 0; i < n; i++) {  // every image is checked before anything is queued
+        const astcb200_astc_image& m = images[i];
+        if (!valid_footprint(m.block_x, m.block_y)) return ASTCB200_INVALID_FOOTPRINT;
+        if (!m.d_blocks || !m.host_out || m.width == 0 || m.height == 0 || m.width >= (1u << 24) || m.height >= (1u << 24))
+            return ASTCB200_BAD_ARG;
+        const uint64_t blocks = (uint64_t)((m.width + m.block_x - 1) / m.block_x) * ((m.height + m.block_y - 1) / m.block_y);
+        if (m.out_len < 16 + 16 * blocks) return ASTCB200_BAD_ARG;
+    }
+    const cudaStream_t s = (cudaStream_t)cuda_stream;
+    for (uint32_t i = 0; i < n; i++) {
+        const astcb200_astc_image& m = images[i];
+        const size_t blocks = (size_t)((m.width + m.block_x - 1) / m.block_x) * ((m.height + m.block_y - 1) / m.block_y);
+        astc_header(m.block_x, m.block_y, m.width, m.height, m.host_out);
+        if (cudaMemcpyAsync(m.host_out + 16, m.d_blocks, blocks * 16, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+            return ASTCB200_CUDA_ERROR;
+    }
+    return ASTCB200_OK;
 }
 
 }  // extern "C"

@@ -236,6 +236,23 @@ int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* 
 int astcb200_store_image(uint32_t block_x, uint32_t block_y, uint32_t dim_x, uint32_t dim_y,
                          const uint8_t* data, size_t data_len, const char* filename);
 
+/* .astc containers of images whose blocks are in device memory, for batch and mip-chain
+ * outputs (no reference counterpart: store_image above writes one image from host memory).
+ * For each image, host_out (pinned host memory for an asynchronous copy) receives the same
+ * 16 bytes store_image writes, then the image's blocks copied from d_blocks by one
+ * device-to-host copy queued on cuda_stream; the call returns once the copies are queued
+ * (synchronise the stream before reading host_out).  out_len must be at least
+ * 16 + 16 * blocks. */
+typedef struct astcb200_astc_image {
+    const uint8_t* d_blocks;  /* device, the image's blocks in raster order */
+    uint8_t* host_out;
+    size_t out_len;
+    uint32_t width, height;
+    uint8_t block_x, block_y;
+    uint8_t reserved[6];
+} astcb200_astc_image;
+int astcb200_astc_containers_device(const astcb200_astc_image* images, uint32_t n, void* cuda_stream);
+
 /* ASTC LDR decoder (no reference counterpart: the reference has none).  Decodes
  * blocks_x*blocks_y blocks of an image of dim_x*dim_y texels into rgba8_out
  * (dim_x*dim_y*4 bytes, UNORM8 with round-to-nearest from the 16-bit result). */

@@ -76,3 +76,16 @@ def test_work_counter_model_reproduces_the_per_block_model():
         pb = flop_model.per_block(lib, bx, by)
         for k in ("search", "front", "refine"):
             assert abs(f[k] - pb[k]) <= 1e-9 * pb[k], (bx, k)
+
+
+def test_astc_containers_argument_errors():
+    """astcb200_astc_containers_device checks every image before queuing any copy."""
+    lib = ab.load_library()
+    img = lambda d, h, n, w, hh, bx, by: (ab.AstcImage * 1)(ab.AstcImage(d, h, n, w, hh, bx, by))
+    assert lib.astcb200_astc_containers_device(img(16, 16, 100, 8, 8, 7, 7), 1, None) == ab.INVALID_FOOTPRINT
+    assert lib.astcb200_astc_containers_device(img(16, 16, 16 + 4 * 16 - 1, 8, 8, 4, 4), 1, None) == ab.BAD_ARG
+    assert lib.astcb200_astc_containers_device(img(0, 16, 100, 8, 8, 4, 4), 1, None) == ab.BAD_ARG
+    assert lib.astcb200_astc_containers_device(img(16, 0, 100, 8, 8, 4, 4), 1, None) == ab.BAD_ARG
+    assert lib.astcb200_astc_containers_device(img(16, 16, 100, 0, 8, 4, 4), 1, None) == ab.BAD_ARG
+    assert lib.astcb200_astc_containers_device(None, 1, None) == ab.BAD_ARG
+    assert lib.astcb200_astc_containers_device(None, 0, None) == ab.OK

@@ -132,6 +132,49 @@ def test_mip_chain_downsample_and_batch(enc):
         assert np.array_equal(o, single(enc, m, bx, by))
 
 
+def test_astc_containers_from_device_equal_store_image(enc, tmp_path):
+    """astcb200_astc_containers_device: header and blocks copied from device memory are the
+    bytes store_image writes for the same blocks."""
+    import torch
+    tex = textures(700)
+    d_img = [torch.from_numpy(img.reshape(-1)).cuda() for img, _, _ in tex]
+    nb = [((img.shape[1] + bx - 1) // bx) * ((img.shape[0] + by - 1) // by) for img, bx, by in tex]
+    d_out = [torch.empty(n * 16, dtype=torch.uint8, device="cuda") for n in nb]
+    s = torch.cuda.current_stream().cuda_stream
+    enc.encode_batch_device([(d_img[i].data_ptr(), img.shape[1], img.shape[0], bx, by, d_out[i].data_ptr(), nb[i] * 16)
+                             for i, (img, bx, by) in enumerate(tex)], s)
+    host = [torch.zeros(16 + n * 16, dtype=torch.uint8).pin_memory().numpy() for n in nb]
+    ab.astc_containers_device([(d_out[i].data_ptr(), host[i], img.shape[1], img.shape[0], bx, by)
+                               for i, (img, bx, by) in enumerate(tex)], s)
+    torch.cuda.synchronize()
+    for i, (img, bx, by) in enumerate(tex):
+        path = tmp_path / ("t%d.astc" % i)
+        ab.store_image(bx, by, img.shape[1], img.shape[0], single(enc, img, bx, by), str(path))
+        assert bytes(host[i]) == path.read_bytes()
+    with pytest.raises(ab.ASTCError):  # host_out too small
+        ab.astc_containers_device([(d_out[0].data_ptr(), host[0][:-1].copy(), 37, 19, 4, 4)], s)
+
+
+def test_mip_chain_astc_writer(enc, tmp_path):
+    """The mip-chain writer (downsampled, encoded and containerised on the device) gives,
+    per level, the file store_image writes for a single encode of that level."""
+    from astc_implementation_b200 import mipchain
+    img = synth.make_texture(45, 22, 33)
+    dims = ab.mip_dims(45, 22)
+    paths = [str(tmp_path / ("level%d.astc" % i)) for i in range(len(dims))]
+    files = mipchain.encode_mip_chain_astc(enc, img, 6, 6, paths=paths)
+    assert len(files) == len(dims)
+    ref = img
+    for i, ((w, h), data) in enumerate(zip(dims, files)):
+        if i:
+            ref = box_down(ref)
+        path = tmp_path / "ref.astc"
+        ab.store_image(6, 6, w, h, single(enc, ref, 6, 6), str(path))
+        assert data == path.read_bytes()
+        assert open(paths[i], "rb").read() == data
+    assert len(mipchain.encode_mip_chain_astc(enc, img, 4, 4, levels=2)) == 2
+
+
 def test_batch_argument_errors(enc):
     img = synth.make_texture(16, 16, 1)
     with pytest.raises(ab.ASTCError) as e:
