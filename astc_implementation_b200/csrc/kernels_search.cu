@@ -11,8 +11,9 @@
 //                       quantisation error, colour-format search, top-8 pick.
 //
 // Sums whose order the reference leaves to float atomics are taken in ascending
-// texel / weight order by a single thread, so results are bit-identical to the
-// CPU oracle (oracle/astc_oracle.cpp), which fixes the same order.
+// texel / weight order, each by one thread or lane, so results are bit-identical
+// to the CPU oracle (oracle/astc_oracle.cpp), which fixes the same order; integer
+// sums, whose order does not matter, may be split or regrouped.
 #include <algorithm>
 
 #include "device_math.cuh"
