@@ -34,6 +34,19 @@
 //      the per-invocation `avg`/`dir` arrays of pass006 (function-scope, so each
 //      invocation only sees its own partition's values, the rest zero), integer
 //      truncation of sums in pass003/006, pass17's float weight interpolation.
+//
+// The "FIXED" mode (orc_set_semantics(1)) keeps S1-S10 and repairs the
+// deterministic bugs whose intent the source makes evident:
+//  F1  REF-BUG-2: pass005 sorts all 1024 (score, index) pairs (the network of
+//      pass005:66-94 compares only pairs whose lower index is below 256).
+//  F2  REF-BUG-4: pass007 emits partition_ordering[rank], the table entry the
+//      candidate was evaluated for, not the rank (pass007:93,107,156-157).
+//  F3  REF-BUG-6: pass07 stores all W quantised weights (pass07:322 packs
+//      floor(W/4) words, so the tail weights read 0).
+//  F4  pass006 keeps `avg` and `dir` in function-scope arrays that each
+//      invocation fills only for its own index (pass006:124-135,186-217), so
+//      most texels see a zero average and direction; here every texel sees its
+//      partition's values, as the workgroup-wide sums they come from intend.
 #include "astc_oracle.h"
 
 #include <algorithm>
@@ -61,6 +74,10 @@ const float CW[4] = {0.30f * 2.25f, 0.59f * 2.25f, 0.11f * 2.25f, 1.0f};  // ast
 const int LEVELS[21] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256};
 const int STEPS_FOR_QUANT[12] = {2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32};  // astc.h:157
 const int FREE_BITS[4] = {111, 111 - 4 - 10, 108 - 4 - 10, 105 - 4 - 10};    // pass07:5
+
+// 0: REF semantics (the parity target), 1: FIXED (F1-F4 in the header).  Set before a call,
+// read by every thread of it.
+int g_fixed = 0;
 
 enum {
     FMT_LUMINANCE = 0, FMT_LUMINANCE_DELTA = 1, FMT_LUMINANCE_ALPHA = 4, FMT_LUMINANCE_ALPHA_DELTA = 5,
@@ -669,7 +686,8 @@ void make_pb(const Footprint& f, const InputBlock& blk, int P, int entry, InputB
 
 // ---------------------------------------------------------------- partition search, passes 001-007
 // Returns the number of partitioned blocks written to out[].
-int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBlock* out, uint32_t* entries_out) {
+int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBlock* out, uint32_t* entries_out,
+                     uint32_t* mismatch_out = nullptr, uint32_t* order_out = nullptr) {
     const int T = f.T;
     const v4* px = blk.px;
     // pass001_init_kmeans.wgsl:61-131
@@ -755,7 +773,13 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
     // pass005_partition_ordering.wgsl:35-94 (partial bitonic network, 256 invocations)
     uint32_t score[1024], index[1024];
     for (unsigned i = 0; i < 1024; i++) { index[i] = i; score[i] = i < sel ? mismatch[i] : 0xFFFFFFFFu; }
-    for (unsigned k = 2; k <= 1024; k *= 2)
+    if (g_fixed) {  // F1: the full ascending (score, index) order
+        std::vector<uint64_t> kv(1024);
+        for (unsigned i = 0; i < 1024; i++) kv[i] = (uint64_t)score[i] << 32 | i;
+        std::sort(kv.begin(), kv.end());
+        for (unsigned i = 0; i < 1024; i++) { score[i] = (uint32_t)(kv[i] >> 32); index[i] = (uint32_t)kv[i]; }
+    }
+    for (unsigned k = 2; k <= 1024 && !g_fixed; k *= 2)
         for (unsigned j = k / 2; j > 0; j /= 2)
             for (unsigned l = 0; l < 256; l++) {
                 unsigned partner = l ^ j;
@@ -765,6 +789,8 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
                     if (sw == asc) { std::swap(score[l], score[partner]); std::swap(index[l], index[partner]); }
                 }
             }
+    if (mismatch_out) for (unsigned i = 0; i < 1024; i++) mismatch_out[i] = i < sel ? mismatch[i] : 0xFFFFFFFFu;
+    if (order_out) for (int i = 0; i < PART_CAND_LIMIT; i++) order_out[i] = index[i];
     // pass006_evaluate_partition_candidates.wgsl:73-296
     float err_u[PART_CAND_LIMIT], err_s[PART_CAND_LIMIT];
     float wie = T <= 20 ? 0.03f : T <= 31 ? 0.04f : T <= 41 ? 0.05f : 0.055f;
@@ -783,7 +809,8 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
             if (c > 0.0f) tavg[p] = {(float)sums[p][0] / c, (float)sums[p][1] / c, (float)sums[p][2] / c, (float)sums[p][3] / c};
         }
         // per-invocation view (S11): invocation t sees avg[q] only for q == t < P
-        auto own = [&](int t, uint32_t p) { return t < P && (int)p == t; };
+        // (FIXED, F4: every texel sees its partition's average and direction)
+        auto own = [&](int t, uint32_t p) { return g_fixed || (t < P && (int)p == t); };
         int32_t axis[4][4][4] = {{{0}}};
         for (int t = 0; t < T; t++) {
             uint32_t p = pi.of_texel[t];
@@ -830,7 +857,7 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
             float tpp = (float)pi.texel_count[p];
             float ew = tpp * wie;
             tu = tu + ew * (ll * ll);
-            v4 a0 = (p == 0) ? tavg[0] : V(0.0f);  // invocation 0's private avg array
+            v4 a0 = (p == 0 || g_fixed) ? tavg[p] : V(0.0f);  // invocation 0's private avg array (F4: all)
             ts = ts + ew * dot4(a0, a0);
         }
         err_u[cand] = tu; err_s[cand] = ts;
@@ -858,8 +885,10 @@ int partition_search(const Footprint& f, const InputBlock& blk, int P, InputBloc
         if (!written) { fin[emitted++] = idx; if (emitted >= req) break; }
     }
     for (int i = 0; i < emitted; i++) {
-        make_pb(f, blk, P, (int)fin[i], out[i]);  // REF-BUG-4: rank used as table index
-        if (entries_out) entries_out[i] = (P - 2) * 1024 + fin[i];
+        // REF-BUG-4: rank used as table index (FIXED, F2: the ordered entry)
+        const uint32_t entry = g_fixed ? index[fin[i]] : fin[i];
+        make_pb(f, blk, P, (int)entry, out[i]);
+        if (entries_out) entries_out[i] = (P - 2) * 1024 + entry;
     }
     return emitted;
 }
@@ -1072,7 +1101,7 @@ void pass07(const Footprint& f, const InputBlock& b, PBWork& w, int P, uint32_t 
         err = err + (d * d) * es;
     }
     r.error = err; r.bitcount = bc;
-    uint32_t nw = (di.W / 4) * 4;  // REF-BUG-6
+    uint32_t nw = g_fixed ? di.W : (di.W / 4) * 4;  // REF-BUG-6 (FIXED, F3: every weight)
     for (uint32_t i = 0; i < nw; i++) r.qw[i] = qi[i];
 }
 
@@ -2017,6 +2046,12 @@ void run_parallel(int n, int threads, F fn) {
 
 extern "C" {
 
+int orc_set_semantics(int fixed) {
+    const int prev = g_fixed;
+    g_fixed = fixed ? 1 : 0;
+    return prev;
+}
+
 int orc_encode(const uint8_t* rgba, int width, int height, int bx, int by, int threads,
                uint8_t* out_blocks, uint32_t* symbolic) {
     if (!rgba || width <= 0 || height <= 0 || !valid_footprint(bx, by) || !out_blocks) return -1;
@@ -2195,6 +2230,17 @@ int orc_partition_search(int bx, int by, const float* texels, int P, uint32_t* e
     flags_from_texels(b, f.T);
     std::unique_ptr<InputBlock[]> out(new InputBlock[4]);
     return partition_search(f, b, P, out.get(), entries);
+}
+int orc_partition_order(int bx, int by, const float* texels, int P, uint32_t* mismatch, uint32_t* order) {
+    if (!valid_footprint(bx, by) || P < 2 || P > 4 || !mismatch || !order) return -1;
+    const Footprint& f = *get_fp(bx, by);
+    InputBlock b; std::memset(&b, 0, sizeof(b));
+    for (int t = 0; t < f.T; t++) for (int c = 0; c < 4; c++) comp(b.px[t], c) = texels[t * 4 + c];
+    flags_from_texels(b, f.T);
+    std::unique_ptr<InputBlock[]> out(new InputBlock[4]);
+    uint32_t entries[4];
+    partition_search(f, b, P, out.get(), entries, mismatch, order);
+    return (int)f.count_selected[P - 1];
 }
 
 }  // extern "C"

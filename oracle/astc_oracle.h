@@ -25,6 +25,13 @@ extern "C" {
 // One SymbolicBlock in the reference layout (code/astc.h:639-655): 108 u32.
 #define ORC_SYMBOLIC_WORDS 108
 
+// Selects the semantics of every later call: 0 = REF (the parity target, the default),
+// 1 = FIXED (REF plus the repairs F1-F4 listed in astc_oracle.cpp: full pass005 sort,
+// pass007 emits the ordered table entry, pass07 keeps every weight, pass006 sees every
+// partition's average and direction).  Returns the previous setting.  Not thread-safe:
+// set it between calls.
+int orc_set_semantics(int fixed);
+
 // Encodes an RGBA8 image (row-major, 4 bytes per texel) into physical ASTC
 // blocks (16 bytes each, blocks in raster order).  `threads` <= 0 uses all
 // OpenMP threads.  `symbolic` (optional) receives ORC_SYMBOLIC_WORDS u32 per block.
@@ -76,6 +83,10 @@ int orc_const_tables(int32_t* q2u, int32_t* qmt, int32_t* cu2u, int32_t* prev_ne
 // Partition search for one block and one partition count (passes 001-007):
 // returns the number of partitioned blocks (<= 4) and their packed table entries.
 int orc_partition_search(int bx, int by, const float* texels, int partition_count, uint32_t* entries);
+// The same search's intermediate order: mismatch[1024] (pass004, 0xFFFFFFFF past the
+// selected partitionings) and order[128] (pass005's first 128 table entries, in the
+// current semantics).  Returns the number of selected partitionings.
+int orc_partition_order(int bx, int by, const float* texels, int partition_count, uint32_t* mismatch, uint32_t* order);
 
 #ifdef __cplusplus
 }
