@@ -66,7 +66,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("chunk_blocks", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("ms", ctypes.c_double)]
 
 
-FLAG_STAGE_TIMING, FLAG_NO_GRAPH = 1, 2
+FLAG_STAGE_TIMING, FLAG_NO_GRAPH, FLAG_FIXED_SEMANTICS = 1, 2, 4
 
 
 class ProposalNet(ctypes.Structure):
@@ -157,14 +157,18 @@ def _ptr(a):
 class ASTCEncoder:
     """One encoder context bound to one GPU and one CUDA stream."""
 
-    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False, use_graphs=True):
+    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False, use_graphs=True, fixed=False):
+        """fixed=True selects the search with the reference's deterministic shader bugs repaired
+        (ASTCB200_FLAG_FIXED_SEMANTICS); the default reproduces the reference bit for bit."""
         lib = load_library()
-        flags = (FLAG_STAGE_TIMING if stage_timing else 0) | (0 if use_graphs else FLAG_NO_GRAPH)
+        flags = ((FLAG_STAGE_TIMING if stage_timing else 0) | (0 if use_graphs else FLAG_NO_GRAPH)
+                 | (FLAG_FIXED_SEMANTICS if fixed else 0))
         cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, flags)
         ctx = ctypes.c_void_p()
         _check(lib.astcb200_create(ctypes.byref(ctx), device, ctypes.byref(cfg)))
         self._ctx = ctx
         self.device = device
+        self.fixed = bool(fixed)
         self.blocksX = self.blocksY = self.numBlocks = 0
         self.textureWidth = self.textureHeight = 0
         self.blockXDim = self.blockYDim = 4

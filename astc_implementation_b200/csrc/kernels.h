@@ -96,6 +96,7 @@ struct KernelArgs {
     unsigned long long* work;
     int front_threads;        // threads per front CTA: 128 (0 selects it), 64 or 32
     int refine_iters;         // refinement iterations (0 selects the reference's 6)
+    int fixed;                // 1: FIXED semantics (ASTCB200_FLAG_FIXED_SEMANTICS), 0: the reference's
 };
 constexpr int kWorkCounters = 16;
 

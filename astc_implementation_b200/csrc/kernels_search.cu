@@ -78,7 +78,46 @@ __device__ __forceinline__ float dist_sq(float4 a, float4 b) {
 
 // ============================================================ passes 001-007
 constexpr int kSearchWarps = 4;
-constexpr int kSearchWarpBytes = 144 * 16 + 1024 * 8 + 128 * 4 * 2 + 160;
+// Per warp: texels, 1024 sort keys, 128 + 128 candidate errors, k-means assignments, then
+// (FIXED semantics) the 128 first keys of the full order and a 132-bin histogram.
+constexpr int kSearchWarpBytes = 144 * 16 + 1024 * 8 + 128 * 4 * 2 + 160 + 128 * 8 + 132 * 4;
+
+// FIXED semantics of pass005 (full sort): the first 128 of all 1024 keys m << 32 | i in
+// ascending order, into ord.  The mismatch counts m of the sel selected entries are at most
+// 128 (the sum of P popcounts of 64-bit words, halved), so a stable counting sort by m in
+// index order gives the full order; entries i >= sel (m = 0xFFFFFFFF) keep rank i.
+__device__ void full_order(const unsigned long long* key, unsigned long long* ord, uint32_t* hist, uint32_t sel, int lane) {
+    for (int b = lane; b < 132; b += 32) hist[b] = 0;
+    __syncwarp();
+    for (uint32_t i = lane; i < sel; i += 32) atomicAdd(&hist[(uint32_t)(key[i] >> 32)], 1u);
+    __syncwarp();
+    uint32_t v[5], s = 0;  // exclusive scan of bins 0..128, five per lane
+#pragma unroll
+    for (int j = 0; j < 5; j++) { const int b = lane * 5 + j; v[j] = b < 129 ? hist[b] : 0u; s += v[j]; }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) { const uint32_t t = __shfl_up_sync(FULL, incl, o); if (lane >= o) incl += t; }
+    uint32_t run = incl - s;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 5; j++) { const int b = lane * 5 + j; if (b < 129) hist[b] = run; run += v[j]; }
+    __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t end = sel > 128u ? sel : 128u;
+    for (uint32_t base = 0; base < end; base += 32) {
+        const uint32_t i = base + lane;
+        const unsigned long long k = key[i];
+        const uint32_t m = (uint32_t)(k >> 32);
+        const bool selected = i < sel;
+        const uint32_t grp = __match_any_sync(FULL, selected ? m : 0xFFFFFFFFu);
+        const uint32_t rank = selected ? hist[m] + __popc(grp & lt) : i;
+        if (rank < 128u) ord[rank] = k;
+        __syncwarp();
+        if (selected && 31 - __clz(grp) == lane) hist[m] += __popc(grp);
+        __syncwarp();
+    }
+    __syncwarp();
+}
 
 template <int P>
 __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, int lane) {
@@ -89,6 +128,8 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
     float* eu = reinterpret_cast<float*>(ws + 144 * 16 + 1024 * 8);
     float* es = eu + 128;
     uint8_t* asg = reinterpret_cast<uint8_t*>(es + 128);
+    unsigned long long* ord_buf = reinterpret_cast<unsigned long long*>(ws + 144 * 16 + 1024 * 8 + 128 * 4 * 2 + 160);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ord_buf + 128);
     const BlockSrc src = block_src(a, blk);
     for (int t = lane; t < T; t += 32) px[t] = src_texel(src, a.L.bx, t);
     __syncwarp();
@@ -204,8 +245,14 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
         key[i] = ((unsigned long long)m << 32) | (uint32_t)i;
     }
     __syncwarp();
-    // pass005: the reference's bitonic network run by 256 invocations (a partial sort)
-    for (unsigned k = 2; k <= 1024; k <<= 1)
+    // pass005: the reference's bitonic network run by 256 invocations (a partial sort); FIXED
+    // semantics: the full order
+    const unsigned long long* ord = key;
+    if (a.fixed) {
+        full_order(key, ord_buf, hist, sel, lane);
+        ord = ord_buf;
+    }
+    for (unsigned k = 2; k <= 1024 && !a.fixed; k <<= 1)
         for (unsigned j = k >> 1; j > 0; j >>= 1) {
 #pragma unroll
             for (int r = 0; r < 8; r++) {
@@ -229,7 +276,7 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
     for (int o = 16; o > 0; o >>= 1) u_all += __shfl_xor_sync(FULL, u_all, o);
     for (int r = 0; r < 4; r++) {
         const int cand = lane + 32 * r;
-        const int e = (int)(uint32_t)key[cand];
+        const int e = (int)(uint32_t)ord[cand];
         const uint8_t* row = tb.part_texels(P, e);
         uint32_t cnt[P], sm[P][4];
 #pragma unroll
@@ -254,7 +301,7 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
             for (int u = 0; u < 4; u++) ax[u][0] = ax[u][1] = ax[u][2] = ax[u][3] = 0;
             for (int t = 0; t < T; t++) {
                 if (row[t] != q) continue;
-                const float4 av = (t == q) ? tavg[q] : mk(0.0f);
+                const float4 av = (a.fixed || t == q) ? tavg[q] : mk(0.0f);
                 const float4 d = px[t] - av;
                 const uint32_t d0 = (uint32_t)f2i(d.x), d1 = (uint32_t)f2i(d.y), d2 = (uint32_t)f2i(d.z), d3 = (uint32_t)f2i(d.w);
                 if (d.x > 0.0f) { ax[0][0] += d0; ax[0][1] += d1; ax[0][2] += d2; ax[0][3] += d3; }
@@ -281,8 +328,31 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
         int32_t lmin[P], lmax[P];
 #pragma unroll
         for (int q = 0; q < P; q++) { lmin[q] = 2147483647; lmax[q] = -2147483647; }
+        if (a.fixed) {  // every texel sees its partition's average and direction
+            float4 sdir[P];
 #pragma unroll
-        for (int t = 0; t < P; t++) {
+            for (int q = 0; q < P; q++) sdir[q] = normalize4(tavg[q]);
+            usum = 0u; ssum = 0u;
+            for (int t = 0; t < T; t++) {
+                const int p = row[t];
+                float4 av = tavg[0], ud = tdir[0], sd = sdir[0];
+#pragma unroll
+                for (int q = 1; q < P; q++) if (p == q) { av = tavg[q]; ud = tdir[q]; sd = sdir[q]; }
+                const float4 x = px[t];
+                const float up = dot4(x, ud);
+                const float4 uproj = av + ud * dot4(x - av, ud);
+                const float4 udiff = x - uproj;
+                usum += f2u(dot4(udiff * udiff, cw));
+                const float4 sproj = sd * dot4(x, sd);
+                const float4 sdiff = x - sproj;
+                ssum += f2u(dot4(sdiff * sdiff, cw));
+                const int32_t upi = f2i(up * 4096.0f);
+#pragma unroll
+                for (int q = 0; q < P; q++) if (p == q) { lmin[q] = min(lmin[q], upi); lmax[q] = max(lmax[q], upi); }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < P && !a.fixed; t++) {
             if (row[t] != t) continue;
             const float4 av = tavg[t], ud = tdir[t];
             const float4 x = px[t];
@@ -303,7 +373,7 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
         }
 #pragma unroll
         for (int q = 0; q < P; q++)  // the partition has a texel of projection 0
-            if (tb.part_count(P, e, q) > (row[q] == q ? 1 : 0)) { lmin[q] = min(lmin[q], 0); lmax[q] = max(lmax[q], 0); }
+            if (!a.fixed && tb.part_count(P, e, q) > (row[q] == q ? 1 : 0)) { lmin[q] = min(lmin[q], 0); lmax[q] = max(lmax[q], 0); }
         float tu = (float)usum, ts = (float)ssum;
 #pragma unroll
         for (int q = 0; q < P; q++) {
@@ -311,7 +381,7 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
             const float ll = fmaxf(mxv - mn, 1e-7f);
             const float ew = (float)tb.part_count(P, e, q) * wie;
             tu = tu + ew * (ll * ll);
-            const float4 a0 = q == 0 ? tavg[0] : mk(0.0f);
+            const float4 a0 = (q == 0 || a.fixed) ? tavg[q] : mk(0.0f);
             ts = ts + ew * dot4(a0, a0);
         }
         eu[cand] = tu;
@@ -345,7 +415,8 @@ __device__ void search_one(const KernelArgs& a, int blk, int lb, uint8_t* ws, in
             if (!seen) fin[emitted++] = idx;
         }
         uint16_t* out = a.picks[lb].v + (P - 2) * 5;
-        for (int i = 0; i < 4; i++) out[i] = (uint16_t)fin[i];
+        // FIXED semantics: the table entry the candidate was evaluated for
+        for (int i = 0; i < 4; i++) out[i] = (uint16_t)(a.fixed && i < emitted ? (uint32_t)ord[fin[i]] : fin[i]);
         out[4] = (uint16_t)emitted;
     }
 }
@@ -1161,7 +1232,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
     if (tid < 4) { rec.avg[tid] = M.avg[tid]; rec.ep0[tid] = M.ep0[tid]; rec.ep1[tid] = M.ep1[tid]; }
     __syncthreads();
     // candidate initial state: the trial's quantised weights (REF-BUG-6: only
-    // floor(W/4)*4 weights are packed by pass07, the rest read as 0)
+    // floor(W/4)*4 weights are packed by pass07, the rest read as 0; FIXED semantics: all W)
     const int ncand = M.ncand;
     for (int k = tid >> 3; k < ncand; k += kFrontThreads / 8) {
         const int i = M.top[k];
@@ -1173,7 +1244,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
             for (int f = 0; f < 4; f++) c.fmt[f] = ccr_fmt[i * 4 + f];
         }
         const BmQuant s = bm_quant_setup(tb, bm, lov + bm.dm * 8, hiv + bm.dm * 8, M.min_cutoff);
-        const int packed_w = (dmi.W / 4) * 4;
+        const int packed_w = a.fixed ? dmi.W : (dmi.W / 4) * 4;
         for (int w = tid & 7; w < 64; w += 8) {
             int v = 0;
             if (w < packed_w) { float qf; v = bm_quant_weight(tb, s, dec[bm.dm * 64 + w], &qf); }

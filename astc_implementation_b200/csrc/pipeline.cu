@@ -57,6 +57,7 @@ int begin_routes(astcb200_ctx* ctx, size_t chunks) {
 int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* ft, Scratch& sc, cudaStream_t s,
                   cudaEvent_t* ev, int8_t* kinds, uint32_t* launches, bool full_only) {
     KernelArgs a = base;
+    a.fixed = (ctx->cfg.flags & ASTCB200_FLAG_FIXED_SEMANTICS) ? 1 : 0;
     a.tables = ft->d;
     a.L = ft->L;
     a.picks = sc.picks;

@@ -44,6 +44,20 @@ typedef struct astcb200_config {
 #define ASTCB200_FLAG_STAGE_TIMING 1u
 /* Batched encodes launch their kernels directly instead of replaying a captured CUDA graph. */
 #define ASTCB200_FLAG_NO_GRAPH 2u
+/* FIXED semantics: the search with four deterministic bugs of the reference's shaders
+ * repaired (the default reproduces them, bit for bit):
+ *   - pass005 sorts all 1024 candidates (shaders/pass005_partition_ordering.wgsl:66-94
+ *     runs a bitonic network whose comparisons stop at index 256, a partial sort);
+ *   - pass007 emits the table entry each candidate was evaluated for, not its rank
+ *     (pass007_prepare_partitioned_blocks.wgsl:93,107,156-157);
+ *   - pass07 keeps all of a block mode's quantised weights, not floor(W/4)*4 of them
+ *     (pass07_weights_and_error_for_bm.wgsl:322);
+ *   - pass006's error estimate sees every partition's average and direction (its
+ *     per-invocation arrays, pass006_evaluate_partition_candidates.wgsl:124-135,186-217,
+ *     leave all but one texel per partition with zeros).
+ * Partitionings then come from the k-means mismatch order and the error estimate as
+ * designed; decoded quality rises by several dB on most images. */
+#define ASTCB200_FLAG_FIXED_SEMANTICS 4u
 
 typedef struct astcb200_stats {
     double ms_wall;       /* host time of the call */
