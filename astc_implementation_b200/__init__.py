@@ -99,6 +99,8 @@ def load_library():
         "astcb200_destroy": (I32, [P]),
         "astcb200_set_image": (I32, [P, U32, U32, ctypes.c_uint8, ctypes.c_uint8]),
         "astcb200_blocks": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+        "astcb200_set_timeout": (I32, [P, U32]),
+        "astcb200_set_inference_wait_limit": (I32, [P, U32]),
         "astcb200_encode": (I32, [P, P, P, SZ, ctypes.POINTER(Stats)]),
         "astcb200_encode_device": (I32, [P, P, P, P]),
         "astcb200_encode_symbolic": (I32, [P, P, P, SZ]),
@@ -326,6 +328,14 @@ class ASTCEncoder:
         c = np.zeros(16, np.uint64)
         _check(load_library().astcb200_work_counters(self._ctx, _ptr(c)), self._ctx)
         return c
+
+    def set_inference_wait_limit(self, polls):
+        """Polls per mbarrier wait of the inference kernel before a CTA gives up (0 = default)."""
+        _check(load_library().astcb200_set_inference_wait_limit(self._ctx, int(polls)), self._ctx)
+
+    def set_timeout(self, timeout_ms):
+        """Bound (ms) on each later host wait; 0 = none (astcb200_set_timeout)."""
+        _check(load_library().astcb200_set_timeout(self._ctx, int(timeout_ms)), self._ctx)
 
     def close(self):
         if getattr(self, "_ctx", None):

@@ -107,7 +107,7 @@ int make_plan(astcb200_ctx* ctx, const astcb200_texture* tex, uint32_t n, bool d
 }
 
 // Streams, events and per-stream scratch for `streams` streams of `chunk` blocks.
-int prepare(astcb200_ctx* ctx, const Plan& p, uint32_t chunk, uint32_t streams) {
+int prepare(astcb200_ctx* ctx, const Plan& p, uint32_t chunk, uint32_t streams, cudaStream_t s) {
     while (ctx->branch.size() + 1 < streams) {
         cudaStream_t s;
         CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -129,7 +129,7 @@ int prepare(astcb200_ctx* ctx, const Plan& p, uint32_t chunk, uint32_t streams) 
         }
     size_t units = 0;
     for (const Group& g : p.groups) units += (g.nblocks + chunk - 1) / chunk;
-    int rc = begin_routes(ctx, units);
+    int rc = begin_routes(ctx, units, s);
     if (rc) return rc;
     return ensure_buf(ctx, ctx->d_segs, ctx->segs_cap, p.segs.size() * sizeof(TexSeg), "cudaMalloc batch descriptors");
 }
@@ -193,7 +193,7 @@ BatchTuning default_tuning(astcb200_ctx* ctx, const Plan& p) {
 
 // Uploads the descriptors and queues (or replays) the batch on stream s.
 int launch_plan(astcb200_ctx* ctx, Plan& p, cudaStream_t s, const BatchTuning& tu, bool use_graph, uint32_t* launches) {
-    int rc = prepare(ctx, p, tu.chunk, tu.streams);
+    int rc = prepare(ctx, p, tu.chunk, tu.streams, s);
     if (rc) return rc;
     // pageable source: the descriptors are consumed before the call returns
     CK(cudaMemcpyAsync(ctx->d_segs, p.segs.data(), p.segs.size() * sizeof(TexSeg), cudaMemcpyHostToDevice, s), "upload batch descriptors");
@@ -245,7 +245,7 @@ extern "C" {
 
 int astcb200_encode_batch_device(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n, void* cuda_stream) {
     if (!ctx) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     Plan p;
     int rc = make_plan(ctx, textures, n, true, p);
     if (rc) return rc;
@@ -256,7 +256,7 @@ int astcb200_encode_batch_device(astcb200_ctx* ctx, const astcb200_texture* text
 int astcb200_encode_batch(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n, astcb200_stats* stats) {
     if (!ctx) return ASTCB200_BAD_ARG;
     const auto t0 = std::chrono::steady_clock::now();
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     Plan check;
     int rc = make_plan(ctx, textures, n, false, check);
     if (rc) return rc;
@@ -284,9 +284,11 @@ int astcb200_encode_batch(astcb200_ctx* ctx, const astcb200_texture* textures, u
     uint32_t launches = 0;
     if ((rc = launch_plan(ctx, p, ctx->stream, default_tuning(ctx, p), !(ctx->cfg.flags & ASTCB200_FLAG_NO_GRAPH), &launches))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
-    for (uint32_t i = 0; i < n; i++)
-        CK(cudaMemcpyAsync(textures[i].out_blocks, dev[i].out_blocks, dev[i].out_len, cudaMemcpyDeviceToHost, ctx->stream), "D2H blocks");
+    HostResults res;
+    for (uint32_t i = 0; i < n; i++) res.add(textures[i].out_blocks, dev[i].out_blocks, dev[i].out_len);
+    if ((rc = res.queue(ctx, ctx->stream))) return rc;
     if ((rc = wait_stream(ctx, ctx->stream))) return rc;
+    res.finish(ctx);
     if (stats) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -305,7 +307,7 @@ int astcb200_encode_batch(astcb200_ctx* ctx, const astcb200_texture* textures, u
 int astcb200_autotune_batch(astcb200_ctx* ctx, const astcb200_texture* textures, uint32_t n, astcb200_tuning* best,
                             astcb200_tuning* tried, uint32_t max_tried, uint32_t* n_tried) {
     if (!ctx || !best) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     Plan p;
     int rc = make_plan(ctx, textures, n, true, p);
     if (rc) return rc;

@@ -41,6 +41,34 @@ int wait_stream(astcb200_ctx* ctx, cudaStream_t s) {
     }
 }
 
+int HostResults::queue(astcb200_ctx* ctx, cudaStream_t s) {
+    size_t need = 0;
+    for (Item& it : items) {
+        cudaPointerAttributes at{};
+        it.pinned = cudaPointerGetAttributes(&at, it.dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+        cudaGetLastError();  // an unregistered pointer is not an error here
+        if (!it.pinned) { it.off = need; need += (it.bytes + 255) & ~(size_t)255; }
+    }
+    if (need > ctx->stage_cap) {
+        // an earlier call that timed out may still be copying into the old buffer
+        CK(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->stage_cap = 0;
+        CK(cudaHostAlloc((void**)&ctx->h_stage, need, cudaHostAllocDefault), "cudaHostAlloc staging");
+        ctx->stage_cap = need;
+    }
+    for (const Item& it : items)
+        CK(cudaMemcpyAsync(it.pinned ? it.dst : (void*)(ctx->h_stage + it.off), it.src, it.bytes, cudaMemcpyDeviceToHost, s),
+           "D2H results");
+    return ASTCB200_OK;
+}
+
+void HostResults::finish(astcb200_ctx* ctx) const {
+    for (const Item& it : items)
+        if (!it.pinned) std::memcpy(it.dst, ctx->h_stage + it.off, it.bytes);
+}
+
 // Tables of footprint bx x by on the context's device, built and uploaded on first use.
 int get_tables(astcb200_ctx* ctx, int bx, int by, const FootTables** out) {
     for (const FootTables* f : ctx->feet)
@@ -85,7 +113,7 @@ int run_search(astcb200_ctx* ctx, const uint8_t* d_img, uint8_t* d_out, uint32_t
     const int nchunks = (int)((ctx->nblocks + ctx->chunk - 1) / ctx->chunk);
     int rc = ensure_chunk_scratch(ctx, ctx->scratch, std::min<size_t>(ctx->chunk, ctx->nblocks), ctx->cur);
     if (rc) return rc;
-    if ((rc = begin_routes(ctx, nchunks))) return rc;
+    if ((rc = begin_routes(ctx, nchunks, s))) return rc;
     constexpr int E = kStageIntervals + 1;
     if (timing) {
         if (!ctx->d_work) CK(cudaMalloc((void**)&ctx->d_work, kWorkCounters * sizeof(unsigned long long)), "cudaMalloc work counters");
@@ -145,7 +173,8 @@ int astcb200_create(astcb200_ctx** out, int device_ordinal, const astcb200_confi
     ctx->chunk = ctx->cfg.chunk_blocks ? ctx->cfg.chunk_blocks : 65536;
     ctx->device = device_ordinal;
     int rc = ASTCB200_OK;
-    cudaError_t e = cudaSetDevice(device_ordinal);
+    DeviceGuard dg(device_ordinal);
+    cudaError_t e = dg.err;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
@@ -156,7 +185,7 @@ int astcb200_create(astcb200_ctx** out, int device_ordinal, const astcb200_confi
 
 int astcb200_destroy(astcb200_ctx* ctx) {
     if (!ctx) return ASTCB200_BAD_ARG;
-    cudaSetDevice(ctx->device);
+    DeviceGuard dg(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     release_batches(ctx);
     free_scratch(ctx->scratch);
@@ -164,6 +193,7 @@ int astcb200_destroy(astcb200_ctx* ctx) {
     for (NetDev* nd : ctx->nets) { cudaFree(nd->mem); delete nd; }
     cudaFree(ctx->d_counts); cudaFree(ctx->d_mlp_error); cudaFree(ctx->d_work);
     cudaFree(ctx->d_img); cudaFree(ctx->d_out); cudaFree(ctx->d_sym);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (cudaEvent_t e : ctx->stage_ev) cudaEventDestroy(e);
@@ -177,7 +207,7 @@ int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8
     if (!valid_footprint(block_x, block_y)) return ASTCB200_INVALID_FOOTPRINT;
     const uint64_t nbx = (width + block_x - 1) / block_x, nby = (height + block_y - 1) / block_y;
     if (nbx * nby > 0x7FFFFFFFull) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     const FootTables* ft = nullptr;
     int rc = get_tables(ctx, block_x, block_y, &ft);
     if (rc) return rc;
@@ -185,6 +215,12 @@ int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8
     ctx->width = width; ctx->height = height; ctx->bx = block_x; ctx->by = block_y;
     ctx->nbx = (uint32_t)nbx; ctx->nby = (uint32_t)nby; ctx->nblocks = (uint32_t)(nbx * nby);
     ctx->have_image = true;
+    return ASTCB200_OK;
+}
+
+int astcb200_set_timeout(astcb200_ctx* ctx, uint32_t timeout_ms) {
+    if (!ctx) return ASTCB200_BAD_ARG;
+    ctx->cfg.timeout_ms = timeout_ms;
     return ASTCB200_OK;
 }
 
@@ -199,14 +235,14 @@ int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d
     if (!ctx || !d_rgba8 || !d_out) return ASTCB200_BAD_ARG;
     if (!ctx->have_image) return ASTCB200_NO_IMAGE;
     if (((uintptr_t)d_rgba8 & 3) || ((uintptr_t)d_out & 15)) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     return run_search(ctx, d_rgba8, d_out, nullptr, s, nullptr);
 }
 
 static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks, uint32_t* symbolic, astcb200_stats* stats) {
     const auto t0 = std::chrono::steady_clock::now();
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     const size_t in_bytes = (size_t)ctx->width * ctx->height * 4, out_bytes = (size_t)ctx->nblocks * 16;
     int rc;
     if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
@@ -217,9 +253,12 @@ static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blo
     uint32_t launches = 0;
     if ((rc = run_search(ctx, ctx->d_img, ctx->d_out, symbolic ? ctx->d_sym : nullptr, ctx->stream, &launches))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
-    if (out_blocks) CK(cudaMemcpyAsync(out_blocks, ctx->d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H blocks");
-    if (symbolic) CK(cudaMemcpyAsync(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H symbolic");
+    HostResults res;
+    if (out_blocks) res.add(out_blocks, ctx->d_out, out_bytes);
+    if (symbolic) res.add(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4);
+    if ((rc = res.queue(ctx, ctx->stream))) return rc;
     if ((rc = wait_stream(ctx, ctx->stream))) return rc;
+    res.finish(ctx);
     if (stats) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -288,7 +327,7 @@ int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16) {
     if (!ctx || !counters16) return ASTCB200_BAD_ARG;
     for (int i = 0; i < kWorkCounters; i++) counters16[i] = 0;
     if (!ctx->d_work) return ASTCB200_OK;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     CK(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
     CK(cudaMemcpy(counters16, ctx->d_work, kWorkCounters * sizeof(uint64_t), cudaMemcpyDeviceToHost), "read work counters");
     return ASTCB200_OK;

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "astcb200.h"
+#include "device_guard.h"
 #include "kernels.h"
 #include "mlp.h"
 #include "tables.h"
@@ -113,8 +114,13 @@ struct astcb200_ctx {
     int* d_counts = nullptr;     // [chunks][mlp::kRouteCounters] routed blocks of the last encode
     size_t counts_cap = 0;
     uint32_t counts_used = 0;    // chunk entries written by the last encode
-    int* d_mlp_error = nullptr;  // set by an inference CTA that gave up waiting
+    int* d_mlp_error = nullptr;  // [0] set by an inference CTA that gave up waiting, [1] its wait limit
     unsigned long long* d_work = nullptr;  // work counters of the last timed encode (kWorkCounters)
+    // Pinned staging for results bound for pageable host memory: the device-to-host copies
+    // stay asynchronous (so a bounded wait can time out) and a call that times out never
+    // writes into the caller's buffers afterwards.
+    uint8_t* h_stage = nullptr;
+    size_t stage_cap = 0;
     std::string err;
 };
 
@@ -127,8 +133,12 @@ int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots);
 // Scratch for `blocks` blocks per chunk of footprint ft (proposal buffers when it is pruned).
 int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const FootTables* ft);
 const NetDev* net_for(const astcb200_ctx* ctx, const FootTables* ft);  // null: full search
-// Room for `chunks` route counters; resets the per-call counter index.
-int begin_routes(astcb200_ctx* ctx, size_t chunks);
+// Room for `chunks` route counters; resets the per-call counter index and (on stream s)
+// the inference kernel's give-up flag.
+int begin_routes(astcb200_ctx* ctx, size_t chunks, cudaStream_t s);
+// The inference kernel's flag pair: [0] set by a CTA that gave up waiting, [1] the polls
+// per wait (0: the default 2^24).
+int ensure_error_flag(astcb200_ctx* ctx);
 // Stage timing: per chunk, an event before the first launch and after each launch
 // (at most kStageIntervals launches), and the stage (0 partition search or network, 1
 // front, 2 refine, 3 select-pack) of each launch, -1 past the last.
@@ -140,6 +150,17 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
                   cudaEvent_t* ev, int8_t* kinds, uint32_t* launches, bool full_only = false);
 void free_scratch(Scratch& sc);
 void release_batches(astcb200_ctx* ctx);
+
+// Device-to-host results of one call.  Pinned destinations are copied into directly;
+// pageable ones go through ctx->h_stage and reach the caller in finish() after a
+// successful wait.
+struct HostResults {
+    struct Item { void* dst; const void* src; size_t bytes; bool pinned; size_t off; };
+    std::vector<Item> items;
+    void add(void* dst, const void* src, size_t bytes) { items.push_back({dst, src, bytes, false, 0}); }
+    int queue(astcb200_ctx* ctx, cudaStream_t s);  // classifies, sizes the staging, queues the copies
+    void finish(astcb200_ctx* ctx) const;          // staged bytes to the caller (after the wait)
+};
 
 template <class T>
 int ensure_buf(astcb200_ctx* ctx, T*& p, size_t& cap, size_t need, const char* what) {

@@ -16,9 +16,9 @@
 // in shared memory and writes the row with one 256-byte bulk copy to global
 // memory (instead of 64 strided stores per thread); CTAs start the chunk
 // sequence at different chunks so that they do not all fetch the same weights
-// from L2 at once.  Every wait on an mbarrier is bounded; a CTA that gives up
-// sets *error_flag, waits (bounded) for its own copies and MMAs in flight,
-// frees its tensor memory and returns.
+// from L2 at once.  Every wait on an mbarrier is bounded (error_flag[1] polls, 0 = 2^24);
+// a CTA that gives up sets error_flag[0], waits (bounded by 2^24 polls) for its own copies
+// and MMAs in flight, frees its tensor memory and returns.
 //
 // k_select: one warp per block turns the logits into the proposal search's
 // inputs: a softmax over the partition classes, the best partitionings (in
@@ -64,8 +64,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; i++)
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase of parity `parity` to complete, at most `limit` polls.  Limits below
+// 2^16 (set by tests of the give-up path) poll with the non-blocking test_wait, so that a
+// wait for work still in flight gives up at once; larger ones use try_wait, which may
+// suspend the thread until the phase completes.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
+    if (limit < (1u << 16)) {
+        for (uint32_t i = 0; i < limit; i++)
+            if (mbar_test_wait(bar, parity)) return true;
+        return false;
+    }
+    for (uint32_t i = 0; i < limit; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -175,6 +195,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     // read different parts of the weights from L2 instead of all the same chunk
     const int j0 = blockIdx.x % nchunks;
     auto chunk_of = [&](int j) { const int c = j0 + j; return c < nchunks ? c : c - nchunks; };
+    const uint32_t wl = error_flag[1] ? (uint32_t)error_flag[1] : kWaitLimit;  // polls per wait
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols)
@@ -192,7 +213,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     const uint32_t tmem = *tmem_slot;
     const uint32_t tmem_row = tmem + ((uint32_t)((warp & 3) * 32) << 16);
 
-    // thread 0's bookkeeping of weight copies and MMA commits in flight
+    // thread 0's bookkeeping of weight copies and MMA commits in flight: a phase counts as
+    // done only once a wait saw it complete, so the drain after a give-up waits for the rest
     uint32_t w_issued[2] = {0, 0}, w_done[2] = {0, 0};
     uint32_t m_issued[3] = {0, 0, 0}, m_done[3] = {0, 0, 0};  // only the waits of all threads advance m_done
     bool ok = true, failed = false;  // failed: the same in every thread (set only at uniform exits)
@@ -228,8 +250,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     // ---- layer 1: X (128 x k0p) . W1^T -> tensor memory columns [0, 256)
     if (tid == 0) {
         tc_after();
-        if (!mbar_wait(&bw[0], (w_done[0]++) & 1)) *abort_flag = 1;
+        if (!mbar_wait(&bw[0], w_done[0] & 1, wl)) *abort_flag = 1;
         else {
+            w_done[0]++;
             for (int kk = 0; kk < S.k0p / 16; kk++)
                 mma_bf16(tmem, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128), smem_desc(w_base + kk * 2 * kLboW256, kLboW256, 128),
                          instr_desc(128, 256), kk > 0);
@@ -239,8 +262,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     }
     __syncthreads();
     if (*abort_flag) { failed = true; goto cleanup; }
-    ok = mbar_wait(&bm[0], m_done[0] & 1);
-    m_done[0]++;
+    ok = mbar_wait(&bm[0], m_done[0] & 1, wl);
+    if (ok) m_done[0]++;
     if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
     tc_after();
     if (tid == 0) { load_weights(sW, net.w2, 256u * 256u * 2, &bw[0]); w_issued[0]++; }
@@ -252,8 +275,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     // ---- layer 2: H1 (128 x 256) . W2^T -> columns [256, 512)
     if (tid == 0) {
         tc_after();
-        if (!mbar_wait(&bw[0], (w_done[0]++) & 1)) *abort_flag = 1;
+        if (!mbar_wait(&bw[0], w_done[0] & 1, wl)) *abort_flag = 1;
         else {
+            w_done[0]++;
             for (int kk = 0; kk < 16; kk++)
                 mma_bf16(tmem + 256, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
                          smem_desc(w_base + kk * 2 * kLboW256, kLboW256, 128), instr_desc(128, 256), kk > 0);
@@ -263,8 +287,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     }
     __syncthreads();
     if (*abort_flag) { failed = true; goto cleanup; }
-    ok = mbar_wait(&bm[0], m_done[0] & 1);
-    m_done[0]++;
+    ok = mbar_wait(&bm[0], m_done[0] & 1, wl);
+    if (ok) m_done[0]++;
     if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
     tc_after();
     if (tid == 0) {
@@ -286,7 +310,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
             tc_after();
             for (int jj = (j == 0 ? 0 : j + 1); jj <= j + 1 && jj < nchunks; jj++) {
                 const int bb = jj & 1;
-                if (!mbar_wait(&bw[bb], (w_done[bb]++) & 1)) { *abort_flag = 1; break; }
+                if (!mbar_wait(&bw[bb], w_done[bb] & 1, wl)) { *abort_flag = 1; break; }
+                w_done[bb]++;
                 for (int kk = 0; kk < 16; kk++)
                     mma_bf16(tmem + bb * kChunkN, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
                              smem_desc(w_base + bb * kW3Buf + kk * 2 * kLboW3, kLboW3, 128), instr_desc(128, kChunkN), kk > 0);
@@ -296,8 +321,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
         }
         __syncthreads();
         if (*abort_flag) { failed = true; goto cleanup; }
-        ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1);
-        m_done[1 + b]++;
+        ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1, wl);
+        if (ok) m_done[1 + b]++;
         if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
         tc_after();
         if (tid == 0 && j + 2 < nchunks) {
@@ -343,7 +368,7 @@ cleanup:
         // give up: record it, then let our own copies and MMAs drain (bounded) before the
         // shared and tensor memory are released
         if (tid == 0) {
-            atomicExch(error_flag, 1);
+            atomicExch(error_flag, 1);  // error_flag[0]
             for (int b = 0; b < 2; b++)
                 while (w_done[b] < w_issued[b]) { mbar_wait(&bw[b], w_done[b] & 1); w_done[b]++; }
             for (int b = 0; b < 3; b++)

@@ -42,15 +42,21 @@ int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const Fo
     return ensure_buf(ctx, sc.pbl, sc.cap_pbl, blocks * 4 * kMaxProposals * sizeof(uint32_t), "cudaMalloc work lists");
 }
 
-int begin_routes(astcb200_ctx* ctx, size_t chunks) {
+int ensure_error_flag(astcb200_ctx* ctx) {
+    if (ctx->d_mlp_error) return ASTCB200_OK;
+    size_t cap = 0;
+    int rc = ensure_buf(ctx, ctx->d_mlp_error, cap, 2 * sizeof(int), "cudaMalloc error flag");
+    if (rc) return rc;
+    CK(cudaMemset(ctx->d_mlp_error, 0, 2 * sizeof(int)), "cudaMemset");
+    return ASTCB200_OK;
+}
+
+int begin_routes(astcb200_ctx* ctx, size_t chunks, cudaStream_t s) {
     ctx->counts_used = 0;
     int rc = ensure_buf(ctx, ctx->d_counts, ctx->counts_cap, std::max<size_t>(chunks, 1) * mlp::kRouteCounters * sizeof(int), "cudaMalloc route counters");
     if (rc) return rc;
-    if (!ctx->d_mlp_error) {
-        size_t cap = 0;
-        if ((rc = ensure_buf(ctx, ctx->d_mlp_error, cap, sizeof(int), "cudaMalloc error flag"))) return rc;
-        CK(cudaMemset(ctx->d_mlp_error, 0, sizeof(int)), "cudaMemset");
-    }
+    if ((rc = ensure_error_flag(ctx))) return rc;
+    CK(cudaMemsetAsync(ctx->d_mlp_error, 0, sizeof(int), s), "reset error flag");  // this call's give-ups only
     return ASTCB200_OK;
 }
 
@@ -185,7 +191,7 @@ int astcb200_proposal_layout(uint8_t bx, uint8_t by, uint32_t* inputs, uint32_t*
 int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* w) {
     if (!ctx || !w || w->struct_size < sizeof(astcb200_proposal_net)) return ASTCB200_BAD_ARG;
     if (!w->w1 || !w->b1 || !w->w2 || !w->b2 || !w->w3 || !w->b3) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     const FootTables* ft = nullptr;
     int rc = get_tables(ctx, w->block_x, w->block_y, &ft);
     if (rc) return rc;
@@ -266,11 +272,22 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     return ASTCB200_OK;
 }
 
+int astcb200_set_inference_wait_limit(astcb200_ctx* ctx, uint32_t polls) {
+    if (!ctx || polls > 0x7FFFFFFFu) return ASTCB200_BAD_ARG;
+    ASTCB200_DEVICE_SCOPE(ctx);
+    int rc = ensure_error_flag(ctx);
+    if (rc) return rc;
+    const int v = (int)polls;
+    CK(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+    CK(cudaMemcpy(ctx->d_mlp_error + 1, &v, sizeof(int), cudaMemcpyHostToDevice), "set wait limit");
+    return ASTCB200_OK;
+}
+
 int astcb200_pruning_stats(astcb200_ctx* ctx, uint64_t* proposal_blocks, uint64_t* full_blocks) {
     if (!ctx || !proposal_blocks || !full_blocks) return ASTCB200_BAD_ARG;
     *proposal_blocks = *full_blocks = 0;
     if (!ctx->counts_used) return ASTCB200_OK;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     CK(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
     std::vector<int> c((size_t)mlp::kRouteCounters * ctx->counts_used);
     CK(cudaMemcpy(c.data(), ctx->d_counts, c.size() * sizeof(int), cudaMemcpyDeviceToHost), "read route counters");
@@ -293,13 +310,13 @@ int astcb200_proposal_logits(astcb200_ctx* ctx, const uint8_t* rgba8, float* log
     if (!nd) { ctx->err = "no network for this footprint"; return ASTCB200_BAD_ARG; }
     const size_t nout = nd->net.s.nout;
     if (len < (size_t)ctx->nblocks * nout) return ASTCB200_BAD_ARG;
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     const size_t in_bytes = (size_t)ctx->width * ctx->height * 4;
     int rc;
     if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
     const size_t chunk = std::min<size_t>(ctx->chunk, ctx->nblocks);
     if ((rc = ensure_buf(ctx, ctx->scratch.logits, ctx->scratch.cap_logits, chunk * nout * 4, "cudaMalloc logits"))) return rc;
-    if ((rc = begin_routes(ctx, 1))) return rc;
+    if ((rc = begin_routes(ctx, 1, ctx->stream))) return rc;
     CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
     KernelArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -330,7 +347,7 @@ int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t
     for (const NetDev* x : ctx->nets)
         if (x->bx == (int)ctx->bx && x->by == (int)ctx->by) nd = x;
     if (!nd) { ctx->err = "no network for this footprint"; return ASTCB200_BAD_ARG; }
-    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    ASTCB200_DEVICE_SCOPE(ctx);
     const size_t in_bytes = (size_t)ctx->width * ctx->height * 4;
     const size_t chunk = std::min<size_t>(ctx->chunk, ctx->nblocks);
     const size_t nchunks = (ctx->nblocks + chunk - 1) / chunk;
@@ -343,7 +360,7 @@ int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t
     if ((rc = ensure_buf(ctx, sc.masks, sc.cap_masks, chunk * 4 * kMaskWords * sizeof(uint64_t), "cudaMalloc block-mode masks"))) return rc;
     if ((rc = ensure_buf(ctx, sc.full_err, sc.cap_ferr, chunk * sizeof(float), "cudaMalloc full-search errors"))) return rc;
     if ((rc = ensure_buf(ctx, sc.pbl, sc.cap_pbl, chunk * 4 * kMaxProposals * sizeof(uint32_t), "cudaMalloc work lists"))) return rc;
-    if ((rc = begin_routes(ctx, nchunks))) return rc;
+    if ((rc = begin_routes(ctx, nchunks, ctx->stream))) return rc;
     CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
     KernelArgs a;
     std::memset(&a, 0, sizeof(a));

@@ -35,7 +35,14 @@ typedef struct astcb200_ctx astcb200_ctx;
 typedef struct astcb200_config {
     uint32_t struct_size;  /* sizeof(astcb200_config); 0 selects all defaults */
     uint32_t chunk_blocks; /* blocks searched per launch sequence; 0 = 65536 */
-    uint32_t timeout_ms;   /* bound on each host wait for the device; 0 = no bound */
+    uint32_t timeout_ms;   /* bound on each host wait for the device; 0 = no bound.  A call
+                              that returns ASTCB200_TIMEOUT leaves its work queued on the
+                              context's stream, where it completes and later calls queue
+                              behind it.  Its results never reach pageable host buffers (they
+                              go through the context's pinned staging); pinned host buffers
+                              passed to it, inputs and outputs, are still read or written by
+                              that work, so keep them valid until a later call on the context
+                              has returned or the context is destroyed. */
     uint32_t flags;        /* ASTCB200_FLAG_* */
 } astcb200_config;
 
@@ -77,6 +84,10 @@ int astcb200_destroy(astcb200_ctx* ctx);
 /* Replaces ASTCEncoder::secondaryInit(textureWidth, textureHeight, blockXDim, blockYDim)
  * (compression_pipeline.cpp:263-321): builds the footprint's tables on the device. */
 int astcb200_set_image(astcb200_ctx* ctx, uint32_t width, uint32_t height, uint8_t block_x, uint8_t block_y);
+/* Changes astcb200_config.timeout_ms for later calls (no reference counterpart: the
+ * reference's blocking map has no bound, webgpu_utils.h:79-87). */
+int astcb200_set_timeout(astcb200_ctx* ctx, uint32_t timeout_ms);
+
 /* ASTCEncoder::blocksX / blocksY (astc.h:736-737). */
 int astcb200_blocks(const astcb200_ctx* ctx, uint32_t* blocks_x, uint32_t* blocks_y);
 
@@ -208,6 +219,14 @@ typedef struct astcb200_pruning {
 } astcb200_pruning;
 /* Applies to later encodes of footprints that have a network (the others use the full search). */
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg);
+/* Polls of each mbarrier wait in the network's inference kernel before its CTA gives up
+ * (0 = the default, 2^24).  A CTA that gives up records it, waits for its own copies and
+ * tensor-core work in flight to land (bounded by 2^24 polls) and returns; the encode that
+ * launched it then reports ASTCB200_TIMEOUT from astcb200_pruning_stats,
+ * astcb200_proposal_logits or astcb200_proposal_selection.  Small values exercise that
+ * path in tests; limits below 65536 poll without suspending, so they give up as soon as a
+ * wait finds the work still in flight. */
+int astcb200_set_inference_wait_limit(astcb200_ctx* ctx, uint32_t polls);
 /* Blocks that took the proposal search and the full search in the last encode call. */
 int astcb200_pruning_stats(astcb200_ctx* ctx, uint64_t* proposal_blocks, uint64_t* full_blocks);
 /* Test hook: the network's logits (blocks x outputs, FP32) for the image set by
