@@ -111,7 +111,6 @@ def load_library():
         "astcb200_stage_times_detail": (I32, [P, P, P]),
         "astcb200_work_counters": (I32, [P, P]),
         "astcb200_encode_noalloc": (I32, [I32, P, U32, U32, ctypes.c_uint8, ctypes.c_uint8, P, P]),
-        "astcb200_fp32_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double)]),
         "astcb200_encode_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Stats)]),
         "astcb200_encode_batch_device": (I32, [P, ctypes.POINTER(Texture), U32, P]),
         "astcb200_autotune_batch": (I32, [P, ctypes.POINTER(Texture), U32, ctypes.POINTER(Tuning), ctypes.POINTER(Tuning),
@@ -418,13 +417,6 @@ def mip_dims(width, height):
         w, h = dims[-1]
         dims.append((max(1, w // 2), max(1, h // 2)))
     return dims
-
-
-def fp32_peak_tflops(device=0):
-    """FP32 FMA throughput of the device in TFLOP/s (dependent-FMA microbenchmark)."""
-    t = ctypes.c_double()
-    _check(load_library().astcb200_fp32_peak(device, ctypes.byref(t)))
-    return t.value
 
 
 def psnr(a, b):

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libastcb200.so")
 
-SOURCES = ["tables.cpp", "decoder.cpp", "kernels_search.cu", "kernels_refine.cu", "capi.cu", "peak_probe.cu", "noalloc.cu", "decoder_gpu.cu", "batch.cu", "mlp.cu", "mlp_train.cu", "pipeline.cu"]
+SOURCES = ["tables.cpp", "decoder.cpp", "kernels_search.cu", "kernels_refine.cu", "capi.cu", "noalloc.cu", "decoder_gpu.cu", "batch.cu", "mlp.cu", "mlp_train.cu", "pipeline.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-I", CSRC, "-I", os.path.join(REPO, "include")]

@@ -15,7 +15,7 @@ it alone).  The metric is Mtexel/s over both encodes.
               copies inside the timed region).
   roofline    the dominant kernel's modelled FP32 operations (flop_model.py)
               over its CUDA-event time, against this GPU's FP32 FMA peak
-              measured by astcb200_fp32_peak.
+              measured by the probe in bench_peak.cu.
   cpu_baseline the CPU oracle (a restatement of the reference's search) on a
               bounded sample of the same workload, all host threads, rank 0.
 
@@ -362,6 +362,28 @@ PRUNING = dict(max_partitionings=4, block_modes=16, refine_candidates=2, coverag
 CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
 
 
+def fp32_peak_tflops(device):
+    """FP32 FMA throughput of the device in TFLOP/s, from the dependent-FMA probe
+    bench_peak.cu (built into bench_peak.so by __graft_entry__.build())."""
+    path = os.path.join(REPO, "bench_peak.so")
+    if not os.path.exists(path):
+        build_bench_peak()
+    lib = ctypes.CDLL(path)
+    t = ctypes.c_double()
+    rc = lib.bench_fp32_peak(device, ctypes.byref(t))
+    if rc != 0:
+        raise RuntimeError("bench_fp32_peak failed (%d)" % rc)
+    return t.value
+
+
+def build_bench_peak():
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    out = os.path.join(REPO, "bench_peak.so")
+    subprocess.check_call([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-shared", "-Xcompiler", "-fPIC",
+                           os.path.join(REPO, "bench_peak.cu"), "-o", out + ".tmp"])
+    os.replace(out + ".tmp", out)
+
+
 def measured_peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     return json.load(open(path)) if os.path.exists(path) else {}
@@ -527,7 +549,7 @@ def main():
     dom_key = ["search", "front", "refine", None][dom]
     dom_ms = tot_ms[dom]
     achieved = flops[dom_key] / (dom_ms / 1000.0) / 1e12 if dom_key and dom_ms > 0 else 0.0
-    peak = ab.fp32_peak_tflops(local)
+    peak = fp32_peak_tflops(local)
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath) and dom_key in ("front", "refine") and stage_n[:, dom].sum():

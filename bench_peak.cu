@@ -1,9 +1,9 @@
-// FP32 throughput probe: each thread runs independent chains of dependent FMAs.
-// Used only to measure the roofline denominator for the FP32-bound search kernels
-// (the recorded peaks of this GPU give HBM and bf16 figures but no FP32 one).
+// FP32 throughput probe for bench.py (not part of the encoder library): each thread
+// runs independent chains of dependent FMAs.  It measures the roofline denominator of
+// the FP32-bound search kernels (the recorded peaks of this GPU give HBM and bf16
+// figures but no FP32 one).  Built into bench_peak.so by __graft_entry__.build():
+//   nvcc -gencode arch=compute_100a,code=sm_100a -O3 -shared -Xcompiler -fPIC bench_peak.cu -o bench_peak.so
 #include <cuda_runtime.h>
-
-#include "astcb200.h"
 
 namespace {
 
@@ -20,14 +20,15 @@ __global__ void k_fma_chain(float* out, int iters, float a, float b) {
 
 }  // namespace
 
-extern "C" int astcb200_fp32_peak(int device, double* tflops) {
-    if (!tflops) return ASTCB200_BAD_ARG;
-    if (cudaSetDevice(device) != cudaSuccess) return ASTCB200_CUDA_ERROR;
+// TFLOP/s of dependent-FMA chains on `device` (an FMA counts 2 ops); 0 on success.
+extern "C" int bench_fp32_peak(int device, double* tflops) {
+    if (!tflops) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 2;
     cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return ASTCB200_CUDA_ERROR;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 2;
     float* out = nullptr;
     const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 1 << 14;
-    if (cudaMalloc((void**)&out, blocks * sizeof(float)) != cudaSuccess) return ASTCB200_OOM;
+    if (cudaMalloc((void**)&out, blocks * sizeof(float)) != cudaSuccess) return 3;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     k_fma_chain<<<blocks, threads>>>(out, 256, 0.999999f, 1e-7f);  // warm-up
@@ -43,8 +44,8 @@ extern "C" int astcb200_fp32_peak(int device, double* tflops) {
     }
     const cudaError_t err = cudaGetLastError();
     cudaEventDestroy(e0); cudaEventDestroy(e1); cudaFree(out);
-    if (err != cudaSuccess) return ASTCB200_CUDA_ERROR;
+    if (err != cudaSuccess) return 2;
     const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
     *tflops = flops / (best * 1e-3) / 1e12;
-    return ASTCB200_OK;
+    return 0;
 }

@@ -103,15 +103,22 @@ int astcb200_encode(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blocks
 int astcb200_encode_device(astcb200_ctx* ctx, const uint8_t* d_rgba8, uint8_t* d_out_blocks, void* cuda_stream);
 
 /* Encode without allocating (no counterpart in the reference).  For callers that cannot
- * call cudaMalloc -- an engine whose allocator owns the device heap, code running during
- * another component's graph capture, a plug-in in a process with a fixed allocation
- * policy.  Inputs and outputs are the caller's device buffers (as for
- * astcb200_encode_device); every intermediate lives in a 48 MiB file-scope device array
- * that each GPU loading this library holds until exit.  At most 2048 blocks per call
- * (ASTCB200_TOO_LARGE beyond).  All calls share that array: calls overlapping on the GPU
- * race and must be serialised by the caller.  The first call on a device resolves the
- * array's address (cudaGetSymbolAddress) and should come before any stream capture.
- * Work is queued on cuda_stream (NULL = the legacy default stream); no wait. */
+ * call cudaMalloc -- an engine whose allocator owns the whole device heap, a plug-in in a
+ * process with a fixed allocation policy.  Inputs and outputs are the caller's device
+ * buffers (as for astcb200_encode_device); every intermediate, and the search tables of
+ * each footprint used so far, live in one 52 MiB file-scope device array.  The CUDA
+ * runtime commits that array on a device when the first call there resolves its address
+ * (cudaGetSymbolAddress), and the device holds it until the process exits: make the
+ * first call at start-up, before the caller's allocator reserves the heap
+ * (ASTCB200_OOM if no room is left then).  The first call of each footprint on a device
+ * also uploads that footprint's tables into the array (a synchronous copy) and sets the
+ * kernels' shared-memory limits; make these first calls before any stream capture.
+ * Later calls only queue kernels.  At most 2048 blocks per call (ASTCB200_TOO_LARGE
+ * beyond).  All calls share the array and it keeps the last call's contents: calls that
+ * overlap on the GPU race and must be serialised by the caller.  Always the exhaustive
+ * search with the reference's semantics: no proposal network, no pruning.  Work is
+ * queued on cuda_stream (NULL = the legacy default stream); no wait.  The caller's
+ * current device is left as it was. */
 int astcb200_encode_noalloc(int device_ordinal, const uint8_t* d_rgba8, uint32_t width, uint32_t height,
                             uint8_t block_x, uint8_t block_y, uint8_t* d_out_blocks, void* cuda_stream);
 
@@ -322,10 +329,6 @@ int astcb200_stage_times_detail(astcb200_ctx* ctx, float* ms9, int32_t* stage9);
  * partition count; [4] decimation modes and [5] block modes it evaluated; [6..9]
  * candidates refined by partition count; [10..12] partition searches for P = 2, 3, 4. */
 int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16);
-
-/* Measures the device's FP32 throughput with a dependent-FMA-chain kernel (diagnostic
- * used by bench.py for the roofline denominator): TFLOP/s counting an FMA as 2 flops. */
-int astcb200_fp32_peak(int device_ordinal, double* tflops);
 
 const char* astcb200_status_string(int status);
 const char* astcb200_last_error(const astcb200_ctx* ctx);

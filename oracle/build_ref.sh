@@ -5,9 +5,13 @@
 # The reference's GPU path (WebGPU/Dawn) is not built; only these four sources:
 #   code/metadata_structures.cpp  code/partition_tables.cpp
 #   code/physical_compression.cpp code/astc_store.cpp
-# Usage: oracle/build_ref.sh [reference_root]   (default: /root/reference)
+# Usage: oracle/build_ref.sh <reference_root>   (the checkout holding code/ and shaders/)
 set -euo pipefail
-REF="${1:-/root/reference}"
+if [ $# -lt 1 ]; then
+  echo "usage: $0 <reference_root>" >&2
+  exit 2
+fi
+REF="$1"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/code" ]; then

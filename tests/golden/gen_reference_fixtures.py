@@ -1,9 +1,9 @@
 """Generates the golden fixtures under tests/golden/ from the reference.
 
-Run in a checkout that has the reference at /root/reference (or pass its path)
-and after `oracle/build_ref.sh` has built oracle/_ref/libastcref.so:
+Run after `oracle/build_ref.sh <reference_root>` has built oracle/_ref/libastcref.so,
+giving the same reference checkout (the directory holding code/ and shaders/):
 
-    python tests/golden/gen_reference_fixtures.py [/path/to/reference]
+    python tests/golden/gen_reference_fixtures.py <reference_root>
 
 Outputs (committed; the tests never read the reference itself):
   reference_tables.npz
@@ -88,7 +88,9 @@ def transfer_scramble(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_reference_fixtures.py <reference_root>")
+    ref = sys.argv[1]
     sh = os.path.join(ref, "shaders")
     code = os.path.join(ref, "code")
     lib = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libastcref.so"))

@@ -1,11 +1,11 @@
 """The allocation-free entry point (astcb200_encode_noalloc).
 
 Some callers cannot allocate device memory: an engine whose own allocator owns the
-whole device heap, code running while another component captures a CUDA graph, a
-plug-in inside a process with a fixed allocation policy.  For them the library keeps
-a fixed 48 MiB scratch array in device memory and encodes at most 2048 blocks per
-call into buffers the caller already owns.  This file is collected last so that a
-run stopping at the first failure has run every other test first.
+whole device heap, a plug-in inside a process with a fixed allocation policy.  For
+them the library keeps a fixed 52 MiB array in device memory (intermediates and the
+tables of the footprints used) and encodes at most 2048 blocks per call into buffers
+the caller already owns.  This file is collected last so that a run stopping at the
+first failure has run every other test first.
 """
 import numpy as np
 import pytest
@@ -43,3 +43,36 @@ def test_noalloc_rejects_oversized_request():
     with pytest.raises(ab.ASTCError) as e:
         ab.encode_noalloc(0, d.data_ptr(), 1024, 1024, 4, 4, d.data_ptr())
     assert e.value.status == ab.TOO_LARGE
+
+
+def test_noalloc_allocates_nothing_after_set_up():
+    """Once a device and its footprints are set up, calls with other images of those
+    footprints leave the device's free memory unchanged, and still match the regular
+    entry point."""
+    import torch
+    cases = [(160, 96, 4, 4, 31), (90, 66, 6, 6, 32), (150, 100, 4, 4, 33), (84, 72, 6, 6, 34)]
+    enc = ab.ASTCEncoder(device=0)
+    stream = torch.cuda.current_stream().cuda_stream
+    ins, outs, expected = [], [], []
+    for w, h, bx, by, seed in cases:
+        img = synth.make_texture(w, h, seed)
+        enc.secondaryInit(w, h, bx, by)
+        d_in = torch.from_numpy(img.reshape(-1)).cuda()
+        ref = torch.zeros(enc.numBlocks * 16, dtype=torch.uint8, device="cuda")
+        enc.encode_device(d_in.data_ptr(), ref.data_ptr(), stream)
+        ins.append(d_in)
+        outs.append(torch.full((enc.numBlocks * 16,), 0xAA, dtype=torch.uint8, device="cuda"))
+        expected.append(ref)
+    torch.cuda.synchronize()
+    expected = [e.cpu().numpy() for e in expected]
+    for (w, h, bx, by, _), d_in, out in zip(cases[:2], ins[:2], outs[:2]):  # set-up: device, 4x4, 6x6
+        ab.encode_noalloc(0, d_in.data_ptr(), w, h, bx, by, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for (w, h, bx, by, _), d_in, out in zip(cases[2:], ins[2:], outs[2:]):
+        ab.encode_noalloc(0, d_in.data_ptr(), w, h, bx, by, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    for out, exp in zip(outs, expected):
+        assert np.array_equal(out.cpu().numpy(), exp)
+    enc.close()
