@@ -1,13 +1,21 @@
-"""The GPU decoder (astcb200_decode_device / astcb200_decode_error_device) against the host
-decoder: the same texels for encoder output at every footprint, for void-extent blocks and
-for arbitrary bytes (reserved modes and HDR blocks decode to the error colour), and the
-same squared-error sums as a host computation."""
+"""The GPU decoder (astcb200_decode_device / astcb200_decode_error_device): against an
+independent reconstruction of every block the GPU encoder emits from its symbolic result
+(oracle/astc_decode_oracle.py, written from the ASTC specification), at every footprint,
+in both search semantics and for the proposal search; against the host decoder for
+void-extent blocks and arbitrary bytes (reserved modes and HDR blocks decode to the error
+colour); and the same squared-error sums as a host computation."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
 import _libs
 import astc_implementation_b200 as ab
-from astc_implementation_b200 import synth
+from astc_implementation_b200 import proposal, synth
+
+sys.path.insert(0, os.path.join(_libs.REPO, "oracle"))
+import astc_decode_oracle as ado  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -53,6 +61,38 @@ def test_decoder_matches_host_on_encoded_blocks(bx, by):
     sse = gpu_sse(bx, by, w, h, blocks, img)
     assert np.array_equal(sse, host_sse(host, img))
     assert abs(ab.psnr_from_sse(sse, w, h) - ab.psnr(host, img)) < 1e-9
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+@pytest.mark.parametrize("bx,by", FOOTPRINTS)
+def test_decoder_matches_symbolic_reconstruction_of_gpu_encodes(bx, by, fixed):
+    """GPU encode -> GPU decode equals the texels the specification gives for the encoder's
+    own symbolic blocks (endpoints, weights, partitioning), for every block."""
+    w, h = 6 * bx + 5, 4 * by + 3
+    img = synth.make_texture(w, h, 700 + bx * 16 + by)
+    enc = ab.ASTCEncoder(device=0, fixed=fixed)
+    enc.secondaryInit(w, h, bx, by)
+    sym = enc.encode_symbolic(img)
+    blocks = enc.encode(img)
+    enc.close()
+    ref = ado.image_from_symbolic(sym, bx, by, w, h, ado.PartitionTables(_libs.oracle(), bx, by))
+    assert np.array_equal(gpu_decode(bx, by, w, h, blocks), ref)
+
+
+@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
+def test_decoder_matches_symbolic_reconstruction_of_proposal_search(bx, by):
+    w, h = 40 * bx + 1, 30 * by + 2
+    img = synth.make_texture(w, h, 800 + bx)
+    enc = ab.ASTCEncoder(device=0)
+    enc.set_proposal_net(proposal.load_weights(bx, by))
+    enc.set_pruning(True)
+    enc.secondaryInit(w, h, bx, by)
+    sym = enc.encode_symbolic(img)
+    blocks = enc.encode(img)
+    assert enc.pruning_stats()[0] > 0
+    enc.close()
+    ref = ado.image_from_symbolic(sym, bx, by, w, h, ado.PartitionTables(_libs.oracle(), bx, by))
+    assert np.array_equal(gpu_decode(bx, by, w, h, blocks), ref)
 
 
 @pytest.mark.parametrize("bx,by", [(4, 4), (6, 6), (8, 5), (12, 12)])
