@@ -22,6 +22,11 @@ it alone).  The metric is Mtexel/s over both encodes.
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                 [--size S] [--footprints 4x4,6x6]      smaller cases (profiling)
                 [--workload batch]                      64 mixed textures, batched vs per-texture
+                [--workload combined --count 256 --max-side 4096 --steps 1]   learned proposal + batches
+                                                        of textures with mip chains
+                [--workload topk]                       4096x4096, max_partitionings 4 / 8 / 16
+                [--workload settings --settings JSON]   proposal-search settings sweep
+                [--semantics ref|fixed]                 the reference's semantics or its bugs repaired
 """
 import argparse
 import ctypes
@@ -81,8 +86,9 @@ def oracle_lib():
     return ctypes.CDLL(path)
 
 
-def cpu_sample_rate(img, sample_side, reps=1):
-    """Oracle Mtexel/s on the top-left sample_side^2 crop at both footprints, all threads."""
+def cpu_sample_rate(img, sample_side, reps=1, blocks=None):
+    """Oracle Mtexel/s on the top-left sample_side^2 crop at both footprints, all threads.
+    blocks (a dict), when given, receives each footprint's encoded blocks."""
     lib = oracle_lib()
     crop = np.ascontiguousarray(img[:sample_side, :sample_side])
     texels, secs = 0, 0.0
@@ -96,7 +102,30 @@ def cpu_sample_rate(img, sample_side, reps=1):
             secs += time.perf_counter() - t0
             assert rc == 0
             texels += sample_side * sample_side
+            if blocks is not None:
+                blocks[(bx, by)] = out
     return texels / secs / 1e6, secs
+
+
+def parity_vs_cpu(crop, cpu_blocks, device):
+    """The GPU full search (the reference's semantics) on the CPU baseline's crop: fraction of
+    blocks bit-identical to the CPU oracle's and the decoded PSNR delta, per footprint."""
+    import astc_implementation_b200 as ab
+    side_h, side_w = crop.shape[:2]
+    enc = ab.ASTCEncoder(device=device)
+    out = {"sample": "%dx%d crop of the seed-1 texture" % (side_w, side_h), "bit_identical_fraction": {},
+           "psnr_delta_db": {}, "psnr_cpu_db": {}}
+    for (bx, by), ref in cpu_blocks.items():
+        enc.secondaryInit(side_w, side_h, bx, by)
+        got = enc.encode(crop)
+        key = "%dx%d" % (bx, by)
+        out["bit_identical_fraction"][key] = float(np.mean(np.all(got.reshape(-1, 16) == ref.reshape(-1, 16), axis=1)))
+        p_gpu = ab.psnr(ab.decode(bx, by, side_w, side_h, got), crop)
+        p_cpu = ab.psnr(ab.decode(bx, by, side_w, side_h, ref), crop)
+        out["psnr_delta_db"][key] = round(float(p_gpu - p_cpu), 4)
+        out["psnr_cpu_db"][key] = round(float(p_cpu), 3)
+    enc.close()
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -357,6 +386,92 @@ def run_combined(args):
     return 0
 
 
+# ---------------------------------------------------------------- settings / top-K sweeps
+def run_settings(args):
+    """Speed and quality of proposal-search settings against the full search in both semantics,
+    on held-out textures (never used for training), one JSON line per footprint and method.
+    --workload topk: 4096x4096 textures (seeds 7, 8) at max_partitionings 4, 8 and 16, the
+    other settings at their defaults (the learned-proposal configuration's top-K sweep);
+    --workload settings: --settings' keyword sets (unspecified fields take the defaults)."""
+    import torch
+    import astc_implementation_b200 as ab
+    from astc_implementation_b200 import proposal, synth
+
+    rank, world, local = rank_info()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    topk = args.workload == "topk"
+    side = 4096 if (topk and args.size == 2048) else args.size
+    seeds = [int(v) for v in (args.seeds or ("7,8" if topk else "7,8,9,10")).split(",")]
+    settings = [{"max_partitionings": k} for k in (4, 8, 16)] if topk else json.loads(args.settings)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sse = torch.zeros(4, dtype=torch.int64, device="cuda")
+    for bx, by in FOOTPRINTS:
+        imgs = [synth.make_texture(side, side, s) for s in seeds]
+        d_in = [torch.from_numpy(im.reshape(-1)).cuda() for im in imgs]
+        nblk = ((side + bx - 1) // bx) * ((side + by - 1) // by)
+        out = torch.empty(nblk * 16, dtype=torch.uint8, device="cuda")
+
+        def timed(enc):
+            enc.encode_device(d_in[0].data_ptr(), out.data_ptr(), stream.cuda_stream)  # warm-up
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for d in d_in:
+                enc.encode_device(d.data_ptr(), out.data_ptr(), stream.cuda_stream)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            return t0.elapsed_time(t1) / len(d_in)
+
+        def quality(enc, routes=None):
+            q = []
+            for d in d_in:
+                enc.encode_device(d.data_ptr(), out.data_ptr(), stream.cuda_stream)
+                ab.decode_error_device(bx, by, side, side, out.data_ptr(), d.data_ptr(), sse.data_ptr(), stream.cuda_stream)
+                q.append(ab.psnr_from_sse(sse.cpu().numpy().astype(np.uint64), side, side))
+                if routes is not None:
+                    r = enc.pruning_stats()
+                    routes[0] += r[0]
+                    routes[1] += r[1]
+            return np.array(q)
+
+        base = {"workload": "%s: %dx%d held-out synthetic textures (seeds %s) at %dx%d"
+                            % (args.workload, side, side, ",".join(map(str, seeds)), bx, by)}
+        full = {}
+        for key, fx in (("ref", False), ("fixed", True)):
+            e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, fixed=fx)
+            e.secondaryInit(side, side, bx, by)
+            full[key] = (timed(e), quality(e))
+            e.close()
+            print(json.dumps(dict(base, method="full search", semantics=key, ms_per_texture=round(full[key][0], 3),
+                                  mtexel_s=round(side * side / full[key][0] / 1e3, 3),
+                                  psnr_db=[round(float(v), 3) for v in full[key][1]])), flush=True)
+        enc = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, fixed=args.semantics == "fixed")
+        enc.secondaryInit(side, side, bx, by)
+        enc.set_proposal_net(proposal.load_weights(bx, by))
+        for st in settings:
+            kw = dict(PRUNING)
+            kw.update(st)
+            enc.set_pruning(True, **kw)
+            ms = timed(enc)
+            routes = [0, 0]
+            q = quality(enc, routes)
+            line = dict(base, method="learned proposal search", semantics=args.semantics, settings=kw,
+                        ms_per_texture=round(ms, 3), mtexel_s=round(side * side / ms / 1e3, 3),
+                        psnr_db=[round(float(v), 3) for v in q],
+                        fallback_rate=round(routes[1] / max(1, routes[0] + routes[1]), 5),
+                        routes={"proposal_blocks": routes[0], "full_search_blocks": routes[1]})
+            for key in ("ref", "fixed"):
+                d = q - full[key][1]
+                line["vs_full_" + key] = {"speedup": round(full[key][0] / ms, 3), "mean_delta_db": round(float(d.mean()), 3),
+                                          "min_delta_db": round(float(d.min()), 3)}
+            print(json.dumps(line), flush=True)
+        enc.close()
+    return 0
+
+
 # ---------------------------------------------------------------- B200 arm
 PRUNING = dict(max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98, threshold=0.5, reroute_error=8.0)
 CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
@@ -400,7 +515,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="texture side (default: the 2048x2048 workload)")
     ap.add_argument("--footprints", default="4x4,6x6")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "combined"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "combined", "settings", "topk"])
     ap.add_argument("--count", type=int, default=32, help="combined workload: textures (256 in the full configuration)")
     ap.add_argument("--min-side", type=int, default=256)
     ap.add_argument("--max-side", type=int, default=1024, help="combined workload: 4096 in the full configuration")
@@ -408,6 +523,10 @@ def main():
                     help="timed method: the learned proposal search (headline) or the full search alone")
     ap.add_argument("--skip-full", action="store_true",
                     help="do not run the full search for comparison (profiling the timed method alone)")
+    ap.add_argument("--semantics", default="ref", choices=["ref", "fixed"],
+                    help="semantics of the timed method: the reference's (bit-exact) or with its shader bugs repaired")
+    ap.add_argument("--settings", default="[{}]", help="settings workload: JSON list of set_pruning keyword sets")
+    ap.add_argument("--seeds", default=None, help="settings workload: generator seeds (default 7,8,9,10, held out)")
     args = ap.parse_args()
     SIZE = args.size
     FOOTPRINTS = [tuple(int(v) for v in f.split("x")) for f in args.footprints.split(",")]
@@ -417,6 +536,8 @@ def main():
         return run_batch(args)
     if args.workload == "combined":
         return run_combined(args)
+    if args.workload in ("settings", "topk"):
+        return run_settings(args)
 
     import torch
     import astc_implementation_b200 as ab
@@ -437,24 +558,28 @@ def main():
     torch.cuda.set_stream(stream)
     d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
     use_prop = args.method == "proposal"
-    encs, outs = [], []
-    for bx, by in FOOTPRINTS:
-        e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, stage_timing=True)
-        e.init()
-        e.secondaryInit(SIZE, SIZE, bx, by)
-        if use_prop:
-            e.set_proposal_net(proposal.load_weights(bx, by))
-        encs.append(e)
-        outs.append(torch.empty(e.numBlocks * 16, dtype=torch.uint8, device="cuda"))
+    fixed = args.semantics == "fixed"
+
+    def make_encs(fixed_sem, with_net):
+        es = []
+        for bx, by in FOOTPRINTS:
+            e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, stage_timing=True, fixed=fixed_sem)
+            e.init()
+            e.secondaryInit(SIZE, SIZE, bx, by)
+            if with_net:
+                e.set_proposal_net(proposal.load_weights(bx, by))
+                e.set_pruning(True, **PRUNING)
+            es.append(e)
+        return es
+
+    encs = make_encs(fixed, use_prop)  # the timed method
+    # the full search in both semantics on the same images: the proposal search's reference points
+    full_sets = {} if (args.skip_full or not use_prop) else {"ref": make_encs(False, False), "fixed": make_encs(True, False)}
+    outs = [torch.empty(blocks_of(bx, by) * 16, dtype=torch.uint8, device="cuda") for bx, by in FOOTPRINTS]
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     names = ["k_partition_search / k_mlp_logits + k_select", "k_front", "k_refine", "k_select_pack"]
 
-    def set_method(prop):
-        for e in encs:
-            if use_prop:
-                e.set_pruning(prop, **PRUNING)
-
-    def run(steps, warmup, record):
+    def run(es, steps, warmup, record):
         """Mean ms per step over `steps` timed steps (max over ranks), per-stage ms and
         launches, and the work counters, summed over the timed steps."""
         stage_ms = np.zeros((len(FOOTPRINTS), 4))
@@ -463,7 +588,7 @@ def main():
 
         def step(i, rec):
             flush.fill_(i & 0xFF)
-            for k, e in enumerate(encs):
+            for k, e in enumerate(es):
                 e.encode_device(d_imgs[i % 4].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
                 if rec:
                     ms, n = e.stage_times()
@@ -487,34 +612,34 @@ def main():
 
     sse = torch.zeros(4, dtype=torch.int64, device="cuda")
 
-    def psnrs():  # encoded, decoded and compared on the GPU (astcb200_decode_error_device)
+    def psnrs(es):  # encoded, decoded and compared on the GPU (astcb200_decode_error_device)
         out = []
         for k, (bx, by) in enumerate(FOOTPRINTS):
             for i in range(len(imgs)):
-                encs[k].encode_device(d_imgs[i].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
+                es[k].encode_device(d_imgs[i].data_ptr(), outs[k].data_ptr(), stream.cuda_stream)
                 ab.decode_error_device(bx, by, SIZE, SIZE, outs[k].data_ptr(), d_imgs[i].data_ptr(), sse.data_ptr(),
                                        stream.cuda_stream)
                 out.append(ab.psnr_from_sse(sse.cpu().numpy().astype(np.uint64), SIZE, SIZE))
         return out
 
-    # the full search on the same images: its speed and quality are the reference point
-    full_rate, full_ms, full_psnr = None, None, None
-    if not args.skip_full:
-        set_method(False)
-        full_ms, _, _, _ = run(max(1, min(args.steps, 3)), 1, True)
-        full_rate, full_ms = job_rate(texels_per_step() * max(1, min(args.steps, 3)), full_ms, dist, "cuda")
-        full_psnr = psnrs() if use_prop else None
+    nfull = max(1, min(args.steps, 3))
+    full = {}
+    for key, es in full_sets.items():
+        fms, _, _, _ = run(es, nfull, 1, False)
+        frate, fms = job_rate(texels_per_step() * nfull, fms, dist, "cuda")
+        full[key] = {"value": frate, "ms": fms / nfull, "psnr": psnrs(es)}
+        for e in es:
+            e.close()
 
     # the timed method
-    set_method(True)
     clocks = ClockSampler(local)
-    ms, stage_ms, stage_n, work = run(args.steps, args.warmup, True)
+    ms, stage_ms, stage_n, work = run(encs, args.steps, args.warmup, True)
     clk = clocks.stop()
     value, ms = job_rate(texels_per_step() * args.steps, ms, dist, "cuda")
     if dist:
         dist.barrier()
     launches = int(stage_n.sum())
-    prop_psnr = psnrs() if use_prop and full_psnr else None
+    prop_psnr = psnrs(encs) if use_prop and full else None
     routes = [e.pruning_stats() for e in encs] if use_prop else None
 
     # e2e through the public host API, same method: inputs from and outputs to pinned host memory
@@ -570,16 +695,19 @@ def main():
                 units = work[:, 0:4].sum() / 13.0 if dom_key == "front" else work[:, 6:10].sum() / 104.0
                 traffic = round(per_block * units / stage_n[:, dom].sum())
     peaks = measured_peaks()
-    cpu = None
+    cpu, parity = None, None
     if not args.no_cpu_baseline:
-        rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample)
+        cpu_blocks = {}
+        rate, secs = cpu_sample_rate(imgs[0], args.cpu_sample, blocks=cpu_blocks)
         cpu = {"value": round(rate, 4), "unit": "Mtexel/s", "cores": os.cpu_count(), "kind": "port",
                "sample": "%dx%d crop of the seed-1 texture at %s, full search (%.1f s wall time on %d threads)"
                          % (args.cpu_sample, args.cpu_sample, " and ".join("%dx%d" % f for f in FOOTPRINTS), secs,
                             os.cpu_count())}
+        parity = parity_vs_cpu(np.ascontiguousarray(imgs[0][:args.cpu_sample, :args.cpu_sample]), cpu_blocks, local)
     fp_names = " and ".join("%dx%d" % f for f in FOOTPRINTS)
     method = ("learned proposal search (%s), full search for low-confidence and poorly encoded blocks"
               % ", ".join("%s=%s" % kv for kv in PRUNING.items())) if use_prop else "full search"
+    method += "; %s semantics" % ("FIXED (the reference's shader bugs repaired)" if fixed else "the reference's (REF)")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mtexel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -589,9 +717,12 @@ def main():
                    "method": method, "image": [SIZE, SIZE], "footprints": ["%dx%d" % f for f in FOOTPRINTS],
                    "chunk_blocks": CHUNK, "l2": "512 MiB memset before every step, inside the timed region",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "full_search": {"value": round(full_rate, 3), "unit": "Mtexel/s",
-                        "ms_per_step": round(full_ms / max(1, min(args.steps, 3)), 3)} if full_rate else None,
-        "speedup_vs_full_search": round(value / full_rate, 3) if full_rate else None,
+        "full_search": {"value": round(full["ref"]["value"], 3), "unit": "Mtexel/s", "semantics": "ref",
+                        "ms_per_step": round(full["ref"]["ms"], 3)} if "ref" in full else None,
+        "speedup_vs_full_search": round(value / full["ref"]["value"], 3) if "ref" in full else None,
+        "full_search_fixed": {"value": round(full["fixed"]["value"], 3), "unit": "Mtexel/s", "semantics": "fixed",
+                              "ms_per_step": round(full["fixed"]["ms"], 3)} if "fixed" in full else None,
+        "speedup_vs_fixed_full_search": round(value / full["fixed"]["value"], 3) if "fixed" in full else None,
         "stage_ms_per_step": {names[i]: round(float(tot_ms[i] / args.steps), 3) for i in range(4)},
         "roofline": {"kernel": names[dom], "bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2),
                      "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak else None, "traffic": traffic,
@@ -603,11 +734,18 @@ def main():
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if parity:
+        line["parity_vs_cpu_oracle"] = parity
     if use_prop and prop_psnr:
-        d = [p - f for p, f in zip(prop_psnr, full_psnr)]
-        line["psnr"] = {"mean_delta_db": round(float(np.mean(d)), 3), "min_delta_db": round(float(np.min(d)), 3),
-                        "full_search_db": [round(v, 3) for v in full_psnr], "proposal_db": [round(v, 3) for v in prop_psnr],
-                        "order": ["%dx%d seed %d" % (fp[0], fp[1], s) for fp in FOOTPRINTS for s in seeds]}
+        order = ["%dx%d seed %d" % (fp[0], fp[1], s) for fp in FOOTPRINTS for s in seeds]
+        for key, name in (("ref", "psnr"), ("fixed", "psnr_vs_fixed")):
+            if key not in full:
+                continue
+            d = [p - f for p, f in zip(prop_psnr, full[key]["psnr"])]
+            line[name] = {"mean_delta_db": round(float(np.mean(d)), 3), "min_delta_db": round(float(np.min(d)), 3),
+                          "full_search_db": [round(v, 3) for v in full[key]["psnr"]],
+                          "proposal_db": [round(v, 3) for v in prop_psnr], "order": order,
+                          "full_search_semantics": key}
     if use_prop:
         line["routes"] = {"%dx%d" % fp: {"proposal_blocks": int(r[0]), "full_search_blocks": int(r[1])}
                           for fp, r in zip(FOOTPRINTS, routes)}
