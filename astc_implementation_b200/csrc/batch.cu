@@ -278,14 +278,15 @@ int astcb200_encode_batch(astcb200_ctx* ctx, const astcb200_texture* textures, u
         io += align256(ib); oo += align256(ob);
         in_bytes += ib; out_bytes += ob;
     }
+    HostResults res;
+    for (uint32_t i = 0; i < n; i++) res.add(textures[i].out_blocks, dev[i].out_blocks, dev[i].out_len);
+    if ((rc = res.reserve(ctx))) return rc;
     Plan p;
     if ((rc = make_plan(ctx, dev.data(), n, true, p))) return rc;
     CK(cudaEventRecord(ctx->ev0, ctx->stream), "event");
     uint32_t launches = 0;
     if ((rc = launch_plan(ctx, p, ctx->stream, default_tuning(ctx, p), !(ctx->cfg.flags & ASTCB200_FLAG_NO_GRAPH), &launches))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
-    HostResults res;
-    for (uint32_t i = 0; i < n; i++) res.add(textures[i].out_blocks, dev[i].out_blocks, dev[i].out_len);
     if ((rc = res.queue(ctx, ctx->stream))) return rc;
     if ((rc = wait_stream(ctx, ctx->stream))) return rc;
     res.finish(ctx);

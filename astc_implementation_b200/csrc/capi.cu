@@ -41,7 +41,7 @@ int wait_stream(astcb200_ctx* ctx, cudaStream_t s) {
     }
 }
 
-int HostResults::queue(astcb200_ctx* ctx, cudaStream_t s) {
+int HostResults::reserve(astcb200_ctx* ctx) {
     size_t need = 0;
     for (Item& it : items) {
         cudaPointerAttributes at{};
@@ -58,6 +58,10 @@ int HostResults::queue(astcb200_ctx* ctx, cudaStream_t s) {
         CK(cudaHostAlloc((void**)&ctx->h_stage, need, cudaHostAllocDefault), "cudaHostAlloc staging");
         ctx->stage_cap = need;
     }
+    return ASTCB200_OK;
+}
+
+int HostResults::queue(astcb200_ctx* ctx, cudaStream_t s) {
     for (const Item& it : items)
         CK(cudaMemcpyAsync(it.pinned ? it.dst : (void*)(ctx->h_stage + it.off), it.src, it.bytes, cudaMemcpyDeviceToHost, s),
            "D2H results");
@@ -248,14 +252,15 @@ static int encode_host(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t* out_blo
     if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
     if ((rc = ensure_buf(ctx, ctx->d_out, ctx->out_cap, out_bytes, "cudaMalloc output"))) return rc;
     if (symbolic && (rc = ensure_buf(ctx, ctx->d_sym, ctx->sym_cap, (size_t)ctx->nblocks * 108 * 4, "cudaMalloc symbolic"))) return rc;
+    HostResults res;
+    if (out_blocks) res.add(out_blocks, ctx->d_out, out_bytes);
+    if (symbolic) res.add(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4);
+    if ((rc = res.reserve(ctx))) return rc;
     CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
     CK(cudaEventRecord(ctx->ev0, ctx->stream), "event");
     uint32_t launches = 0;
     if ((rc = run_search(ctx, ctx->d_img, ctx->d_out, symbolic ? ctx->d_sym : nullptr, ctx->stream, &launches))) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->stream), "event");
-    HostResults res;
-    if (out_blocks) res.add(out_blocks, ctx->d_out, out_bytes);
-    if (symbolic) res.add(symbolic, ctx->d_sym, (size_t)ctx->nblocks * 108 * 4);
     if ((rc = res.queue(ctx, ctx->stream))) return rc;
     if ((rc = wait_stream(ctx, ctx->stream))) return rc;
     res.finish(ctx);

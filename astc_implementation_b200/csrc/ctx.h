@@ -158,7 +158,10 @@ struct HostResults {
     struct Item { void* dst; const void* src; size_t bytes; bool pinned; size_t off; };
     std::vector<Item> items;
     void add(void* dst, const void* src, size_t bytes) { items.push_back({dst, src, bytes, false, 0}); }
-    int queue(astcb200_ctx* ctx, cudaStream_t s);  // classifies, sizes the staging, queues the copies
+    // Classifies the destinations and grows the staging; call it before queuing the call's
+    // work (growing waits for earlier calls' work on the context's stream, never for this one's).
+    int reserve(astcb200_ctx* ctx);
+    int queue(astcb200_ctx* ctx, cudaStream_t s);  // queues the copies
     void finish(astcb200_ctx* ctx) const;          // staged bytes to the caller (after the wait)
 };
 
