@@ -11,7 +11,8 @@ Training (needs a GPU):
     python -m astc_implementation_b200.proposal --footprint 4x4 --out weights/proposal_4x4.npz
 
 labels 2M blocks of synthetic textures (generator seeds 100-199) with the full search
-and trains the network on them (inputs: texels / 255 in bf16; classes: the winning
+(FIXED semantics by default: the reference's search with its shader bugs repaired) and trains
+the network on them (inputs: texels / 255 in bf16; classes: the winning
 partitioning or the single-partition class, and the winning block mode of that
 partition count).  PyTorch only holds the device memory and the stream.
 """
@@ -133,13 +134,13 @@ def mip_down(img):
     return (s >> 2).astype(np.uint8)
 
 
-def make_dataset(bx, by, seeds, side, device=0, log=print, mips=0):
+def make_dataset(bx, by, seeds, side, device=0, log=print, mips=0, fixed=False):
     """Inputs (n, k0p) float32 and labels of every block of side x side textures of the
     given generator seeds and of their first `mips` mip levels, labelled by the full search
-    on the GPU."""
+    on the GPU (with the reference's semantics, or FIXED ones: fixed=True)."""
     from . import synth
     lay = Layout(bx, by)
-    enc = ASTCEncoder(device=device)
+    enc = ASTCEncoder(device=device, fixed=fixed)
     enc.init()
     xs, ps, bs = [], [], []
     t0 = time.time()
@@ -324,6 +325,8 @@ def main():
     ap.add_argument("--batch", type=int, default=2048)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--mips", type=int, default=2, help="also train on this many mip levels of each texture")
+    ap.add_argument("--semantics", default="fixed", choices=["ref", "fixed"],
+                    help="labels from the full search with the reference's semantics or with its shader bugs repaired")
     ap.add_argument("--out", required=True)
     args = ap.parse_args()
     bx, by = (int(v) for v in args.footprint.split("x"))
@@ -331,7 +334,7 @@ def main():
     seeds = list(range(100, 200))
     per = args.blocks / len(seeds)
     side = int(np.ceil(np.sqrt(per))) * max(bx, by)  # about blocks/100 blocks per texture
-    X, part, bm = make_dataset(bx, by, seeds, side, mips=args.mips)
+    X, part, bm = make_dataset(bx, by, seeds, side, mips=args.mips, fixed=args.semantics == "fixed")
     nval = min(65536, len(X) // 20)
     tr = Trainer(lay, init_weights(lay, seed=1), batch=args.batch, lr=args.lr)
     t0 = time.time()
