@@ -305,8 +305,10 @@ def save_weights(path, w, lay):
                         footprint=np.array([lay.bx, lay.by]), outputs=np.array(lay.outputs))
 
 
-def load_weights(bx, by, path=None):
-    path = path or os.path.join(WEIGHTS_DIR, "proposal_%dx%d.npz" % (bx, by))
+def load_weights(bx, by, path=None, labels="fixed"):
+    """A shipped network: trained on the FIXED full search's labels (the default) or, with
+    labels="ref", on the labels of the full search with the reference's semantics."""
+    path = path or os.path.join(WEIGHTS_DIR, "proposal_%dx%d%s.npz" % (bx, by, "" if labels == "fixed" else "_ref"))
     d = np.load(path)
     to32 = lambda a: (a.astype(np.uint32) << 16).view(np.float32)
     return {"w1": to32(d["w1"]), "w2": to32(d["w2"]), "w3": to32(d["w3"]), "b1": d["b1"].astype(np.float32),
