@@ -273,10 +273,11 @@ class ASTCEncoder:
                           arrs["w3"].shape[0], *[arrs[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")])
         _check(load_library().astcb200_set_proposal_net(self._ctx, ctypes.byref(net)), self._ctx)
 
-    def set_pruning(self, enable=True, max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98,
-                    threshold=0.5, reroute_error=8.0, front_threads=0, refine_iterations=3,
-                    single_partition_floor=0.0, fallback_iterations=3):
-        """Proposal-search settings for later encodes of footprints with a network."""
+    def set_pruning(self, enable=True, max_partitionings=0, block_modes=0, refine_candidates=0, coverage=0.95,
+                    threshold=0.5, reroute_error=8.0, front_threads=0, refine_iterations=0,
+                    single_partition_floor=0.0, fallback_iterations=0):
+        """Proposal-search settings for later encodes of footprints with a network; 0 in the
+        integer settings selects the footprint's tuned value (see astcb200_pruning)."""
         cfg = Pruning(ctypes.sizeof(Pruning), 1 if enable else 0, max_partitionings, block_modes, refine_candidates,
                       coverage, threshold, reroute_error, front_threads, refine_iterations, single_partition_floor,
                       fallback_iterations)

@@ -95,7 +95,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         if (launches) *launches += ni;
         return ASTCB200_OK;
     }
-    const Pruning& pr = ctx->pruning;
+    const Pruning pr = resolve_pruning(ctx->pruning, ft->L.T);
     const size_t n = (size_t)a.nblocks;
     if ((ctx->counts_used + 1) * mlp::kRouteCounters > ctx->counts_cap / sizeof(int)) {
         ctx->err = "route counters exhausted";
@@ -250,8 +250,8 @@ int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* w)
 
 int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     if (!ctx || !cfg || cfg->struct_size < sizeof(astcb200_pruning)) return ASTCB200_BAD_ARG;
-    if (cfg->enable && (cfg->max_partitionings > (uint32_t)kMaxProposals || cfg->block_modes == 0 || cfg->block_modes > 64 ||
-                        cfg->refine_candidates == 0 || cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
+    if (cfg->enable && (cfg->max_partitionings > (uint32_t)kMaxProposals || cfg->block_modes > 64 ||
+                        cfg->refine_candidates > (uint32_t)kNumCand || !(cfg->coverage >= 0.0f) ||
                         !(cfg->threshold >= 0.0f) || !(cfg->reroute_error >= 0.0f) ||
                         (cfg->front_threads && cfg->front_threads != 32 && cfg->front_threads != 64 && cfg->front_threads != 128) ||
                         cfg->refine_iterations > 6 || !(cfg->single_partition_floor >= 0.0f) || cfg->fallback_iterations > 6))
@@ -265,9 +265,9 @@ int astcb200_set_pruning(astcb200_ctx* ctx, const astcb200_pruning* cfg) {
     p.threshold = cfg->threshold;
     p.reroute_error = cfg->reroute_error;
     p.front_threads = (int)cfg->front_threads;
-    p.refine_iters = cfg->struct_size >= sizeof(astcb200_pruning) && cfg->refine_iterations ? (int)cfg->refine_iterations : 3;
-    p.p1_floor = cfg->struct_size >= sizeof(astcb200_pruning) ? cfg->single_partition_floor : 0.0f;
-    p.fallback_iters = cfg->fallback_iterations ? (int)cfg->fallback_iterations : 3;
+    p.refine_iters = (int)cfg->refine_iterations;
+    p.p1_floor = cfg->single_partition_floor;
+    p.fallback_iters = (int)cfg->fallback_iterations;
     release_batches(ctx);  // captured graphs hold the previous settings
     return ASTCB200_OK;
 }
@@ -368,7 +368,7 @@ int astcb200_proposal_selection(astcb200_ctx* ctx, const uint8_t* rgba8, uint8_t
     a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
     a.tables = ctx->cur->d;
     a.L = ctx->cur->L;
-    const Pruning& pr = ctx->pruning;
+    const Pruning pr = resolve_pruning(ctx->pruning, ctx->cur->L.T);
     mlp::Select sel;
     sel.kmax = pr.kmax; sel.coverage = pr.coverage; sel.threshold = pr.threshold; sel.kbm = pr.kbm;
     sel.p1_floor = pr.p1_floor;

@@ -303,9 +303,13 @@ def run_combined(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     spec = combined_textures(args.count, args.min_side, args.max_side)
+    # the textures are generated on all host cores by spawned workers (fresh processes, no CUDA state)
+    import multiprocessing
+    with multiprocessing.get_context("spawn").Pool(max(1, min(16, os.cpu_count() or 1))) as pool:
+        host = pool.starmap(synth.make_texture, spec)
     levels = []  # (device tensor, w, h)
-    for w, h, seed in spec:
-        d = torch.from_numpy(synth.make_texture(w, h, seed).reshape(-1)).cuda()
+    for (w, h, seed), img in zip(spec, host):
+        d = torch.from_numpy(img.reshape(-1)).cuda()
         dims = ab.mip_dims(w, h)
         levels.append((d, w, h))
         for (pw, ph), (cw, ch) in zip(dims[:-1], dims[1:]):
@@ -345,11 +349,12 @@ def run_combined(args):
                 k += 1
         return np.array(q)
 
-    full = ab.ASTCEncoder(device=local)
+    fixed = args.semantics == "fixed"
+    full = ab.ASTCEncoder(device=local, fixed=fixed)
     ms_full = timed(full, 1)
     q_full = quality()
     full.close()
-    enc = ab.ASTCEncoder(device=local)
+    enc = ab.ASTCEncoder(device=local, fixed=fixed)
     for fp in (4, 6):
         enc.set_proposal_net(proposal.load_weights(fp, fp))
     enc.set_pruning(True, **PRUNING)
@@ -372,7 +377,7 @@ def run_combined(args):
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "%d textures, sides log-uniform %d-%d per axis, full box-filtered mip chains to 1x1, "
                                "at 6x6 and 4x4, one batch per step" % (args.count, args.min_side, args.max_side),
-                   "textures_with_mips": len(levels), "texels_per_step": texels},
+                   "textures_with_mips": len(levels), "texels_per_step": texels, "semantics": args.semantics},
         "full_search": {"value": round(texels / (ms_full / 1000.0) / 1e6, 3), "ms_per_step": round(ms_full, 3)},
         "speedup_vs_full_search": round(ms_full / ms, 3),
         "psnr": {"mean_delta_db": round(float(d.mean()), 3), "min_delta_db": round(float(d.min()), 3),
@@ -473,7 +478,14 @@ def run_settings(args):
 
 
 # ---------------------------------------------------------------- B200 arm
-PRUNING = dict(max_partitionings=4, block_modes=16, refine_candidates=2, coverage=0.98, threshold=0.5, reroute_error=8.0)
+# The library's tuned per-footprint proposal settings (astcb200_pruning zeros): for 4x4, 8
+# partitionings, all block modes, 8 candidates, 6 iterations (6 in the fallback); for 6x6, 4
+# partitionings, 8 block modes per partition count, 4 candidates, 6 iterations (3 in the
+# fallback); coverage 0.95, threshold 0.5, reroute above 8.  Chosen on held-out seeds 7-8
+# (this workload encodes seeds 1-4) as the fastest within 0.1 dB of the FIXED full search.
+PRUNING = dict(coverage=0.95, threshold=0.5, reroute_error=8.0)
+TUNED = {"4x4": dict(max_partitionings=8, block_modes=64, refine_candidates=8, refine_iterations=6, fallback_iterations=6),
+         "6x6": dict(max_partitionings=4, block_modes=8, refine_candidates=4, refine_iterations=6, fallback_iterations=3)}
 CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
 
 
@@ -523,8 +535,9 @@ def main():
                     help="timed method: the learned proposal search (headline) or the full search alone")
     ap.add_argument("--skip-full", action="store_true",
                     help="do not run the full search for comparison (profiling the timed method alone)")
-    ap.add_argument("--semantics", default="ref", choices=["ref", "fixed"],
-                    help="semantics of the timed method: the reference's (bit-exact) or with its shader bugs repaired")
+    ap.add_argument("--semantics", default="fixed", choices=["ref", "fixed"],
+                    help="semantics of the timed method and of the full search it is compared with: FIXED (the "
+                         "reference's shader bugs repaired, the default) or the reference's own (bit-exact to it)")
     ap.add_argument("--settings", default="[{}]", help="settings workload: JSON list of set_pruning keyword sets")
     ap.add_argument("--seeds", default=None, help="settings workload: generator seeds (default 7,8,9,10, held out)")
     args = ap.parse_args()
@@ -559,6 +572,7 @@ def main():
     d_imgs = [torch.from_numpy(im.reshape(-1)).to("cuda") for im in imgs]
     use_prop = args.method == "proposal"
     fixed = args.semantics == "fixed"
+    same = args.semantics
 
     def make_encs(fixed_sem, with_net):
         es = []
@@ -705,8 +719,10 @@ def main():
                             os.cpu_count())}
         parity = parity_vs_cpu(np.ascontiguousarray(imgs[0][:args.cpu_sample, :args.cpu_sample]), cpu_blocks, local)
     fp_names = " and ".join("%dx%d" % f for f in FOOTPRINTS)
-    method = ("learned proposal search (%s), full search for low-confidence and poorly encoded blocks"
-              % ", ".join("%s=%s" % kv for kv in PRUNING.items())) if use_prop else "full search"
+    method = ("learned proposal search (tuned per footprint: %s; %s), full search for low-confidence and poorly "
+              "encoded blocks" % ("; ".join("%s %s" % (f, ", ".join("%s=%s" % kv for kv in TUNED[f].items()))
+                                            for f in ["%dx%d" % fp for fp in FOOTPRINTS] if f in TUNED),
+                                  ", ".join("%s=%s" % kv for kv in PRUNING.items()))) if use_prop else "full search"
     method += "; %s semantics" % ("FIXED (the reference's shader bugs repaired)" if fixed else "the reference's (REF)")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mtexel/s", "n_gpus": world, "steps": args.steps,
@@ -717,9 +733,12 @@ def main():
                    "method": method, "image": [SIZE, SIZE], "footprints": ["%dx%d" % f for f in FOOTPRINTS],
                    "chunk_blocks": CHUNK, "l2": "512 MiB memset before every step, inside the timed region",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "full_search": {"value": round(full["ref"]["value"], 3), "unit": "Mtexel/s", "semantics": "ref",
-                        "ms_per_step": round(full["ref"]["ms"], 3)} if "ref" in full else None,
-        "speedup_vs_full_search": round(value / full["ref"]["value"], 3) if "ref" in full else None,
+        "full_search": {"value": round(full[same]["value"], 3), "unit": "Mtexel/s", "semantics": same,
+                        "ms_per_step": round(full[same]["ms"], 3)} if same in full else None,
+        "speedup_vs_full_search": round(value / full[same]["value"], 3) if same in full else None,
+        "full_search_ref": {"value": round(full["ref"]["value"], 3), "unit": "Mtexel/s", "semantics": "ref",
+                            "ms_per_step": round(full["ref"]["ms"], 3)} if "ref" in full else None,
+        "speedup_vs_ref_full_search": round(value / full["ref"]["value"], 3) if "ref" in full else None,
         "full_search_fixed": {"value": round(full["fixed"]["value"], 3), "unit": "Mtexel/s", "semantics": "fixed",
                               "ms_per_step": round(full["fixed"]["ms"], 3)} if "fixed" in full else None,
         "speedup_vs_fixed_full_search": round(value / full["fixed"]["value"], 3) if "fixed" in full else None,
@@ -738,7 +757,7 @@ def main():
         line["parity_vs_cpu_oracle"] = parity
     if use_prop and prop_psnr:
         order = ["%dx%d seed %d" % (fp[0], fp[1], s) for fp in FOOTPRINTS for s in seeds]
-        for key, name in (("ref", "psnr"), ("fixed", "psnr_vs_fixed")):
+        for key, name in ((same, "psnr"), ("ref", "psnr_vs_ref"), ("fixed", "psnr_vs_fixed")):
             if key not in full:
                 continue
             d = [p - f for p, f in zip(prop_psnr, full[key]["psnr"])]

@@ -118,11 +118,11 @@ def test_batch_fixed_equals_single_images():
     enc.close()
 
 
-@pytest.mark.parametrize("bx,by", [(4, 4), (6, 6)])
-def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by):
-    """The proposal search with FIXED semantics: every proposal-search block equals the FIXED
-    oracle restricted to the GPU's selection; every other block equals the FIXED full search
-    with the fallback's iteration count."""
+@pytest.mark.parametrize("bx,by,topn,iters,fb", [(4, 4, 8, 6, 6), (6, 6, 4, 6, 3)])
+def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by, topn, iters, fb):
+    """The proposal search with FIXED semantics and the footprint's tuned settings: every
+    proposal-search block equals the FIXED oracle restricted to the GPU's selection; every
+    other block equals the FIXED full search with the fallback's iteration count."""
     net = proposal.load_weights(bx, by)
     w, h = 11 * bx + 3, 7 * by + 2
     img = synth.make_texture(w, h, 190 + bx)
@@ -140,9 +140,9 @@ def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by):
     found = np.zeros(n, np.uint8)
     with fixed_oracle():
         assert _libs.oracle().orc_encode_restricted(_libs.ptr(img), w, h, bx, by, 0, _libs.ptr(np.ascontiguousarray(picks)),
-                                                    _libs.ptr(np.ascontiguousarray(masks)), 2, 3, _libs.ptr(r_out),
+                                                    _libs.ptr(np.ascontiguousarray(masks)), topn, iters, _libs.ptr(r_out),
                                                     _libs.ptr(r_sym), _libs.ptr(found)) == 0
-    f_out, f_sym = oracle_encode(img, bx, by, iters=3)
+    f_out, f_sym = oracle_encode(img, bx, by, iters=fb)
     prop = (route == 0) & found.astype(bool)
     assert prop.sum() > 0.5 * n
     assert np.array_equal(sym[prop], r_sym[prop]) and np.array_equal(blocks[prop], r_out[prop])

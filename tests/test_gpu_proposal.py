@@ -179,8 +179,10 @@ def full_oracle(img, bx, by, iters=6):
 
 
 @pytest.mark.parametrize("bx,by,net_kind,prune", [
-    (4, 4, "shipped", dict(topn=2, iters=3, fb=3)),
-    (6, 6, "shipped", dict(topn=2, iters=3, fb=3)),
+    (4, 4, "shipped", dict(topn=8, iters=6, fb=6)),  # the tuned settings of 4x4 (all zeros: defaults)
+    (6, 6, "shipped", dict(topn=4, iters=6, fb=3)),  # and of 6x6
+    (6, 6, "shipped", dict(max_partitionings=4, block_modes=16, refine_candidates=2, refine_iterations=3,
+                           fallback_iterations=3, coverage=0.98, topn=2, iters=3, fb=3)),
     (4, 4, "random", dict(max_partitionings=6, block_modes=8, refine_candidates=4, refine_iterations=6,
                           coverage=0.999, threshold=1e-4, single_partition_floor=0.3, topn=4, iters=6,
                           fallback_iterations=6, fb=6)),
@@ -263,12 +265,13 @@ def test_reroute_keeps_the_better_of_both_searches(bx, by):
 
 
 def test_shipped_networks_beat_the_full_search():
-    """The trained networks (astc_implementation_b200/weights) with the default settings:
-    held-out textures (generator seeds 7-9, never used for training) encode at least as
-    well as with the full search, and the untrained network of the same shape does worse."""
+    """The trained networks (astc_implementation_b200/weights) with the tuned default settings,
+    in FIXED semantics: held-out textures (generator seeds 7-9, never used for training)
+    encode within 0.1 dB of the FIXED full search on average, and the untrained network of
+    the same shape does worse."""
     for bx in (4, 6):
         imgs = [synth.make_texture(256, 256, s) for s in (7, 8, 9)]
-        enc = ab.ASTCEncoder(device=0)
+        enc = ab.ASTCEncoder(device=0, fixed=True)
         enc.secondaryInit(256, 256, bx, bx)
         dec = lambda: [ab.psnr(ab.decode(bx, bx, 256, 256, enc.encode(im)), im) for im in imgs]
         full = dec()
