@@ -267,28 +267,34 @@ def test_reroute_keeps_the_better_of_both_searches(bx, by):
 def test_shipped_networks_beat_the_full_search():
     """The trained networks (astc_implementation_b200/weights), in FIXED semantics, on held-out
     textures (generator seeds 7-9, never used for training): with the tuned default settings
-    they encode within 0.1 dB of the FIXED full search on average and better than the
-    untrained network of the same shape; with a small budget (2 partitionings, 8 block modes,
-    2 candidates), where the network's ranking decides what is searched at all, the gain over
-    the untrained network is above 1 dB."""
-    small = dict(max_partitionings=2, block_modes=8, refine_candidates=2, refine_iterations=3)
+    they encode within 0.1 dB of the FIXED full search on average.  Against the untrained
+    network of the same shape, both searching only what they propose (no confidence
+    fallback and no reroute: an untrained network's low confidence would hand every block to
+    the full search), the trained one is better with the tuned settings and by more with a
+    small budget (2 partitionings, 8 block modes, 2 candidates), where its ranking decides
+    what is searched at all."""
+    own = dict(threshold=0.0, reroute_error=0.0)
+    small = dict(max_partitionings=2, block_modes=8, refine_candidates=2, refine_iterations=3, **own)
     for bx in (4, 6):
         imgs = [synth.make_texture(256, 256, s) for s in (7, 8, 9)]
         enc = ab.ASTCEncoder(device=0, fixed=True)
         enc.secondaryInit(256, 256, bx, bx)
         dec = lambda: np.mean([ab.psnr(ab.decode(bx, bx, 256, 256, enc.encode(im)), im) for im in imgs])
         full = dec()
+        enc.set_proposal_net(proposal.load_weights(bx, bx))
+        enc.set_pruning(True)
+        tuned = dec()
         res = {}
         for name, net in (("trained", proposal.load_weights(bx, bx)),
                           ("untrained", dict(proposal.init_weights(proposal.Layout(bx, bx), seed=3), footprint=(bx, bx)))):
             enc.set_proposal_net(net)
-            enc.set_pruning(True)
+            enc.set_pruning(True, **own)
             res[name] = dec()
             enc.set_pruning(True, **small)
             res[name + "_small"] = dec()
         enc.close()
-        assert res["trained"] >= full - 0.1, (bx, res, full)
-        assert res["trained"] > res["untrained"] + 0.2, (bx, res)
+        assert tuned >= full - 0.1, (bx, tuned, full)
+        assert res["trained"] > res["untrained"] + 0.3, (bx, res)
         assert res["trained_small"] > res["untrained_small"] + 1.0, (bx, res)
 
 
