@@ -551,6 +551,7 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
         for (int q = 0; q < P; q++) unpack_endpoints(ffmt[q], cs.packed + q * 8, cs.u0[q], cs.u1[q]);
         if (it == 0) final_error();
         // ---------------- pass16: move each weight one quant step if that lowers the error
+        bool moved = false;
         if (direct) {
             for (int t = 0; t < T; t++) {
                 const int p = tp[t];
@@ -563,8 +564,8 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                 const float4 cd = (base + offs * (float)uqw) - px[t];
                 const float4 cdd = cd + offs * (float)(dn - uqw), cdu = cd + offs * (float)(up - uqw);
                 const float eb = dot4(cd * cd, cw), ed = dot4(cdd * cdd, cw), eu = dot4(cdu * cdu, cw);
-                if ((eu < eb) && (eu < ed) && (uqw < 64)) cs.qw[t] = (uint8_t)up;
-                else if ((ed < eb) && (uqw > 0)) cs.qw[t] = (uint8_t)dn;
+                if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[t] = (uint8_t)up; moved |= up != uqw; }
+                else if ((ed < eb) && (uqw > 0)) { cs.qw[t] = (uint8_t)dn; moved |= dn != uqw; }
             }
         } else {
             for (int we = 0; we < dmi.W; we++) {
@@ -596,11 +597,17 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
                     ebv = ebv + cd * cd; edv = edv + cdd * cdd; euv = euv + cdu * cdu;
                 }
                 const float eb = dot4(ebv, cw), ed = dot4(edv, cw), eu = dot4(euv, cw);
-                if ((eu < eb) && (eu < ed) && (uqw < 64)) cs.qw[we] = (uint8_t)up;
-                else if ((ed < eb) && (uqw > 0)) cs.qw[we] = (uint8_t)dn;
+                if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[we] = (uint8_t)up; moved |= (int32_t)up != uqw; }
+                else if ((ed < eb) && (uqw > 0)) { cs.qw[we] = (uint8_t)dn; moved |= (int32_t)dn != uqw; }
             }
         }
         final_error();
+        // A pass16 that moved no weight leaves a fixed point: the next iteration's pass13
+        // recomputes the same endpoints from the same weights (channels whose system is
+        // degenerate keep the previous values, which are these), so packing, unpacking,
+        // realignment and the final error repeat exactly and can never lower the error.
+        // Stopping here gives the same result as running the remaining iterations.
+        if (!moved) break;
     }
 }
 
