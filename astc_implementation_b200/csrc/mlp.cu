@@ -487,8 +487,19 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
             r.pb_list[(size_t)p * r.pb_stride + atomicAdd(&r.counts[2 + p], 1)] = ((uint32_t)pos << 5) | (uint32_t)(k + 1);
         }
     }
-    // block-mode masks: the kbm best modes of each needed head; lane l holds modes l + 32u
+    // block-mode masks: the kbm best modes of each needed head; lane l holds modes l + 32u.
+    // When kbm covers every mode, each needed head's mask is every mode (the ranking would
+    // pick them all).
     uint64_t* mk = r.masks + (size_t)pos * 4 * kMaskWords;
+    if (sel.kbm >= S.nbm) {
+        if (lane < 4 * kMaskWords) {
+            const int p = lane / kMaskWords, w = lane % kMaskWords;
+            const int lo = w * 64;
+            const uint64_t all = S.nbm - lo >= 64 ? ~0ull : S.nbm > lo ? ((1ull << (S.nbm - lo)) - 1) : 0ull;
+            mk[lane] = ((heads >> p) & 1) ? all : 0ull;
+        }
+        return;
+    }
     for (int p = 0; p < 4; p++) {
         if (!((heads >> p) & 1)) continue;
         const float* h = z + S.head_base + p * S.nbm_pad;
