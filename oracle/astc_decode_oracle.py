@@ -5,7 +5,9 @@ decode_block.cuh, compiled for the host and the GPU): instead of parsing the 128
 bits, it starts from the encoder's symbolic result (code/astc.h:639-655, 108 u32 words:
 [1] block mode, [2] partition count, [3] partition seed, [8..11] endpoint formats,
 [12 + 8p ..] partition p's endpoint values on the 0..255 scale, [44 ..] weights on the
-0..64 scale) and applies the ASTC specification's decoding steps to those values:
+0..64 scale; for the library's optional encodings [6] = 1 + the plane-2 component of a
+dual-plane block, whose plane-2 weights are at [76 ..], and [7] = 1 for a void-extent block,
+whose colour is [12..15]) and applies the ASTC specification's decoding steps to those values:
 
   * block-mode fields (weight grid size and weight range) from the 11 mode bits
     (Khronos Data Format Specification 1.3, ASTC section "Block Mode");
@@ -170,10 +172,15 @@ class PartitionTables:
 
 def block_texels(sym, bx, by, parts):
     """(bx*by, 4) uint8 texels of one block from its SymbolicBlock words."""
+    if int(sym[7]):  # void extent: the colour as 16-bit UNORM (x 257), back to 8 bits
+        return np.tile(np.array([((int(v) * 257) * 255 + 32767) // 65535 for v in sym[12:16]], np.uint8), (bx * by, 1))
     g = block_mode_grid(int(sym[1]) & 2047)
-    assert g is not None and g[3] == 0, "single-plane block expected"
+    dual = int(sym[6]) > 0
+    assert g is not None and g[3] == (1 if dual else 0), "plane count of the block mode"
     gx, gy = g[0], g[1]
     w = infill_weights(bx, by, gx, gy, sym[44:44 + gx * gy])
+    w2 = infill_weights(bx, by, gx, gy, sym[76:76 + gx * gy]) if dual else w
+    ccs = int(sym[6]) - 1 if dual else -1
     pc = int(sym[2])
     tp = parts.of_texel(pc, int(sym[3])) if pc > 1 else np.zeros(bx * by, np.int64)
     out = np.zeros((bx * by, 4), np.uint8)
@@ -186,7 +193,8 @@ def block_texels(sym, bx, by, parts):
         e0, e1 = eps[tp[t]]
         for c in range(4):
             c0, c1 = e0[c] * 257, e1[c] * 257
-            v16 = (c0 * (64 - int(w[t])) + c1 * int(w[t]) + 32) >> 6
+            wt = int(w2[t]) if c == ccs else int(w[t])
+            v16 = (c0 * (64 - wt) + c1 * wt + 32) >> 6
             out[t, c] = (v16 + 128) // 257
     return out
 

@@ -1964,6 +1964,13 @@ int bitrev8(int p) {
 // code/physical_compression.cpp:843-1003 symbolic_to_physical (single plane)
 void sym_to_phys(const Footprint& f, const uint32_t* s, uint8_t* pcb) {
     const ConstTables& ct = CT();
+    if (s[7]) {  // extension: LDR void-extent block (mode bits 0x1FC, bits 10-11 set), every
+                 // extent coordinate all ones (no extent), then RGBA as 16-bit UNORM (colour x 257)
+        const uint8_t head[8] = {0xFC, 0xFD, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF};
+        for (int i = 0; i < 8; i++) pcb[i] = head[i];
+        for (int c = 0; c < 4; c++) { pcb[8 + 2 * c] = (uint8_t)s[12 + c]; pcb[9 + 2 * c] = (uint8_t)s[12 + c]; }
+        return;
+    }
     unsigned pc = s[2];
     uint8_t wbuf[16] = {0};
     const BlockMode& bm = f.bms[f.bm_index[s[1]]];
@@ -2006,6 +2013,9 @@ void sym_to_phys(const Footprint& f, const uint32_t* s, uint8_t* pcb) {
     } else {
         write_bits((uint8_t)s[8], 4, 13, pcb);
     }
+    // extension: the plane-2 component of a dual-plane block (the reference leaves it
+    // out, physical_compression.cpp:967-971); single partition only
+    if (bm.dual && pc == 1) write_bits(s[6] - 1, 2, 128 - bits_w - 2, pcb);
     uint8_t vals[32]; int nv = 0;
     const uint8_t* tab = ct.cscr[s[5] - 4];
     for (unsigned i = 0; i < pc; i++) {
@@ -2023,6 +2033,220 @@ void sym_to_words(const Sym& s, uint32_t* o) {
     for (int i = 0; i < 4; i++) o[8 + i] = s.fmt[i];
     for (int i = 0; i < 32; i++) o[12 + i] = s.packed[i];
     for (int i = 0; i < 64; i++) o[44 + i] = s.qw[i];
+}
+
+
+// ---------------------------------------------------------------- extension (no reference counterpart)
+// Opt-in encodings the reference never emits (orc_set_extensions): an LDR void-extent block
+// for a block whose texels are all equal, and single-partition dual-plane blocks, tried after
+// the search and kept when their decoded error is lower.  Errors here are exact decoded
+// errors: integer texels against the 8-bit texels a decoder produces (weights infilled with
+// the specification's integer weights, endpoints x257, integer interpolation, 16-bit to 8-bit
+// rounding), weighted by the channel weights x 10^4 in 64-bit integers.
+// Symbolic words of these blocks: [6] = 1 + plane-2 component (dual plane), [7] = 1 (void
+// extent, colour in [12..15]); dual plane: plane-1 weights [44..], plane-2 weights [76..].
+int g_ext = 0;  // bit 0: void extent, bit 1: dual plane
+const int64_t CWI[4] = {6750, 13275, 2475, 10000};
+
+inline int dec8(int32_t v16) { return (int)(((uint32_t)v16 * 255u + 32767u) / 65535u); }
+inline int32_t lerp16(int32_t e0, int32_t e1, int32_t w) { return (e0 * (64 - w) + e1 * w + 32) >> 6; }
+
+// Integer infill of texel t from 0..64 grid weights (the specification's weights / 16).
+int32_t infill_int(const Footprint& f, const DecInfo& di, const uint32_t* qw, int t) {
+    if (di.W == di.T) return (int32_t)qw[t];
+    int32_t s = 0;
+    for (uint32_t j = 0; j < di.tw_count[t]; j++) {
+        const uint32_t k = di.tw_off[t] + j;
+        s += (int32_t)(f.t2w_c[k] * 16.0f) * (int32_t)qw[f.t2w_idx[k]];
+    }
+    return (s + 8) >> 4;
+}
+
+// Exact decoded error of a single-plane symbolic block (words) against 8-bit texels c8.
+int64_t exact_error_single(const Footprint& f, const uint32_t* s, const uint8_t (*c8)[4]) {
+    const BlockMode& bm = f.bms[f.bm_index[s[1] & 2047]];
+    const DecInfo& di = f.dis[bm.dm];
+    const int P = (int)s[2];
+    Cand c; std::memset(&c, 0, sizeof(c));
+    for (int i = 0; i < 4; i++) c.ffmt[i] = s[8 + i];
+    for (int i = 0; i < 32; i++) c.packed[i] = s[12 + i];
+    int32_t e0[4][4], e1[4][4];
+    pass15(P, c, e0, e1);
+    const PartInfo* pi = P > 1 ? &f.pinfo[(P - 2) * 1024 + f.packed_index[P - 2][s[3]]] : nullptr;
+    int64_t err = 0;
+    for (int t = 0; t < f.T; t++) {
+        const int p = pi ? (int)pi->of_texel[t] : 0;
+        const int32_t w = infill_int(f, di, &s[44], t);
+        for (int ch = 0; ch < 4; ch++) {
+            const int d = (int)c8[t][ch] - dec8(lerp16(e0[p][ch], e1[p][ch], w));
+            err += CWI[ch] * (int64_t)(d * d);
+        }
+    }
+    return err;
+}
+
+// Dual-plane search of one block (single partition): plane-2 component c = 0..3 (3 only when
+// alpha varies), every dual-plane block mode of the footprint whose grid is a trial
+// decimation mode, in block-mode order; the first minimum of the exact error wins.
+// Returns the error (INT64_MAX if no candidate fits) and its symbolic words in `o`.
+int64_t dual_plane_search(const Footprint& f, const uint8_t (*c8)[4], uint32_t* o) {
+    const ConstTables& ct = CT();
+    const int T = f.T;
+    bool calpha = true;
+    int sum[4] = {0, 0, 0, 0};
+    for (int t = 0; t < T; t++) { calpha = calpha && c8[t][3] == 255; for (int ch = 0; ch < 4; ch++) sum[ch] += c8[t][ch]; }
+    bool const_a = true;
+    for (int t = 0; t < T; t++) const_a = const_a && c8[t][3] == c8[0][3];
+    std::vector<uint32_t> lookup(f.dis.size(), 0xFFFF);
+    for (uint32_t d = 0; d < f.valid_dms.size(); d++) lookup[f.valid_dms[d]] = d;
+    int64_t best = INT64_MAX;
+    float w1[MAX_TEXELS], w2[MAX_TEXELS];
+    for (int ccs = 0; ccs < 4; ccs++) {
+        if (ccs == 3 && const_a) continue;
+        // plane 1: the other channels' line through the mean, direction by positive-deviation sums
+        float mu[4];
+        for (int ch = 0; ch < 4; ch++) mu[ch] = (float)sum[ch] / (float)T;
+        float S[4][4] = {{0}};
+        for (int t = 0; t < T; t++) {
+            float d[4];
+            for (int ch = 0; ch < 4; ch++) d[ch] = ch == ccs ? 0.0f : (float)c8[t][ch] - mu[ch];
+            for (int ax = 0; ax < 4; ax++)
+                if (ax != ccs && d[ax] > 0.0f)
+                    for (int ch = 0; ch < 4; ch++) S[ax][ch] = S[ax][ch] + d[ch];
+        }
+        int bax = -1; float bl = 0.0f;
+        for (int ax = 0; ax < 4; ax++) {
+            if (ax == ccs) continue;
+            float l = S[ax][0] * S[ax][0]; l = l + S[ax][1] * S[ax][1]; l = l + S[ax][2] * S[ax][2]; l = l + S[ax][3] * S[ax][3];
+            if (l > bl) { bl = l; bax = ax; }
+        }
+        float dir[4] = {0, 0, 0, 0};
+        if (bax >= 0) { const float len = std::sqrt(bl); for (int ch = 0; ch < 4; ch++) dir[ch] = S[bax][ch] / len; }
+        float pmin = 1e30f, pmax = -1e30f, prm[MAX_TEXELS];
+        for (int t = 0; t < T; t++) {
+            float d[4];
+            for (int ch = 0; ch < 4; ch++) d[ch] = ch == ccs ? 0.0f : (float)c8[t][ch] - mu[ch];
+            float v = d[0] * dir[0]; v = v + d[1] * dir[1]; v = v + d[2] * dir[2]; v = v + d[3] * dir[3];
+            prm[t] = v; pmin = fmn(pmin, v); pmax = fmx(pmax, v);
+        }
+        int vmin = 255, vmax = 0;
+        for (int t = 0; t < T; t++) { vmin = std::min(vmin, (int)c8[t][ccs]); vmax = std::max(vmax, (int)c8[t][ccs]); }
+        for (int t = 0; t < T; t++) {
+            w1[t] = pmax > pmin ? (prm[t] - pmin) / (pmax - pmin) : 0.0f;
+            w2[t] = vmax > vmin ? (float)(c8[t][ccs] - vmin) / (float)(vmax - vmin) : 0.0f;
+        }
+        const bool rgb_only = calpha && ccs != 3;
+        const int cem = rgb_only ? FMT_RGB : FMT_RGBA, nint = rgb_only ? 6 : 8;
+        for (uint32_t m = 0; m < 2048; m++) {
+            const uint32_t bi = f.bm_index[m];
+            if (bi == 0xFFFF) continue;
+            const BlockMode& bm = f.bms[bi];
+            if (!bm.dual || lookup[bm.dm] == 0xFFFF) continue;
+            const DecInfo& di = f.dis[bm.dm];
+            const int avail = 109 - (int)bm.weight_bits;
+            int qc = -1;
+            for (int q = 20; q >= 4; q--) if ((int)ise_bitcount(nint, q) <= avail) { qc = q; break; }
+            if (qc < 0) continue;
+            // decimate, quantise (pass07's rule over [0, 1]) both planes
+            uint32_t qw[2][MAX_WEIGHTS];
+            const float qlm1 = (float)(LEVELS[bm.quant] - 1);
+            const int off = ct.q2u_off[bm.quant];
+            for (int pl = 0; pl < 2; pl++) {
+                const float* wv = pl ? w2 : w1;
+                for (uint32_t i = 0; i < di.W; i++) {
+                    float dw;
+                    if (di.W == di.T) dw = wv[i];
+                    else {
+                        float num = 0.0f, den = 0.0f;
+                        for (uint32_t j = 0; j < di.wt_count[i]; j++) {
+                            const uint32_t k = di.wt_off[i] + j;
+                            num = num + f.w2t_c[k] * wv[f.w2t_idx[k]];
+                            den = den + f.w2t_c[k];
+                        }
+                        dw = num / den;
+                    }
+                    const float ix = clampf(dw, 0.0f, 1.0f), ix1 = ix * qlm1;
+                    const uint32_t wl = f2u(ix1), wh = std::min(wl + 1, f2u(qlm1));
+                    const uint32_t li = ct.q2u[off + wl], hi = ct.q2u[off + wh];
+                    qw[pl][i] = ((float)li + (float)hi) < (128.0f * ix) ? hi : li;
+                }
+            }
+            // endpoints per channel by least squares on the channel's plane
+            int32_t wt[2][MAX_TEXELS];
+            for (int t = 0; t < T; t++) { wt[0][t] = infill_int(f, di, qw[0], t); wt[1][t] = infill_int(f, di, qw[1], t); }
+            int ue[2][4];
+            for (int ch = 0; ch < 4; ch++) {
+                const int32_t* wp = wt[ch == ccs ? 1 : 0];
+                float a = 0.0f, b = 0.0f, cc = 0.0f, s0 = 0.0f, s1 = 0.0f;
+                for (int t = 0; t < T; t++) {
+                    const float w = (float)wp[t] / 64.0f, om = 1.0f - w, x = (float)c8[t][ch];
+                    a = a + om * om; b = b + om * w; cc = cc + w * w; s0 = s0 + om * x; s1 = s1 + w * x;
+                }
+                const float det = a * cc - b * b;
+                float e0, e1;
+                if (det > 0.0001f * (a * cc)) { e0 = (cc * s0 - b * s1) / det; e1 = (a * s1 - b * s0) / det; }
+                else { e0 = e1 = (float)sum[ch] / (float)T; }
+                e0 = clampf(e0, 0.0f, 255.0f); e1 = clampf(e1, 0.0f, 255.0f);
+                ue[0][ch] = ct.cu2u[qc - 4][(int)rne(e0) * 2 + 1];
+                ue[1][ch] = ct.cu2u[qc - 4][(int)rne(e1) * 2 + 1];
+            }
+            if (rgb_only) { ue[0][3] = 255; ue[1][3] = 255; }
+            // the decoder swaps RGB(A) direct endpoints whose second sum is the smaller
+            if (ue[1][0] + ue[1][1] + ue[1][2] < ue[0][0] + ue[0][1] + ue[0][2]) {
+                for (int ch = 0; ch < 4; ch++) std::swap(ue[0][ch], ue[1][ch]);
+                for (int pl = 0; pl < 2; pl++)
+                    for (uint32_t i = 0; i < di.W; i++) qw[pl][i] = 64 - qw[pl][i];
+                for (int t = 0; t < T; t++) { wt[0][t] = infill_int(f, di, qw[0], t); wt[1][t] = infill_int(f, di, qw[1], t); }
+            }
+            int64_t err = 0;
+            for (int t = 0; t < T; t++)
+                for (int ch = 0; ch < 4; ch++) {
+                    const int d = (int)c8[t][ch] - dec8(lerp16(ue[0][ch] * 257, ue[1][ch] * 257, wt[ch == ccs ? 1 : 0][t]));
+                    err += CWI[ch] * (int64_t)(d * d);
+                }
+            if (err < best) {
+                best = err;
+                std::memset(o, 0, ORC_SYMBOLIC_WORDS * 4);
+                const float fe = (float)err * 1e-4f;
+                std::memcpy(&o[0], &fe, 4);
+                o[1] = m; o[2] = 1; o[5] = (uint32_t)qc; o[6] = 1 + ccs; o[8] = (uint32_t)cem;
+                for (int ch = 0; ch < nint / 2; ch++) { o[12 + 2 * ch] = (uint32_t)ue[0][ch]; o[12 + 2 * ch + 1] = (uint32_t)ue[1][ch]; }
+                for (uint32_t i = 0; i < di.W; i++) { o[44 + i] = qw[0][i]; o[76 + i] = qw[1][i]; }
+            }
+        }
+    }
+    return best;
+}
+
+// Applies the enabled extensions to one block's symbolic words (c8: its edge-clamped texels).
+void apply_extensions(const Footprint& f, const uint8_t (*c8)[4], uint32_t* s) {
+    if (!g_ext) return;
+    const int T = f.T;
+    bool constant = true;
+    for (int t = 1; t < T && constant; t++)
+        for (int ch = 0; ch < 4; ch++) constant = constant && c8[t][ch] == c8[0][ch];
+    if ((g_ext & 1) && constant) {
+        std::memset(s, 0, ORC_SYMBOLIC_WORDS * 4);
+        s[2] = 1; s[7] = 1;
+        for (int ch = 0; ch < 4; ch++) s[12 + ch] = c8[0][ch];
+        return;
+    }
+    if (!(g_ext & 2)) return;
+    const int64_t es = exact_error_single(f, s, c8);
+    uint32_t o[ORC_SYMBOLIC_WORDS];
+    const int64_t ed = dual_plane_search(f, c8, o);
+    if (ed < es) std::memcpy(s, o, sizeof(o));
+}
+
+void block_c8(const uint8_t* img, int w, int h, int bx, int by, int bxi, int byi, uint8_t (*c8)[4]) {
+    int t = 0;
+    for (int dy = 0; dy < by; dy++) {
+        const int y = std::min(byi * by + dy, h - 1);
+        for (int dx = 0; dx < bx; dx++, t++) {
+            const int x = std::min(bxi * bx + dx, w - 1);
+            for (int c = 0; c < 4; c++) c8[t][c] = img[((size_t)y * w + x) * 4 + c];
+        }
+    }
 }
 
 template <class F>
@@ -2046,6 +2270,12 @@ void run_parallel(int n, int threads, F fn) {
 
 extern "C" {
 
+int orc_set_extensions(int flags) {
+    const int prev = g_ext;
+    g_ext = flags & 3;
+    return prev;
+}
+
 int orc_set_semantics(int fixed) {
     const int prev = g_fixed;
     g_fixed = fixed ? 1 : 0;
@@ -2062,6 +2292,7 @@ int orc_encode(const uint8_t* rgba, int width, int height, int bx, int by, int t
         InputBlock b; make_block(rgba, width, height, bx, by, i % nbx, i / nbx, b);
         Sym s = encode_block(f, b, w);
         uint32_t words[ORC_SYMBOLIC_WORDS]; sym_to_words(s, words);
+        if (g_ext) { uint8_t c8[MAX_TEXELS][4]; block_c8(rgba, width, height, bx, by, i % nbx, i / nbx, c8); apply_extensions(f, c8, words); }
         if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
         sym_to_phys(f, words, out_blocks + (size_t)i * 16);
     });
@@ -2078,6 +2309,7 @@ int orc_encode_iters(const uint8_t* rgba, int width, int height, int bx, int by,
         InputBlock b; make_block(rgba, width, height, bx, by, i % nbx, i / nbx, b);
         Sym s = encode_block(f, b, w, refine_iters);
         uint32_t words[ORC_SYMBOLIC_WORDS]; sym_to_words(s, words);
+        if (g_ext) { uint8_t c8[MAX_TEXELS][4]; block_c8(rgba, width, height, bx, by, i % nbx, i / nbx, c8); apply_extensions(f, c8, words); }
         if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
         sym_to_phys(f, words, out_blocks + (size_t)i * 16);
     });
@@ -2128,6 +2360,7 @@ int orc_encode_restricted(const uint8_t* rgba, int width, int height, int bx, in
         uint32_t words[ORC_SYMBOLIC_WORDS];
         if (ok) sym_to_words(s, words);
         else std::memset(words, 0, sizeof(words));  // no block to describe
+        if (ok && g_ext) { uint8_t c8[MAX_TEXELS][4]; block_c8(rgba, width, height, bx, by, i % nbx, i / nbx, c8); apply_extensions(f, c8, words); }
         if (symbolic) std::memcpy(symbolic + (size_t)i * ORC_SYMBOLIC_WORDS, words, sizeof(words));
         if (out_blocks) {
             if (ok) sym_to_phys(f, words, out_blocks + (size_t)i * 16);

@@ -32,6 +32,13 @@ extern "C" {
 // set it between calls.
 int orc_set_semantics(int fixed);
 
+// Selects the encodings beyond the reference's (no counterpart in it) for later calls:
+// bit 0 = void-extent blocks for blocks of one colour, bit 1 = single-partition dual-plane
+// blocks where their exact decoded error is lower than the search's result.  Symbolic
+// words of such blocks: [6] = 1 + plane-2 component, [7] = 1 for void extent (colour in
+// [12..15]), plane-2 weights at [76..].  Returns the previous flags.  Not thread-safe.
+int orc_set_extensions(int flags);
+
 // Encodes an RGBA8 image (row-major, 4 bytes per texel) into physical ASTC
 // blocks (16 bytes each, blocks in raster order).  `threads` <= 0 uses all
 // OpenMP threads.  `symbolic` (optional) receives ORC_SYMBOLIC_WORDS u32 per block.
