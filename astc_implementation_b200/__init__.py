@@ -66,7 +66,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("chunk_blocks", ctypes.c_uint32), ("streams", ctypes.c_uint32), ("ms", ctypes.c_double)]
 
 
-FLAG_STAGE_TIMING, FLAG_NO_GRAPH, FLAG_FIXED_SEMANTICS = 1, 2, 4
+FLAG_STAGE_TIMING, FLAG_NO_GRAPH, FLAG_FIXED_SEMANTICS, FLAG_VOID_EXTENT, FLAG_DUAL_PLANE = 1, 2, 4, 8, 16
 
 
 class ProposalNet(ctypes.Structure):
@@ -158,12 +158,16 @@ def _ptr(a):
 class ASTCEncoder:
     """One encoder context bound to one GPU and one CUDA stream."""
 
-    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False, use_graphs=True, fixed=False):
+    def __init__(self, device=0, chunk_blocks=0, timeout_ms=0, stage_timing=False, use_graphs=True, fixed=False,
+                 void_extent=False, dual_plane=False):
         """fixed=True selects the search with the reference's deterministic shader bugs repaired
-        (ASTCB200_FLAG_FIXED_SEMANTICS); the default reproduces the reference bit for bit."""
+        (ASTCB200_FLAG_FIXED_SEMANTICS); the default reproduces the reference bit for bit.
+        void_extent / dual_plane enable the encodings the reference never emits
+        (ASTCB200_FLAG_VOID_EXTENT, ASTCB200_FLAG_DUAL_PLANE)."""
         lib = load_library()
         flags = ((FLAG_STAGE_TIMING if stage_timing else 0) | (0 if use_graphs else FLAG_NO_GRAPH)
-                 | (FLAG_FIXED_SEMANTICS if fixed else 0))
+                 | (FLAG_FIXED_SEMANTICS if fixed else 0) | (FLAG_VOID_EXTENT if void_extent else 0)
+                 | (FLAG_DUAL_PLANE if dual_plane else 0))
         cfg = _Config(ctypes.sizeof(_Config), chunk_blocks, timeout_ms, flags)
         ctx = ctypes.c_void_p()
         _check(lib.astcb200_create(ctypes.byref(ctx), device, ctypes.byref(cfg)))

@@ -15,7 +15,7 @@
 // parse_block, the optimised device build decoded some weights wrongly (found by the
 // device-against-host decoder tests; the debug build and the out-of-line build agree
 // with the host on every block).
-#define ASTC_HD_CALL __host__ __device__ __noinline__
+#define ASTC_HD_CALL static __host__ __device__ __noinline__
 #else
 #define ASTC_HD inline
 #define ASTC_HD_CALL inline

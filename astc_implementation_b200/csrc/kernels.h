@@ -190,5 +190,8 @@ cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_front(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_select_pack(const KernelArgs& a, cudaStream_t s);
+// Optional encodings over the chunk's blocks after the search (flags: bit 0 void extent,
+// bit 1 dual plane); nothing is launched when neither is set.
+cudaError_t launch_extend(const KernelArgs& a, int flags, cudaStream_t s);
 
 }  // namespace astcb200

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <type_traits>
 
+#include "decode_block.cuh"
 #include "device_math.cuh"
 #include "kernels.h"
 
@@ -880,6 +881,350 @@ __global__ void __launch_bounds__(128) k_select_pack(const __grid_constant__ Ker
 }
 
 }  // namespace
+
+namespace {
+
+// ------------------------------------------------------------ optional encodings
+// Encodings the reference never emits, enabled by ASTCB200_FLAG_VOID_EXTENT and
+// ASTCB200_FLAG_DUAL_PLANE, applied to a chunk's blocks after the search has written them:
+// a block whose texels are all equal becomes an LDR void-extent block; otherwise single-
+// partition dual-plane encodings are tried (plane-2 component 0..3, every dual-plane block
+// mode on a trial decimation mode) and the best replaces the search's block when its exact
+// decoded error is lower.  The search's block is decoded with the library's decoder; the
+// candidates' texels are computed the way a decoder produces them (integer weight infill,
+// endpoints x257, integer interpolation, 16-bit to 8-bit rounding); errors are integer
+// weighted squared differences (channel weights x 10^4).  One warp per block; the CPU
+// oracle (orc_set_extensions) computes the same choices bit for bit.
+constexpr int kExtWarps = 4;
+__constant__ int c_cwi[4] = {6750, 13275, 2475, 10000};
+
+struct ExtWarp {
+    uchar4 c8[kMaxTexels];
+    float w1[kMaxTexels], w2[kMaxTexels];
+    float S[4][4];
+    dec::Block kb;
+    uint8_t qw[32][2][32];  // per lane: two planes of up to 32 grid weights
+};
+
+__device__ __forceinline__ int ext_dec8(int v16) { return (int)(((uint32_t)v16 * 255u + 32767u) / 65535u); }
+__device__ __forceinline__ int ext_lerp(int e0, int e1, int w) { return (e0 * (64 - w) + e1 * w + 32) >> 6; }
+
+// Integer infill of texel t from 0..64 grid weights (the specification's weights / 16).
+__device__ __forceinline__ int ext_infill(const uint8_t* tabs, const TableLayout& L, int W, int dmi, const uint8_t* qw, int t) {
+    if (W == L.T) return qw[t];
+    const uint64_t e4 = reinterpret_cast<const uint64_t*>(tabs + L.off_tw4)[(size_t)dmi * L.T + t];
+    int s = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
+        s += (int)(e >> 8) * (int)qw[e & 0xFF];
+    }
+    return (s + 8) >> 4;
+}
+
+// Dual-plane candidate (ccs, dual mode j) from the warp's plane weights: its exact error
+// (LLONG_MAX when no colour quant fits), and with phys != nullptr its block and symbolic words.
+__device__ __noinline__ long long dual_candidate(const KernelArgs& a, const ExtWarp& ws, int ccs, int j, bool calpha,
+                                                 const int* sum, uint8_t (*qw)[32], uint8_t* phys, uint32_t* sym) {
+    const uint8_t* tabs = a.tables;
+    const TableLayout& L = a.L;
+    const int T = L.T;
+    const DevBm bm = reinterpret_cast<const DevBm*>(tabs + L.off_dual)[j];
+    const DevDm dm = reinterpret_cast<const DevDm*>(tabs + L.off_dm)[bm.dm];
+    const int W = dm.W;
+    const bool rgb_only = calpha && ccs != 3;
+    const int nint = rgb_only ? 6 : 8, cem = rgb_only ? 8 : 12;
+    const int avail = 109 - (int)bm.weight_bits;
+    int qc = -1;
+    for (int q = 20; q >= 4; q--)
+        if ((int)ise_bits(nint, q) <= avail) { qc = q; break; }
+    if (qc < 0) return LLONG_MAX;
+    // decimate and quantise both planes (pass07's rule over [0, 1])
+    const float qlm1 = (float)(c_levels_r[bm.quant] - 1);
+    const uint8_t* q2u = tabs + L.off_q2u;
+    const int qoff = tabs[L.off_q2u_start + bm.quant];
+    for (int pl = 0; pl < 2; pl++) {
+        const float* wv = pl ? ws.w2 : ws.w1;
+        for (int i = 0; i < W; i++) {
+            float dw;
+            if (W == T) dw = wv[i];
+            else {
+                float num = 0.0f, den = 0.0f;
+                const int n = tabs[L.off_wt_count + bm.dm * 64 + i];
+                const int base = dm.wt_base + reinterpret_cast<const uint16_t*>(tabs + L.off_wt_start)[bm.dm * 64 + i];
+                for (int k = 0; k < n; k++) {
+                    const uint32_t e = reinterpret_cast<const uint16_t*>(tabs + L.off_w2t)[base + k];
+                    const float c = (float)(e >> 8) * (1.0f / 16.0f);
+                    num = num + c * wv[e & 0xFF];
+                    den = den + c;
+                }
+                dw = num / den;
+            }
+            const float ix = fminf(fmaxf(dw, 0.0f), 1.0f), ix1 = ix * qlm1;
+            const uint32_t wl = f2u(ix1), wh = min(wl + 1, f2u(qlm1));
+            const uint32_t li = q2u[qoff + wl], hi = q2u[qoff + wh];
+            qw[pl][i] = (uint8_t)(((float)li + (float)hi) < (128.0f * ix) ? hi : li);
+        }
+    }
+    // endpoints per channel: least squares on the channel's plane
+    float a1 = 0.0f, b1 = 0.0f, k1 = 0.0f, a2 = 0.0f, b2 = 0.0f, k2 = 0.0f;
+    float s0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, s1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int t = 0; t < T; t++) {
+        const float w1 = (float)ext_infill(tabs, L, W, bm.dm, qw[0], t) / 64.0f;
+        const float w2 = (float)ext_infill(tabs, L, W, bm.dm, qw[1], t) / 64.0f;
+        const float o1 = 1.0f - w1, o2 = 1.0f - w2;
+        a1 = a1 + o1 * o1; b1 = b1 + o1 * w1; k1 = k1 + w1 * w1;
+        a2 = a2 + o2 * o2; b2 = b2 + o2 * w2; k2 = k2 + w2 * w2;
+        const uchar4 x = ws.c8[t];
+        const float xv[4] = {(float)x.x, (float)x.y, (float)x.z, (float)x.w};
+#pragma unroll
+        for (int ch = 0; ch < 4; ch++) {
+            const float w = ch == ccs ? w2 : w1, o = ch == ccs ? o2 : o1;
+            s0[ch] = s0[ch] + o * xv[ch];
+            s1[ch] = s1[ch] + w * xv[ch];
+        }
+    }
+    const uint8_t* cu2u = tabs + L.off_cu2u + (qc - 4) * 512;
+    int ue[2][4];
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) {
+        const float aa = ch == ccs ? a2 : a1, bb = ch == ccs ? b2 : b1, cc = ch == ccs ? k2 : k1;
+        const float det = aa * cc - bb * bb;
+        float e0, e1;
+        if (det > 0.0001f * (aa * cc)) { e0 = (cc * s0[ch] - bb * s1[ch]) / det; e1 = (aa * s1[ch] - bb * s0[ch]) / det; }
+        else { e0 = e1 = (float)sum[ch] / (float)T; }
+        e0 = fminf(fmaxf(e0, 0.0f), 255.0f);
+        e1 = fminf(fmaxf(e1, 0.0f), 255.0f);
+        ue[0][ch] = cu2u[(int)rintf(e0) * 2 + 1];
+        ue[1][ch] = cu2u[(int)rintf(e1) * 2 + 1];
+    }
+    if (rgb_only) { ue[0][3] = 255; ue[1][3] = 255; }
+    if (ue[1][0] + ue[1][1] + ue[1][2] < ue[0][0] + ue[0][1] + ue[0][2]) {  // the decoder would swap
+#pragma unroll
+        for (int ch = 0; ch < 4; ch++) { const int t = ue[0][ch]; ue[0][ch] = ue[1][ch]; ue[1][ch] = t; }
+        for (int pl = 0; pl < 2; pl++)
+            for (int i = 0; i < W; i++) qw[pl][i] = (uint8_t)(64 - qw[pl][i]);
+    }
+    long long err = 0;
+    for (int t = 0; t < T; t++) {
+        const int w1 = ext_infill(tabs, L, W, bm.dm, qw[0], t), w2 = ext_infill(tabs, L, W, bm.dm, qw[1], t);
+        const uchar4 x = ws.c8[t];
+        const int xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int ch = 0; ch < 4; ch++) {
+            const int d = xv[ch] - ext_dec8(ext_lerp(ue[0][ch] * 257, ue[1][ch] * 257, ch == ccs ? w2 : w1));
+            err += (long long)c_cwi[ch] * (long long)(d * d);
+        }
+    }
+    if (phys) {
+        for (int i = 0; i < 108; i++) sym[i] = 0;
+        sym[0] = __float_as_uint((float)err * 1e-4f);
+        sym[1] = bm.mode_index; sym[2] = 1; sym[5] = (uint32_t)qc; sym[6] = 1u + (uint32_t)ccs; sym[8] = (uint32_t)cem;
+        for (int ch = 0; ch < nint / 2; ch++) { sym[12 + 2 * ch] = (uint32_t)ue[0][ch]; sym[13 + 2 * ch] = (uint32_t)ue[1][ch]; }
+        for (int i = 0; i < W; i++) { sym[44 + i] = qw[0][i]; sym[76 + i] = qw[1][i]; }
+        // physical block: interleaved plane weights, mode, partition count, format, plane-2
+        // component below the weights, colour values (single partition)
+        const int q = bm.quant;
+        const uint8_t* wscr = tabs + L.off_wscr + q * 32;
+        const float levels = (float)c_levels_r[q];
+        uint8_t wv[64], wbuf[18];
+        for (int i = 0; i < 18; i++) wbuf[i] = 0;
+        for (int i = 0; i < W; i++) {
+            wv[2 * i] = wscr[(int)((((float)qw[0][i]) / 64.0f) * (levels - 1.0f) + 0.5f)];
+            wv[2 * i + 1] = wscr[(int)((((float)qw[1][i]) / 64.0f) * (levels - 1.0f) + 0.5f)];
+        }
+        const uint32_t wbits = ise_bits(2 * W, q);
+        encode_ise(L, tabs, q, 2 * W, wv, wbuf, 0);
+        for (int i = 0; i < 16; i++) phys[i] = (uint8_t)bitrev8(wbuf[15 - i]);
+        write_bits(bm.mode_index, 11, 0, phys);
+        write_bits(0, 2, 11, phys);
+        write_bits((uint32_t)cem, 4, 13, phys);
+        write_bits((uint32_t)ccs, 2, 128 - wbits - 2, phys);
+        const uint8_t* cscr = tabs + L.off_cscr + (qc - 4) * 256;
+        uint8_t vals[8];
+        for (int k = 0; k < nint; k++) vals[k] = cscr[sym[12 + k]];
+        encode_ise(L, tabs, qc, nint, vals, phys, 17);
+    }
+    return err;
+}
+
+__global__ void __launch_bounds__(kExtWarps * 32) k_extend(const __grid_constant__ KernelArgs a, int flags) {
+    __shared__ ExtWarp wsm[kExtWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    ExtWarp& ws = wsm[warp];
+    const int T = a.L.T, bx = a.L.bx, by = a.L.by;
+    constexpr unsigned FULL = 0xffffffffu;
+    for (int lb = blockIdx.x * kExtWarps + warp; lb < a.nblocks; lb += gridDim.x * kExtWarps) {
+        const int blk = chunk_block(a, lb);
+        if (blk < 0) continue;
+        const BlockSrc src = block_src(a, blk);
+        for (int t = lane; t < T; t += 32) ws.c8[t] = src_rgba8(src, bx, t);
+        __syncwarp();
+        const uchar4 c0 = ws.c8[0];
+        bool same = true, opaque = true, const_a = true;
+        int sum[4] = {0, 0, 0, 0};
+        for (int t = lane; t < T; t += 32) {
+            const uchar4 x = ws.c8[t];
+            same = same && x.x == c0.x && x.y == c0.y && x.z == c0.z && x.w == c0.w;
+            opaque = opaque && x.w == 255;
+            const_a = const_a && x.w == c0.w;
+            sum[0] += x.x; sum[1] += x.y; sum[2] += x.z; sum[3] += x.w;
+        }
+        same = __all_sync(FULL, same);
+        opaque = __all_sync(FULL, opaque);
+        const_a = __all_sync(FULL, const_a);
+#pragma unroll
+        for (int ch = 0; ch < 4; ch++) sum[ch] = __reduce_add_sync(FULL, sum[ch]);
+        uint4* dst = block_dst(a, blk);
+        if (same && (flags & 1)) {  // LDR void-extent block of the colour x 257, no extent
+            if (lane == 0) {
+                *dst = make_uint4(0xFFFFFDFCu, 0xFFFFFFFFu, (uint32_t)c0.x * 0x101u | ((uint32_t)c0.y * 0x101u) << 16,
+                                  (uint32_t)c0.z * 0x101u | ((uint32_t)c0.w * 0x101u) << 16);
+                if (a.symbolic) {
+                    uint32_t* s = a.symbolic + (size_t)blk * 108;
+                    for (int i = 0; i < 108; i++) s[i] = 0;
+                    s[2] = 1; s[7] = 1; s[12] = c0.x; s[13] = c0.y; s[14] = c0.z; s[15] = c0.w;
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        if (!(flags & 2)) { __syncwarp(); continue; }
+        // exact error of the search's block, decoded
+        if (lane == 0) {
+            const uint4 v = *dst;
+            uint8_t raw[16];
+            const uint32_t wv4[4] = {v.x, v.y, v.z, v.w};
+            for (int i = 0; i < 16; i++) raw[i] = (uint8_t)(wv4[i >> 2] >> (8 * (i & 3)));
+            dec::parse_block(raw, bx, by, ws.kb);
+        }
+        __syncwarp();
+        long long es = 0;
+        for (int t = lane; t < T; t += 32) {
+            uint16_t v16[4];
+            dec::texel16(ws.kb, bx, by, t % bx, t / bx, v16);
+            const uchar4 x = ws.c8[t];
+            const int xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int ch = 0; ch < 4; ch++) {
+                const int d = xv[ch] - (int)dec::to_unorm8(v16[ch]);
+                es += (long long)c_cwi[ch] * (long long)(d * d);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) es += __shfl_xor_sync(FULL, es, o);
+        // dual-plane candidates: plane-2 component outer, block modes inner
+        long long best = LLONG_MAX;
+        int best_idx = 0x7FFFFFFF;
+        const int nd = a.L.ndual;
+        for (int pass = 0; pass < 2; pass++) {
+            int ccs_lo = 0, ccs_hi = 3, win_ccs = -1, win_j = -1;
+            if (pass == 1) {  // the winner's plane weights again, then its encoding
+                long long b = best;
+                int bi = best_idx;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const long long ob = __shfl_xor_sync(FULL, b, o);
+                    const int oi = __shfl_xor_sync(FULL, bi, o);
+                    if (ob < b || (ob == b && oi < bi)) { b = ob; bi = oi; }
+                }
+                if (!(b < es)) break;  // the search's block stays
+                win_ccs = bi / nd; win_j = bi % nd;
+                ccs_lo = ccs_hi = win_ccs;
+            }
+            for (int ccs = ccs_lo; ccs <= ccs_hi; ccs++) {
+                if (ccs == 3 && const_a) continue;
+                float mu[4];
+#pragma unroll
+                for (int ch = 0; ch < 4; ch++) mu[ch] = (float)sum[ch] / (float)T;
+                if (lane < 4 && lane != ccs) {  // positive-deviation sums along axis `lane`, in texel order
+                    float Sx = 0.0f, Sy = 0.0f, Sz = 0.0f, Sw = 0.0f;
+                    for (int t = 0; t < T; t++) {
+                        const uchar4 x = ws.c8[t];
+                        const float d0 = ccs == 0 ? 0.0f : (float)x.x - mu[0], d1 = ccs == 1 ? 0.0f : (float)x.y - mu[1];
+                        const float d2 = ccs == 2 ? 0.0f : (float)x.z - mu[2], d3 = ccs == 3 ? 0.0f : (float)x.w - mu[3];
+                        const float dl = lane == 0 ? d0 : lane == 1 ? d1 : lane == 2 ? d2 : d3;
+                        if (dl > 0.0f) { Sx = Sx + d0; Sy = Sy + d1; Sz = Sz + d2; Sw = Sw + d3; }
+                    }
+                    ws.S[lane][0] = Sx; ws.S[lane][1] = Sy; ws.S[lane][2] = Sz; ws.S[lane][3] = Sw;
+                }
+                __syncwarp();
+                int bax = -1;
+                float bl = 0.0f;
+                for (int ax = 0; ax < 4; ax++) {
+                    if (ax == ccs) continue;
+                    float l = ws.S[ax][0] * ws.S[ax][0];
+                    l = l + ws.S[ax][1] * ws.S[ax][1];
+                    l = l + ws.S[ax][2] * ws.S[ax][2];
+                    l = l + ws.S[ax][3] * ws.S[ax][3];
+                    if (l > bl) { bl = l; bax = ax; }
+                }
+                float dir[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (bax >= 0) {
+                    const float len = sqrtf(bl);
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) dir[ch] = ws.S[bax][ch] / len;
+                }
+                float pmin = 1e30f, pmax = -1e30f;
+                int vmin = 255, vmax = 0;
+                for (int t = lane; t < T; t += 32) {
+                    const uchar4 x = ws.c8[t];
+                    const float d0 = ccs == 0 ? 0.0f : (float)x.x - mu[0], d1 = ccs == 1 ? 0.0f : (float)x.y - mu[1];
+                    const float d2 = ccs == 2 ? 0.0f : (float)x.z - mu[2], d3 = ccs == 3 ? 0.0f : (float)x.w - mu[3];
+                    float v = d0 * dir[0];
+                    v = v + d1 * dir[1];
+                    v = v + d2 * dir[2];
+                    v = v + d3 * dir[3];
+                    ws.w1[t] = v;
+                    pmin = fminf(pmin, v); pmax = fmaxf(pmax, v);
+                    const int c = ccs == 0 ? x.x : ccs == 1 ? x.y : ccs == 2 ? x.z : x.w;
+                    vmin = min(vmin, c); vmax = max(vmax, c);
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    pmin = fminf(pmin, __shfl_xor_sync(FULL, pmin, o)); pmax = fmaxf(pmax, __shfl_xor_sync(FULL, pmax, o));
+                    vmin = min(vmin, __shfl_xor_sync(FULL, vmin, o)); vmax = max(vmax, __shfl_xor_sync(FULL, vmax, o));
+                }
+                for (int t = lane; t < T; t += 32) {
+                    const uchar4 x = ws.c8[t];
+                    const int c = ccs == 0 ? x.x : ccs == 1 ? x.y : ccs == 2 ? x.z : x.w;
+                    ws.w1[t] = pmax > pmin ? (ws.w1[t] - pmin) / (pmax - pmin) : 0.0f;
+                    ws.w2[t] = vmax > vmin ? (float)(c - vmin) / (float)(vmax - vmin) : 0.0f;
+                }
+                __syncwarp();
+                if (pass == 0) {
+                    for (int j = lane; j < nd; j += 32) {
+                        const long long e = dual_candidate(a, ws, ccs, j, opaque, sum, ws.qw[lane], nullptr, nullptr);
+                        if (e < best) { best = e; best_idx = ccs * nd + j; }
+                    }
+                } else if (lane == 0) {
+                    uint8_t phys[18];
+                    uint32_t sym[108];
+                    for (int i = 0; i < 18; i++) phys[i] = 0;
+                    dual_candidate(a, ws, win_ccs, win_j, opaque, sum, ws.qw[0], phys, sym);
+                    *dst = make_uint4(phys[0] | (phys[1] << 8) | (phys[2] << 16) | ((uint32_t)phys[3] << 24),
+                                      phys[4] | (phys[5] << 8) | (phys[6] << 16) | ((uint32_t)phys[7] << 24),
+                                      phys[8] | (phys[9] << 8) | (phys[10] << 16) | ((uint32_t)phys[11] << 24),
+                                      phys[12] | (phys[13] << 8) | (phys[14] << 16) | ((uint32_t)phys[15] << 24));
+                    if (a.symbolic) {
+                        uint32_t* s = a.symbolic + (size_t)blk * 108;
+                        for (int i = 0; i < 108; i++) s[i] = sym[i];
+                    }
+                }
+                __syncwarp();  // the next plane-2 component overwrites the plane weights
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_extend(const KernelArgs& a, int flags, cudaStream_t s) {
+    if (!(flags & 3)) return cudaSuccess;
+    int grid = (a.nblocks + kExtWarps - 1) / kExtWarps;
+    if (a.block_list) grid = std::min(grid, kListGridPack);
+    if (grid <= 0) return cudaSuccess;
+    k_extend<<<grid, kExtWarps * 32, 0, s>>>(a, flags);
+    return cudaGetLastError();
+}
 
 size_t refine_smem_bytes(const TableLayout& L, int topn) {
     const size_t pbs = (size_t)refine_pbs(L.T, topn);

@@ -64,6 +64,8 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
                   cudaEvent_t* ev, int8_t* kinds, uint32_t* launches, bool full_only) {
     KernelArgs a = base;
     a.fixed = (ctx->cfg.flags & ASTCB200_FLAG_FIXED_SEMANTICS) ? 1 : 0;
+    // optional encodings after the search (not timed by the stage events)
+    const int ext = ((ctx->cfg.flags & ASTCB200_FLAG_VOID_EXTENT) ? 1 : 0) | ((ctx->cfg.flags & ASTCB200_FLAG_DUAL_PLANE) ? 2 : 0);
     a.tables = ft->d;
     a.L = ft->L;
     a.picks = sc.picks;
@@ -92,6 +94,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         if ((rc = done(launch_front(a, s), "k_front", 1))) return rc;
         if ((rc = done(launch_refine(a, s), "k_refine", 2))) return rc;
         if ((rc = done(launch_select_pack(a, s), "k_select_pack", 3))) return rc;
+        if (ext) { CK(launch_extend(a, ext, s), "k_extend"); ni++; }
         if (launches) *launches += ni;
         return ASTCB200_OK;
     }
@@ -150,6 +153,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     if ((rc = done(launch_front(af, s), "k_front", 1))) return rc;
     if ((rc = done(launch_refine(af, s), "k_refine", 2))) return rc;
     if ((rc = done(launch_select_pack(af, s), "k_select_pack", 3))) return rc;
+    if (ext) { CK(launch_extend(a, ext, s), "k_extend"); ni++; }  // every block of the chunk, after both passes
     if (launches) *launches += ni;
     return ASTCB200_OK;
 }

@@ -543,6 +543,15 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
             pinfo[k] = p.seed;
             for (int q = 0; q < pc; q++) cov[k * 4 + q] = h.cov[pc][(size_t)e * pc + q];
         }
+    std::vector<DevBm> dual;  // dual-plane block modes whose grid is a trial decimation mode
+    {
+        std::vector<uint32_t> lookup(h.dms.size(), 0xFFFF);
+        for (uint32_t d = 0; d < h.valid_dms.size(); d++) lookup[h.valid_dms[d]] = d;
+        for (const HostTables::Bm& b : h.bms)
+            if (b.dual && lookup[b.dm] != 0xFFFF)
+                dual.push_back(DevBm{(uint16_t)b.mode, (uint8_t)lookup[b.dm], (uint8_t)b.quant, (uint8_t)b.bits, {0, 0, 0}});
+    }
+    L.ndual = (int)dual.size();
     std::vector<uint16_t> order(L.nbm);
     for (int i = 0; i < L.nbm; i++) order[i] = (uint16_t)i;
     std::stable_sort(order.begin(), order.end(), [&](uint16_t x, uint16_t y) { return bms[x].dm < bms[y].dm; });
@@ -556,6 +565,7 @@ bool build_tables(int bx, int by, TableLayout& L, std::vector<uint8_t>& blob) {
     L.off_w2t = put(blob, w2t.data(), w2t.size());
     L.off_tw4 = put(blob, tw4.data(), tw4.size());
     L.off_bm_order = put(blob, order.data(), order.size());
+    L.off_dual = put(blob, dual.data(), dual.size());
     L.off_part_texel = put(blob, ptex.data(), ptex.size());
     L.off_part_info = put(blob, pinfo.data(), pinfo.size());
     L.off_part_counts = put(blob, pcnt.data(), pcnt.size());

@@ -55,6 +55,9 @@ struct TableLayout {
     uint32_t off_tw4;         // u64[ndm][T]: the texel's (up to 4) entries of t2w, padded with 0
                               // (weight 0, contribution 0), four u16 in list order
     uint32_t off_bm_order;    // u16[nbm]: block-mode trial indices sorted by decimation mode
+    uint32_t off_dual;        // DevBm[ndual]: dual-plane block modes on trial decimation modes, in
+                              // block-mode order (the optional dual-plane search; no reference use)
+    int32_t ndual;
     uint32_t off_w2t;         // u16 entries: texel index  | (contribution*16) << 8
     uint32_t off_part_texel;  // u8 [3][1024][T]  partition of texel (P = 2..4)
     uint32_t off_part_info;   // u32[3][1024]     seed | count0<<10 | ... (see kernels)

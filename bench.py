@@ -574,10 +574,11 @@ def main():
     fixed = args.semantics == "fixed"
     same = args.semantics
 
-    def make_encs(fixed_sem, with_net):
+    def make_encs(fixed_sem, with_net, ext=False):
         es = []
         for bx, by in FOOTPRINTS:
-            e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, stage_timing=True, fixed=fixed_sem)
+            e = ab.ASTCEncoder(device=local, chunk_blocks=CHUNK, stage_timing=True, fixed=fixed_sem, void_extent=ext,
+                               dual_plane=ext)
             e.init()
             e.secondaryInit(SIZE, SIZE, bx, by)
             if with_net:
@@ -671,6 +672,21 @@ def main():
     h2d = SIZE * SIZE * 4 * len(FOOTPRINTS)
     d2h = sum(blocks_of(bx, by) * 16 for bx, by in FOOTPRINTS)
 
+    # the same method with the optional encodings (void-extent and dual-plane blocks)
+    ext = None
+    if use_prop and prop_psnr and not args.skip_full:
+        for e in encs:
+            e.close()
+        encs = make_encs(fixed, True, ext=True)
+        xms, _, _, _ = run(encs, nfull, 1, False)
+        xrate, xms = job_rate(texels_per_step() * nfull, xms, dist, "cuda")
+        xpsnr = psnrs(encs)
+        d = [p - q for p, q in zip(xpsnr, prop_psnr)]
+        ext = {"value": round(xrate, 3), "unit": "Mtexel/s", "ms_per_step": round(xms / nfull, 3),
+               "psnr_gain_db": {"mean": round(float(np.mean(d)), 3), "min": round(float(np.min(d)), 3),
+                                "per_image": [round(v, 3) for v in d]},
+               "method": "the timed method plus ASTCB200_FLAG_VOID_EXTENT and ASTCB200_FLAG_DUAL_PLANE"}
+
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -755,6 +771,8 @@ def main():
     }
     if parity:
         line["parity_vs_cpu_oracle"] = parity
+    if ext:
+        line["extensions"] = ext
     if use_prop and prop_psnr:
         order = ["%dx%d seed %d" % (fp[0], fp[1], s) for fp in FOOTPRINTS for s in seeds]
         for key, name in ((same, "psnr"), ("ref", "psnr_vs_ref"), ("fixed", "psnr_vs_fixed")):

@@ -65,6 +65,20 @@ typedef struct astcb200_config {
  * Partitionings then come from the k-means mismatch order and the error estimate as
  * designed; decoded quality rises by several dB on most images. */
 #define ASTCB200_FLAG_FIXED_SEMANTICS 4u
+/* Encodings the reference never emits (no counterpart in it; both off by default), applied
+ * to every block after the search:
+ *   VOID_EXTENT: a block whose texels are all one colour is written as an LDR void-extent
+ *     block (the colour as 16-bit UNORM, no extent); it decodes to the same texels.
+ *   DUAL_PLANE: single-partition dual-plane encodings are tried (each colour channel as the
+ *     second plane, every dual-plane block mode whose weight grid the search uses, RGB or
+ *     RGBA direct endpoints at the finest colour quantisation that fits) and the best one
+ *     replaces the search's block when its decoded error is lower.  Errors are those of the
+ *     decoded 8-bit texels, weighted R 0.675, G 1.3275, B 0.2475, A 1.
+ * astcb200_encode_symbolic describes such blocks in the reference's record with two of its
+ * padding words: [6] = 1 + the second plane's channel, [7] = 1 for void extent (colour in
+ * packed_color_values[0..3]); the second plane's weights are quantized_weights[32..]. */
+#define ASTCB200_FLAG_VOID_EXTENT 8u
+#define ASTCB200_FLAG_DUAL_PLANE 16u
 
 typedef struct astcb200_stats {
     double ms_wall;       /* host time of the call */
