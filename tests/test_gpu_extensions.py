@@ -78,7 +78,7 @@ def test_void_extent_only():
     assert (sym[:, 7] > 0).any() and not (sym[:, 6] > 0).any()
 
 
-@pytest.mark.parametrize("bx,by,topn,iters,fb", [(4, 4, 8, 6, 6), (6, 6, 4, 6, 3)])
+@pytest.mark.parametrize("bx,by,topn,iters,fb", [(4, 4, 8, 6, 6), (6, 6, 3, 6, 3)])
 def test_extensions_after_the_proposal_search(bx, by, topn, iters, fb):
     """The extensions follow the proposal search too: proposal-search blocks equal the FIXED
     oracle restricted to the GPU's selection with the extensions, the others its full search."""
