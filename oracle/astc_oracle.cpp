@@ -2062,16 +2062,71 @@ int32_t infill_int(const Footprint& f, const DecInfo& di, const uint32_t* qw, in
     return (s + 8) >> 4;
 }
 
+// LDR endpoint decoding of the ASTC specification ("LDR Endpoint Decoding": bit transfer,
+// blue contraction, clamping) for the endpoint modes the encoder emits; 0..255 values.
+void spec_endpoints(uint32_t cem, const uint32_t* v, int32_t* e0, int32_t* e1) {
+    auto bts = [](int32_t& a, int32_t& b) {  // bit_transfer_signed(a, b)
+        b = (b >> 1) | (a & 0x80);
+        a = (a >> 1) & 0x3F;
+        if (a & 0x20) a -= 0x40;
+    };
+    auto clamp255 = [](int32_t x) { return std::min(255, std::max(0, x)); };
+    auto set = [](int32_t* e, int32_t r, int32_t g, int32_t b, int32_t a) { e[0] = r; e[1] = g; e[2] = b; e[3] = a; };
+    int32_t x[8];
+    for (int i = 0; i < 8; i++) x[i] = (int32_t)v[i];
+    switch (cem) {
+        case FMT_LUMINANCE: default: set(e0, x[0], x[0], x[0], 255); set(e1, x[1], x[1], x[1], 255); break;
+        case FMT_LUMINANCE_DELTA: {
+            const int32_t l0 = (x[0] >> 2) | (x[1] & 0xC0), l1 = std::min(l0 + (x[1] & 0x3F), 255);
+            set(e0, l0, l0, l0, 255); set(e1, l1, l1, l1, 255); break;
+        }
+        case FMT_LUMINANCE_ALPHA: set(e0, x[0], x[0], x[0], x[2]); set(e1, x[1], x[1], x[1], x[3]); break;
+        case FMT_LUMINANCE_ALPHA_DELTA: {
+            bts(x[1], x[0]); bts(x[3], x[2]);
+            set(e0, clamp255(x[0]), clamp255(x[0]), clamp255(x[0]), clamp255(x[2]));
+            const int32_t l = clamp255(x[0] + x[1]), a = clamp255(x[2] + x[3]);
+            set(e1, l, l, l, a); break;
+        }
+        case FMT_RGB_SCALE: case FMT_RGB_SCALE_ALPHA: {
+            const int32_t a0 = cem == FMT_RGB_SCALE ? 255 : x[4], a1 = cem == FMT_RGB_SCALE ? 255 : x[5];
+            set(e0, (x[0] * x[3]) >> 8, (x[1] * x[3]) >> 8, (x[2] * x[3]) >> 8, a0);
+            set(e1, x[0], x[1], x[2], a1); break;
+        }
+        case FMT_RGB: case FMT_RGBA: {
+            const int32_t a0 = cem == FMT_RGB ? 255 : x[6], a1 = cem == FMT_RGB ? 255 : x[7];
+            if (x[1] + x[3] + x[5] >= x[0] + x[2] + x[4]) { set(e0, x[0], x[2], x[4], a0); set(e1, x[1], x[3], x[5], a1); }
+            else {
+                set(e0, (x[1] + x[5]) >> 1, (x[3] + x[5]) >> 1, x[5], a1);
+                set(e1, (x[0] + x[4]) >> 1, (x[2] + x[4]) >> 1, x[4], a0);
+            }
+            break;
+        }
+        case FMT_RGB_DELTA: case FMT_RGBA_DELTA: {
+            bts(x[1], x[0]); bts(x[3], x[2]); bts(x[5], x[4]);
+            int32_t b3 = 0, a3 = 255;
+            if (cem == FMT_RGBA_DELTA) { bts(x[7], x[6]); b3 = x[7]; a3 = x[6]; }
+            int32_t c0[4] = {x[0], x[2], x[4], a3}, c1[4] = {x[0] + x[1], x[2] + x[3], x[4] + x[5], a3 + b3};
+            if (x[1] + x[3] + x[5] < 0) {
+                const int32_t t0[4] = {(c1[0] + c1[2]) >> 1, (c1[1] + c1[2]) >> 1, c1[2], c1[3]};
+                const int32_t t1[4] = {(c0[0] + c0[2]) >> 1, (c0[1] + c0[2]) >> 1, c0[2], c0[3]};
+                for (int k = 0; k < 4; k++) { c0[k] = t0[k]; c1[k] = t1[k]; }
+            }
+            for (int k = 0; k < 4; k++) { e0[k] = clamp255(c0[k]); e1[k] = clamp255(c1[k]); }
+            break;
+        }
+    }
+}
+
 // Exact decoded error of a single-plane symbolic block (words) against 8-bit texels c8.
 int64_t exact_error_single(const Footprint& f, const uint32_t* s, const uint8_t (*c8)[4]) {
     const BlockMode& bm = f.bms[f.bm_index[s[1] & 2047]];
     const DecInfo& di = f.dis[bm.dm];
     const int P = (int)s[2];
-    Cand c; std::memset(&c, 0, sizeof(c));
-    for (int i = 0; i < 4; i++) c.ffmt[i] = s[8 + i];
-    for (int i = 0; i < 32; i++) c.packed[i] = s[12 + i];
     int32_t e0[4][4], e1[4][4];
-    pass15(P, c, e0, e1);
+    for (int p = 0; p < P; p++) {
+        spec_endpoints(s[8 + p], &s[12 + p * 8], e0[p], e1[p]);
+        for (int k = 0; k < 4; k++) { e0[p][k] *= 257; e1[p][k] *= 257; }
+    }
     const PartInfo* pi = P > 1 ? &f.pinfo[(P - 2) * 1024 + f.packed_index[P - 2][s[3]]] : nullptr;
     int64_t err = 0;
     for (int t = 0; t < f.T; t++) {
