@@ -336,14 +336,23 @@ __host__ __device__ inline int refine_pbs(int T, int topn) {
     return by_threads < by_smem ? by_threads : (by_smem > 16 ? by_smem : 16);
 }
 
-// Per-thread candidate state in shared memory (41 words: an odd stride, so a
-// warp's threads hit distinct banks).  Endpoints live in per-thread local arrays.
+// A candidate's state in shared memory, kept at the candidate's staging position for all
+// iterations whichever thread runs it (73 words: an odd stride, so distinct candidates of a
+// warp mostly hit distinct banks).
 struct CandSmem {
     uint16_t u0[4][4], u1[4][4];  // unpacked endpoints x257 (0..65535)
     uint8_t qw[64];
     uint8_t packed[32];
-    uint32_t pad;
+    float ep[4][8];               // per partition: the least-squares endpoints ep0 (xyzw), ep1 (xyzw)
+    uint32_t item;                // partitioned block of this staging position (lb + 1 | slot << 27), 0 if none
 };
+static_assert(sizeof(CandSmem) == 292, "odd word stride");
+__device__ __forceinline__ float4 ld_ep(const float* e) { return make_float4(e[0], e[1], e[2], e[3]); }
+__device__ __forceinline__ void st_ep(float* e, float4 v) { e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w; }
+__device__ __forceinline__ uint4 ld_u4(const uint8_t* p) {  // 4-byte aligned shared memory
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(p);
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
 
 
 struct RTabs {
@@ -395,9 +404,16 @@ template <> struct TexelRow<false> {
     __device__ __forceinline__ float4 operator[](int t) const { return c[t]; }
 };
 
+// One refinement iteration (passes 13-17) of candidate k of a partitioned block, its
+// state in cs; iteration 0 first loads the front's initial state.  Returns whether pass16
+// moved a weight: a pass16 that moved none leaves a fixed point, where the next iteration's
+// pass13 recomputes the same endpoints from the same weights (channels whose system is
+// degenerate keep the previous values, which are these), so packing, unpacking, realignment
+// and the final error repeat exactly and can never lower the error: stopping there gives
+// the result of running the remaining iterations.
 template <class Row>
-__device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const int P, int k, const Row px, const uint8_t* tp,
-                                 CandSmem& cs, Snap* snap) {
+__device__ bool refine_step(const KernelArgs& a, const PBRec& rec, const int P, int k, const Row px, const uint8_t* tp,
+                            CandSmem& cs, Snap* snap, const int it) {
     const RTabs tb{a.tables, &a.L};
     const int T = a.L.T;
     const CandInit& ci = rec.c[k];
@@ -407,12 +423,16 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
     const float4 cw = chan_w();
     const float lsw = (cw.x + cw.y) + cw.z;
     const Packer pk{a.tables + a.L.off_cu2u};
-    float4 ep0[4], ep1[4], rgbs[4];
+    float4 rgbs[4];
     uint8_t packed_mod[32];
+    if (it == 0) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) { ep0[q] = rec.ep0[q]; ep1[q] = rec.ep1[q]; }
-    for (int w = 0; w < 64; w++) cs.qw[w] = ci.qw[w];
-    float top_err = ERR_DEFAULT;
+        for (int q = 0; q < 4; q++) { st_ep(cs.ep[q], rec.ep0[q]); st_ep(cs.ep[q] + 4, rec.ep1[q]); }
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(ci.qw);  // 8-byte aligned in PBRec
+        uint32_t* dst = reinterpret_cast<uint32_t*>(cs.qw);
+#pragma unroll
+        for (int w = 0; w < 16; w++) dst[w] = src[w];
+    }
     uint32_t ffmt[4] = {0, 0, 0, 0}, matched = 0, final_q = ci.ql;
     // infilled weights are recomputed where read: caching them per thread in shared memory
     // costs more resident CTAs than the recomputation
@@ -433,183 +453,173 @@ __device__ void refine_candidate(const KernelArgs& a, const PBRec& rec, const in
             d = vmin(make_float4(fabsf(d.x), fabsf(d.y), fabsf(d.z), fabsf(d.w)), mk(1e15f));
             total = total + fminf(dot4(d * d, cw), ERR_DEFAULT);
         }
-        if (total < top_err) {
-            top_err = total;
-            snap->err = total; snap->bm = ci.bm; snap->final_q = (uint8_t)final_q; snap->matched = (uint8_t)matched;
+        if (total < snap->err) {  // the snapshot's error is the best so far (ERR_DEFAULT at first)
+            uint4* d = reinterpret_cast<uint4*>(snap);  // 16-byte aligned: 112-byte records
+            d[0] = make_uint4(__float_as_uint(total), (uint32_t)ci.bm | final_q << 16 | matched << 24,
+                              ffmt[0] | ffmt[1] << 8 | ffmt[2] << 16 | ffmt[3] << 24, 0u);
+            d[1] = ld_u4(cs.packed); d[2] = ld_u4(cs.packed + 16);
 #pragma unroll
-            for (int q = 0; q < 4; q++) snap->ffmt[q] = (uint8_t)ffmt[q];
-            for (int i = 0; i < 32; i++) snap->packed[i] = cs.packed[i];
-            for (int i = 0; i < 64; i++) snap->qw[i] = cs.qw[i];
+            for (int i = 0; i < 4; i++) d[3 + i] = ld_u4(cs.qw + 16 * i);
         }
     };
 
-    const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
-    for (int it = 0; it < iters; it++) {
-        // ---------------- pass13: least-squares endpoints from the current weights
+    // ---------------- pass13: least-squares endpoints from the current weights
+#pragma unroll 1
+    for (int q = 0; q < P; q++) {
+        const float ps = P == 1 ? (float)T : (float)tb.part_count(P, rec.entry, q);
+        const float4 rsum = (rec.avg[q] * ps) * cw;
+        const float4 rws = vmax(cw * ps, mk(1e-17f));
+        float4 sv = rsum / rws; sv.w = 0.0f;
+        const float4 sdir = normalize4(sv);
+        float wmin = 1.0f, wmax = 0.0f, ls = 0.0f, ms = 0.0f, rs = 0.0f, smin = 1e10f, smax = 0.0f, sv0 = 0.0f, sv1 = 0.0f;
+        float4 cx = mk(0.0f), cy = mk(0.0f);
+        for (int t = 0; t < T; t++) {
+            if (tp[t] != q) continue;
+            const float4 rgba = px[t];
+            const float w = UW(t);
+            if (w < wmin) wmin = w;
+            if (w > wmax) wmax = w;
+            const float sc = dot3(rgba, sdir);
+            if (sc < smin) smin = sc;
+            if (sc > smax) smax = sc;
+            const float om = 1.0f - w;
+            ls = ls + om * om; ms = ms + om * w; rs = rs + w * w;
+            const float4 cyc = rgba * w;
+            cy = cy + cyc;
+            cx = cx + (rgba - cyc);
+            sv0 = sv0 + (om * sc) * lsw;
+            sv1 = sv1 + (w * sc) * lsw;
+        }
+        const float4 colx = cx * cw, coly = cy * cw;
+        const float4 lv = mk(ls) * cw, mv = mk(ms) * cw, rv = mk(rs) * cw;
+        const float lx = ls * lsw, my = ms * lsw, rz = rs * lsw;
+        const float scalediv = clampf(smin / fmaxf(smax, 1e-10f), 0.0f, 1.0f);
+        const float4 sds = sdir * smax;
+        rgbs[q] = make_float4(sds.x, sds.y, sds.z, scalediv);
+        float4 e0 = ld_ep(cs.ep[q]), e1 = ld_ep(cs.ep[q] + 4);
+        if (wmin >= wmax * 0.999f) {
+            const float4 ac = (colx + coly) / vmax(cw * ps, mk(1e-17f));
+            if (ac.x == ac.x) { e0.x = ac.x; e1.x = ac.x; }
+            if (ac.y == ac.y) { e0.y = ac.y; e1.y = ac.y; }
+            if (ac.z == ac.z) { e0.z = ac.z; e1.z = ac.z; }
+            if (ac.w == ac.w) { e0.w = ac.w; e1.w = ac.w; }
+            rgbs[q] = make_float4(sds.x, sds.y, sds.z, 1.0f);
+        } else {
+            const float4 det = (lv * rv) - (mv * mv);
+            const float4 rdet = mk(1.0f) / det;
+            const float lsdet = (lx * rz) - (my * my), lsrdet = 1.0f / lsdet;
+            const float4 mss = ((lv * lv) + mk(2.0f) * (mv * mv)) + (rv * rv);
+            const float lsmss = ((lx * lx) + 2.0f * (my * my)) + (rz * rz);
+            const float4 ne0 = ((rv * colx) - (mv * coly)) * rdet;
+            const float4 ne1 = ((lv * coly) - (mv * colx)) * rdet;
+            if (fabsf(det.x) > (mss.x * 1e-4f) && ne0.x == ne0.x && ne1.x == ne1.x) { e0.x = ne0.x; e1.x = ne1.x; }
+            if (fabsf(det.y) > (mss.y * 1e-4f) && ne0.y == ne0.y && ne1.y == ne1.y) { e0.y = ne0.y; e1.y = ne1.y; }
+            if (fabsf(det.z) > (mss.z * 1e-4f) && ne0.z == ne0.z && ne1.z == ne1.z) { e0.z = ne0.z; e1.z = ne1.z; }
+            if (fabsf(det.w) > (mss.w * 1e-4f) && ne0.w == ne0.w && ne1.w == ne1.w) { e0.w = ne0.w; e1.w = ne1.w; }
+            const float se0 = ((rz * sv0) - (my * sv1)) * lsrdet;
+            const float se1 = ((lx * sv1) - (my * sv0)) * lsrdet;
+            if ((fabsf(lsdet) > (lsmss * 1e-4f)) && se0 == se0 && se1 == se1 && se0 < se1) {
+                const float4 sdsm = sdir * se1;
+                rgbs[q] = make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1);
+            }
+        }
+        st_ep(cs.ep[q], e0); st_ep(cs.ep[q] + 4, e1);
+    }
+    // ---------------- pass14: pack at the trial quant level, then the "mod" level
+    {
+        bool all_same = ci.ql != ci.qlm;
+        uint32_t fn[4] = {0, 0, 0, 0}, vals[8];
+        for (int i = 0; i < 32; i++) cs.packed[i] = 0;
 #pragma unroll 1
         for (int q = 0; q < P; q++) {
-            const float ps = P == 1 ? (float)T : (float)tb.part_count(P, rec.entry, q);
-            const float4 rsum = (rec.avg[q] * ps) * cw;
-            const float4 rws = vmax(cw * ps, mk(1e-17f));
-            float4 sv = rsum / rws; sv.w = 0.0f;
-            const float4 sdir = normalize4(sv);
-            float wmin = 1.0f, wmax = 0.0f, ls = 0.0f, ms = 0.0f, rs = 0.0f, smin = 1e10f, smax = 0.0f, sv0 = 0.0f, sv1 = 0.0f;
-            float4 cx = mk(0.0f), cy = mk(0.0f);
-            for (int t = 0; t < T; t++) {
-                if (tp[t] != q) continue;
-                const float4 rgba = px[t];
-                const float w = UW(t);
-                if (w < wmin) wmin = w;
-                if (w > wmax) wmax = w;
-                const float sc = dot3(rgba, sdir);
-                if (sc < smin) smin = sc;
-                if (sc > smax) smax = sc;
-                const float om = 1.0f - w;
-                ls = ls + om * om; ms = ms + om * w; rs = rs + w * w;
-                const float4 cyc = rgba * w;
-                cy = cy + cyc;
-                cx = cx + (rgba - cyc);
-                sv0 = sv0 + (om * sc) * lsw;
-                sv1 = sv1 + (w * sc) * lsw;
-            }
-            const float4 colx = cx * cw, coly = cy * cw;
-            const float4 lv = mk(ls) * cw, mv = mk(ms) * cw, rv = mk(rs) * cw;
-            const float lx = ls * lsw, my = ms * lsw, rz = rs * lsw;
-            const float scalediv = clampf(smin / fmaxf(smax, 1e-10f), 0.0f, 1.0f);
-            const float4 sds = sdir * smax;
-            rgbs[q] = make_float4(sds.x, sds.y, sds.z, scalediv);
-            if (wmin >= wmax * 0.999f) {
-                const float4 ac = (colx + coly) / vmax(cw * ps, mk(1e-17f));
-                float4 e0 = ep0[q], e1 = ep1[q];
-                if (ac.x == ac.x) { e0.x = ac.x; e1.x = ac.x; }
-                if (ac.y == ac.y) { e0.y = ac.y; e1.y = ac.y; }
-                if (ac.z == ac.z) { e0.z = ac.z; e1.z = ac.z; }
-                if (ac.w == ac.w) { e0.w = ac.w; e1.w = ac.w; }
-                ep0[q] = e0; ep1[q] = e1;
-                rgbs[q] = make_float4(sds.x, sds.y, sds.z, 1.0f);
-            } else {
-                const float4 det = (lv * rv) - (mv * mv);
-                const float4 rdet = mk(1.0f) / det;
-                const float lsdet = (lx * rz) - (my * my), lsrdet = 1.0f / lsdet;
-                const float4 mss = ((lv * lv) + mk(2.0f) * (mv * mv)) + (rv * rv);
-                const float lsmss = ((lx * lx) + 2.0f * (my * my)) + (rz * rz);
-                const float4 ne0 = ((rv * colx) - (mv * coly)) * rdet;
-                const float4 ne1 = ((lv * coly) - (mv * colx)) * rdet;
-                float4 e0 = ep0[q], e1 = ep1[q];
-                if (fabsf(det.x) > (mss.x * 1e-4f) && ne0.x == ne0.x && ne1.x == ne1.x) { e0.x = ne0.x; e1.x = ne1.x; }
-                if (fabsf(det.y) > (mss.y * 1e-4f) && ne0.y == ne0.y && ne1.y == ne1.y) { e0.y = ne0.y; e1.y = ne1.y; }
-                if (fabsf(det.z) > (mss.z * 1e-4f) && ne0.z == ne0.z && ne1.z == ne1.z) { e0.z = ne0.z; e1.z = ne1.z; }
-                if (fabsf(det.w) > (mss.w * 1e-4f) && ne0.w == ne0.w && ne1.w == ne1.w) { e0.w = ne0.w; e1.w = ne1.w; }
-                ep0[q] = e0; ep1[q] = e1;
-                const float se0 = ((rz * sv0) - (my * sv1)) * lsrdet;
-                const float se1 = ((lx * sv1) - (my * sv0)) * lsrdet;
-                if ((fabsf(lsdet) > (lsmss * 1e-4f)) && se0 == se0 && se1 == se1 && se0 < se1) {
-                    const float4 sdsm = sdir * se1;
-                    rgbs[q] = make_float4(sdsm.x, sdsm.y, sdsm.z, se0 / se1);
-                }
-            }
+            const uint32_t f = pk.pack(ld_ep(cs.ep[q]), ld_ep(cs.ep[q] + 4), rgbs[q], ci.fmt[q], ci.ql, vals);
+            fn[0] = q == 0 ? f : fn[0]; fn[1] = q == 1 ? f : fn[1]; fn[2] = q == 2 ? f : fn[2]; fn[3] = q == 3 ? f : fn[3];
+#pragma unroll
+            for (int i = 0; i < 8; i++) cs.packed[q * 8 + i] = (uint8_t)vals[i];
+            if (q > 0) all_same = all_same && f == fn[0];
         }
-        // ---------------- pass14: pack at the trial quant level, then the "mod" level
-        {
-            bool all_same = ci.ql != ci.qlm;
-            uint32_t fn[4] = {0, 0, 0, 0}, vals[8];
-            for (int i = 0; i < 32; i++) cs.packed[i] = 0;
+        bool m = false;
+        if (P >= 2 && all_same) {
+            uint32_t fm[4] = {0, 0, 0, 0};
+            uint8_t* vm = packed_mod;
+            bool same_mod = true;
 #pragma unroll 1
             for (int q = 0; q < P; q++) {
-                const uint32_t f = pk.pack(ep0[q], ep1[q], rgbs[q], ci.fmt[q], ci.ql, vals);
-                fn[0] = q == 0 ? f : fn[0]; fn[1] = q == 1 ? f : fn[1]; fn[2] = q == 2 ? f : fn[2]; fn[3] = q == 3 ? f : fn[3];
+                const uint32_t f = pk.pack(ld_ep(cs.ep[q]), ld_ep(cs.ep[q] + 4), rgbs[q], ci.fmt[q], ci.qlm, vals);
+                fm[0] = q == 0 ? f : fm[0]; fm[1] = q == 1 ? f : fm[1]; fm[2] = q == 2 ? f : fm[2]; fm[3] = q == 3 ? f : fm[3];
 #pragma unroll
-                for (int i = 0; i < 8; i++) cs.packed[q * 8 + i] = (uint8_t)vals[i];
-                if (q > 0) all_same = all_same && f == fn[0];
+                for (int i = 0; i < 8; i++) vm[q * 8 + i] = (uint8_t)vals[i];
+                if (q > 0 && f != fm[0]) { same_mod = false; break; }
             }
-            bool m = false;
-            if (P >= 2 && all_same) {
-                uint32_t fm[4] = {0, 0, 0, 0};
-                uint8_t* vm = packed_mod;
-                bool same_mod = true;
-#pragma unroll 1
-                for (int q = 0; q < P; q++) {
-                    const uint32_t f = pk.pack(ep0[q], ep1[q], rgbs[q], ci.fmt[q], ci.qlm, vals);
-                    fm[0] = q == 0 ? f : fm[0]; fm[1] = q == 1 ? f : fm[1]; fm[2] = q == 2 ? f : fm[2]; fm[3] = q == 3 ? f : fm[3];
+            if (same_mod) {
+                m = true;
 #pragma unroll
-                    for (int i = 0; i < 8; i++) vm[q * 8 + i] = (uint8_t)vals[i];
-                    if (q > 0 && f != fm[0]) { same_mod = false; break; }
-                }
-                if (same_mod) {
-                    m = true;
-#pragma unroll
-                    for (int q = 0; q < 4; q++) fn[q] = fm[q];
-                    for (int i = 0; i < 32; i++) cs.packed[i] = i < P * 8 ? vm[i] : 0;
-                }
+                for (int q = 0; q < 4; q++) fn[q] = fm[q];
+                for (int i = 0; i < 32; i++) cs.packed[i] = i < P * 8 ? vm[i] : 0;
             }
-            matched = m ? 1 : 0;
-            final_q = m ? ci.qlm : ci.ql;
-#pragma unroll
-            for (int q = 0; q < 4; q++) ffmt[q] = fn[q];
         }
-        // ---------------- pass15
+        matched = m ? 1 : 0;
+        final_q = m ? ci.qlm : ci.ql;
+#pragma unroll
+        for (int q = 0; q < 4; q++) ffmt[q] = fn[q];
+    }
+    // ---------------- pass15
 #pragma unroll 1
-        for (int q = 0; q < P; q++) unpack_endpoints(ffmt[q], cs.packed + q * 8, cs.u0[q], cs.u1[q]);
-        if (it == 0) final_error();
-        // ---------------- pass16: move each weight one quant step if that lowers the error
-        bool moved = false;
-        if (direct) {
-            for (int t = 0; t < T; t++) {
+    for (int q = 0; q < P; q++) unpack_endpoints(ffmt[q], cs.packed + q * 8, cs.u0[q], cs.u1[q]);
+    if (it == 0) final_error();
+    // ---------------- pass16: move each weight one quant step if that lowers the error
+    bool moved = false;
+    if (direct) {
+        for (int t = 0; t < T; t++) {
+            const int p = tp[t];
+            const int32_t uqw = cs.qw[t];
+            const uint32_t pn = tb.prev_next(bm.quant, uqw);
+            const int32_t dn = pn & 0xFF, up = (pn >> 8) & 0xFF;
+            const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
+            const float4 offs = make_float4((float)((int32_t)cs.u1[p][0] - (int32_t)cs.u0[p][0]), (float)((int32_t)cs.u1[p][1] - (int32_t)cs.u0[p][1]),
+                                            (float)((int32_t)cs.u1[p][2] - (int32_t)cs.u0[p][2]), (float)((int32_t)cs.u1[p][3] - (int32_t)cs.u0[p][3])) * (1.0f / 64.0f);
+            const float4 cd = (base + offs * (float)uqw) - px[t];
+            const float4 cdd = cd + offs * (float)(dn - uqw), cdu = cd + offs * (float)(up - uqw);
+            const float eb = dot4(cd * cd, cw), ed = dot4(cdd * cdd, cw), eu = dot4(cdu * cdu, cw);
+            if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[t] = (uint8_t)up; moved |= up != uqw; }
+            else if ((ed < eb) && (uqw > 0)) { cs.qw[t] = (uint8_t)dn; moved |= dn != uqw; }
+        }
+    } else {
+        for (int we = 0; we < dmi.W; we++) {
+            const int32_t uqw = cs.qw[we];
+            const uint32_t pn = tb.prev_next(bm.quant, uqw);
+            const float dn = (float)(pn & 0xFF), up = (float)((pn >> 8) & 0xFF), ub = (float)uqw;
+            const float ddn = dn - ub, dup = up - ub;
+            float4 ebv = mk(0.0f), edv = mk(0.0f), euv = mk(0.0f);
+            const int nt = tb.wt_count(bm.dm, we), wbase = dmi.wt_base + tb.wt_start(bm.dm, we);
+            for (int te = 0; te < nt; te++) {
+                // the weight's own contribution to texel t is the w2t entry's
+                // (each (texel, weight) pair appears once in both maps)
+                const uint32_t we2 = tb.w2t(wbase + te);
+                const int t = we2 & 0xFF;
+                const float twb = (float)(we2 >> 8) * (1.0f / 16.0f);
+                const uint64_t e4 = tb.tw4(bm.dm, t);
+                float wb = 0.0f;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
+                    wb = wb + (float)cs.qw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f));
+                }
                 const int p = tp[t];
-                const int32_t uqw = cs.qw[t];
-                const uint32_t pn = tb.prev_next(bm.quant, uqw);
-                const int32_t dn = pn & 0xFF, up = (pn >> 8) & 0xFF;
                 const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
                 const float4 offs = make_float4((float)((int32_t)cs.u1[p][0] - (int32_t)cs.u0[p][0]), (float)((int32_t)cs.u1[p][1] - (int32_t)cs.u0[p][1]),
                                                 (float)((int32_t)cs.u1[p][2] - (int32_t)cs.u0[p][2]), (float)((int32_t)cs.u1[p][3] - (int32_t)cs.u0[p][3])) * (1.0f / 64.0f);
-                const float4 cd = (base + offs * (float)uqw) - px[t];
-                const float4 cdd = cd + offs * (float)(dn - uqw), cdu = cd + offs * (float)(up - uqw);
-                const float eb = dot4(cd * cd, cw), ed = dot4(cdd * cdd, cw), eu = dot4(cdu * cdu, cw);
-                if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[t] = (uint8_t)up; moved |= up != uqw; }
-                else if ((ed < eb) && (uqw > 0)) { cs.qw[t] = (uint8_t)dn; moved |= dn != uqw; }
+                const float4 cd = (base + offs * wb) - px[t];
+                const float4 cdd = cd + offs * (ddn * twb), cdu = cd + offs * (dup * twb);
+                ebv = ebv + cd * cd; edv = edv + cdd * cdd; euv = euv + cdu * cdu;
             }
-        } else {
-            for (int we = 0; we < dmi.W; we++) {
-                const int32_t uqw = cs.qw[we];
-                const uint32_t pn = tb.prev_next(bm.quant, uqw);
-                const float dn = (float)(pn & 0xFF), up = (float)((pn >> 8) & 0xFF), ub = (float)uqw;
-                const float ddn = dn - ub, dup = up - ub;
-                float4 ebv = mk(0.0f), edv = mk(0.0f), euv = mk(0.0f);
-                const int nt = tb.wt_count(bm.dm, we), wbase = dmi.wt_base + tb.wt_start(bm.dm, we);
-                for (int te = 0; te < nt; te++) {
-                    // the weight's own contribution to texel t is the w2t entry's
-                    // (each (texel, weight) pair appears once in both maps)
-                    const uint32_t we2 = tb.w2t(wbase + te);
-                    const int t = we2 & 0xFF;
-                    const float twb = (float)(we2 >> 8) * (1.0f / 16.0f);
-                    const uint64_t e4 = tb.tw4(bm.dm, t);
-                    float wb = 0.0f;
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const uint32_t e = (uint32_t)(e4 >> (16 * j)) & 0xFFFF;
-                        wb = wb + (float)cs.qw[e & 0xFF] * ((float)(e >> 8) * (1.0f / 16.0f));
-                    }
-                    const int p = tp[t];
-                    const float4 base = make_float4((float)cs.u0[p][0], (float)cs.u0[p][1], (float)cs.u0[p][2], (float)cs.u0[p][3]);
-                    const float4 offs = make_float4((float)((int32_t)cs.u1[p][0] - (int32_t)cs.u0[p][0]), (float)((int32_t)cs.u1[p][1] - (int32_t)cs.u0[p][1]),
-                                                    (float)((int32_t)cs.u1[p][2] - (int32_t)cs.u0[p][2]), (float)((int32_t)cs.u1[p][3] - (int32_t)cs.u0[p][3])) * (1.0f / 64.0f);
-                    const float4 cd = (base + offs * wb) - px[t];
-                    const float4 cdd = cd + offs * (ddn * twb), cdu = cd + offs * (dup * twb);
-                    ebv = ebv + cd * cd; edv = edv + cdd * cdd; euv = euv + cdu * cdu;
-                }
-                const float eb = dot4(ebv, cw), ed = dot4(edv, cw), eu = dot4(euv, cw);
-                if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[we] = (uint8_t)up; moved |= (int32_t)up != uqw; }
-                else if ((ed < eb) && (uqw > 0)) { cs.qw[we] = (uint8_t)dn; moved |= (int32_t)dn != uqw; }
-            }
+            const float eb = dot4(ebv, cw), ed = dot4(edv, cw), eu = dot4(euv, cw);
+            if ((eu < eb) && (eu < ed) && (uqw < 64)) { cs.qw[we] = (uint8_t)up; moved |= (int32_t)up != uqw; }
+            else if ((ed < eb) && (uqw > 0)) { cs.qw[we] = (uint8_t)dn; moved |= (int32_t)dn != uqw; }
         }
-        final_error();
-        // A pass16 that moved no weight leaves a fixed point: the next iteration's pass13
-        // recomputes the same endpoints from the same weights (channels whose system is
-        // degenerate keep the previous values, which are these), so packing, unpacking,
-        // realignment and the final error repeat exactly and can never lower the error.
-        // Stopping here gives the same result as running the remaining iterations.
-        if (!moved) break;
     }
+    final_error();
+    return moved;
 }
 
 // CPB: candidate threads per partitioned block (refine_cpb of the launch's top-N), a
@@ -628,29 +638,31 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
     Px* pxs = reinterpret_cast<Px*>(U8 ? smem + sizeof(CandSmem) * kRefineThreads + 256 * 4 : smem + sizeof(CandSmem) * kRefineThreads);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + pbs * T);
     int* keys = reinterpret_cast<int*>(tps + ((pbs * T + 15) & ~15));
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // Items: every slot of every block in slot-major order (consecutive CTAs hold
     // partitioned blocks of the same slot, hence the same partition count, so
     // co-resident warps run the same code), or the proposal pass's work list.
     const int nb = list_blocks(a);
     const int npb = a.pb_list ? pb_total(a) : nb * a.slots;
     const int ngroups = (npb + pbs - 1) / pbs;
+    const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
     __shared__ unsigned int refined[4];  // candidates refined by this CTA, by P (work counters)
+    __shared__ int live_in_warp[kRefineThreads / 32];
     if (tid < 4) refined[tid] = 0;
     if (U8)
         for (int v = tid; v < 256; v += kRefineThreads) lut[v] = ((float)v / 255.0f) * 65536.0f;  // as src_texel
     // (the first group's barrier below orders these writes before any read)
     for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-        int my_lb = -1, my_slot = 0;  // this thread's partitioned block in the staging order
         {
             const int pbl = tid / cpb, k = tid % cpb;
             const int li = grp * pbs + pbl;
             int key = 0x3FFFFF;  // empty slots sort last
+            uint32_t item = 0;
             if (pbl < pbs && li < npb) {
                 int slot, lb;
                 if (a.pb_list) pb_item(a, li, lb, slot);
                 else { slot = li / nb; lb = li % nb; }
-                my_lb = lb; my_slot = slot;
+                item = (uint32_t)(lb + 1) | ((uint32_t)slot << 27);
                 const PBRec& r = a.pbrec[lb * a.slots + slot];
                 if (k < (int)r.ncand) {
                     const int dm = reinterpret_cast<const DevBm*>(a.tables + a.L.off_bm)[r.c[k].bm].dm;
@@ -670,13 +682,13 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
                 }
             }
             keys[tid] = key * kRefineThreads + tid;  // unique keys: P, formats, decimation mode, then position
-            cs[tid].pad = (uint32_t)(my_lb + 1) | ((uint32_t)my_slot << 27);  // item of staging position tid
+            cs[tid].item = item;  // of staging position tid
         }
         __syncthreads();
         // Thread tid takes the candidate of rank tid in (partition count, endpoint formats,
         // decimation mode) order, so a warp's candidates mostly take the same packing path
         // and share loop bounds and table rows.
-        int mine = 0;
+        int cand = -1;  // staging position of the candidate this thread runs
         {
             const int kk = keys[tid];
             int rank = 0;
@@ -684,24 +696,55 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
             __syncthreads();
             keys[rank] = tid;
             __syncthreads();
-            mine = keys[tid];
-        }
-        const int pbl = mine / cpb, k = mine % cpb;
-        const uint32_t item = cs[pbl * cpb].pad;  // written by the threads that staged partitioned block pbl
-        __syncthreads();  // every thread has read the item words before the candidate state overwrites them
-        if (item != 0) {
-            const int lb = (int)(item & 0x07FFFFFFu) - 1, slot = (int)(item >> 27);
-            const int pb = lb * a.slots + slot;
-            const PBRec& rec = a.pbrec[pb];
-            Snap* snap = &a.snaps[(size_t)pb * kNumCand + k];
-            snap->err = ERR_DEFAULT;  // inert slot unless refined below
-            if (k < (int)rec.ncand) {
-                if constexpr (U8) refine_candidate(a, rec, (int)rec.P, k, TexelRow<true>{pxs + pbl * T, lut}, tps + pbl * T, cs[tid], snap);
-                else refine_candidate(a, rec, (int)rec.P, k, TexelRow<false>{pxs + pbl * T}, tps + pbl * T, cs[tid], snap);
-                if (a.work) atomicAdd(&refined[rec.P - 1], 1u);
+            const int mine = keys[tid];
+            const int pbl = mine / cpb, k = mine % cpb;
+            const uint32_t item = cs[pbl * cpb].item;
+            if (item != 0) {
+                const int lb = (int)(item & 0x07FFFFFFu) - 1, slot = (int)(item >> 27);
+                const size_t pbi = (size_t)lb * a.slots + slot;
+                a.snaps[pbi * kNumCand + k].err = ERR_DEFAULT;  // inert slot unless refined below
+                if (k < (int)a.pbrec[pbi].ncand) {
+                    cand = mine;
+                    if (a.work) atomicAdd(&refined[a.pbrec[pbi].P - 1], 1u);
+                }
             }
         }
-        __syncthreads();  // the next group reuses shared memory
+        // Iterations.  Candidates stop at different iterations (at a fixed point of pass16),
+        // so after every iteration the live candidates are gathered onto the lowest threads,
+        // in the same order: warps stay full while any work is left, and warps with none
+        // wait at the barrier without issuing.  The staged texels and each candidate's state
+        // stay where they are; only the candidate-to-thread map changes.
+        for (int it = 0; ; it++) {
+            const bool live = cand >= 0;
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
+            if (lane == 0) live_in_warp[warp] = __popc(bal);
+            __syncthreads();  // also: every thread has read keys[] before it is rewritten
+            int nlive = 0, before = 0;
+#pragma unroll
+            for (int w = 0; w < kRefineThreads / 32; w++) {
+                const int n = live_in_warp[w];
+                nlive += n;
+                before += w < warp ? n : 0;
+            }
+            if (nlive == 0) break;
+            if (live) keys[before + __popc(bal & ((1u << lane) - 1u))] = cand;
+            __syncthreads();
+            cand = tid < nlive ? keys[tid] : -1;
+            if (cand >= 0) {
+                const int pbl = cand / cpb, k = cand % cpb;
+                const uint32_t item = cs[pbl * cpb].item;
+                const int lb = (int)(item & 0x07FFFFFFu) - 1, slot = (int)(item >> 27);
+                const size_t pbi = (size_t)lb * a.slots + slot;
+                const PBRec& rec = a.pbrec[pbi];
+                Snap* snap = &a.snaps[pbi * kNumCand + k];
+                bool moved;
+                if constexpr (U8) moved = refine_step(a, rec, (int)rec.P, k, TexelRow<true>{pxs + pbl * T, lut}, tps + pbl * T, cs[cand], snap, it);
+                else moved = refine_step(a, rec, (int)rec.P, k, TexelRow<false>{pxs + pbl * T}, tps + pbl * T, cs[cand], snap, it);
+                if (!moved || it + 1 >= iters) cand = -1;
+            }
+            // (the next pass's first barrier orders this iteration's state writes before
+            // other threads read them; the counts and the map were read before its second)
+        }
     }
     if (a.work && tid < 4 && refined[tid]) atomicAdd(a.work + 6 + tid, (unsigned long long)refined[tid]);
 }
