@@ -511,23 +511,32 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
             hv[u] = c < S.nbm ? h[c] : 0.0f;
             if (c >= S.nbm) picked |= 1u << u;  // absent: never offered
         }
-        for (int k = 0; k < sel.kbm && k < S.nbm; k++) {
+        // The kbm best modes by (value descending, index ascending), one pick per round.  When
+        // kbm is above half the modes, the rounds pick the others instead, worst first (value
+        // ascending, index descending): the same set in fewer rounds.
+        const int kk = sel.kbm < S.nbm ? sel.kbm : S.nbm;
+        const bool worst = 2 * kk > S.nbm;
+        const int rounds = worst ? S.nbm - kk : kk;
+        for (int k = 0; k < rounds; k++) {
             uint32_t key = 0;
             int mine = -1;
             float mv = 0.0f;
 #pragma unroll
             for (int u = 0; u < 2 * kMaskWords; u++)
-                if (!((picked >> u) & 1) && (mine < 0 || hv[u] > mv)) { mine = u; mv = hv[u]; }
-            if (mine >= 0) key = okey(mv);
+                if (!((picked >> u) & 1) && (mine < 0 || (worst ? hv[u] <= mv : hv[u] > mv))) { mine = u; mv = hv[u]; }
+            if (mine >= 0) key = worst ? ~okey(mv) : okey(mv);
             const uint32_t best = __reduce_max_sync(kFull, key);
             if (best == 0u) break;
-            const uint32_t ci = __reduce_min_sync(kFull, key == best ? (uint32_t)(lane + 32 * mine) : 0xFFFFFFFFu);
-            if (mine >= 0 && (uint32_t)(lane + 32 * mine) == ci) picked |= 1u << mine;
+            const uint32_t idx = (uint32_t)(lane + 32 * mine);
+            const uint32_t ci = worst ? __reduce_max_sync(kFull, key == best ? idx : 0u)
+                                      : __reduce_min_sync(kFull, key == best ? idx : 0xFFFFFFFFu);
+            if (mine >= 0 && idx == ci) picked |= 1u << mine;
         }
         uint64_t word = 0;
 #pragma unroll
         for (int u = 0; u < 2 * kMaskWords; u++) {
-            const uint32_t chosen = __ballot_sync(kFull, ((picked >> u) & 1) && lane + 32 * u < S.nbm);
+            const bool valid = lane + 32 * u < S.nbm;
+            const uint32_t chosen = __ballot_sync(kFull, valid && (((picked >> u) & 1) != 0) != worst);
             if (lane == (u >> 1)) word |= (uint64_t)chosen << (32 * (u & 1));
         }
         if (lane < kMaskWords) mk[p * kMaskWords + lane] = word;
