@@ -99,7 +99,7 @@ int ensure_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, int slots) {
 
 void free_scratch(Scratch& sc) {
     cudaFree(sc.picks); cudaFree(sc.pbrec); cudaFree(sc.snaps);
-    cudaFree(sc.logits); cudaFree(sc.lists); cudaFree(sc.prop); cudaFree(sc.masks); cudaFree(sc.pbl); cudaFree(sc.full_err);
+    cudaFree(sc.logits); cudaFree(sc.lists); cudaFree(sc.prop); cudaFree(sc.masks); cudaFree(sc.pbl); cudaFree(sc.full_err); cudaFree(sc.tail);
     sc = Scratch();
 }
 

@@ -36,8 +36,14 @@ struct Scratch {
     PropPicks* prop = nullptr;
     uint64_t* masks = nullptr;
     uint32_t* pbl = nullptr;       // [4][blocks * kMaxProposals] partitioned-block work lists
-    size_t cap_logits = 0, cap_lists = 0, cap_prop = 0, cap_masks = 0, cap_pbl = 0, cap_ferr = 0;
+    uint4* tail = nullptr;         // refinement-tail entries (kTailWords words each)
+    size_t cap_logits = 0, cap_lists = 0, cap_prop = 0, cap_masks = 0, cap_pbl = 0, cap_ferr = 0, cap_tail = 0;
 };
+// Refinement-tail entries per block of a chunk (a CTA that finds the tail full finishes its
+// candidates itself), and the live candidates at or below which a refinement CTA hands
+// them to the tail.
+constexpr size_t kTailPerBlock = 4;
+constexpr int kSpillLive = 32;
 
 // A footprint's proposal network on the device.
 struct NetDev {

@@ -92,12 +92,22 @@ struct KernelArgs {
     int pb_stride;
     // Work counters (null: not counted): [0..3] partitioned blocks searched by the front,
     // by P; [4] decimation modes and [5] block modes it evaluated; [6..9] candidates
-    // refined, by P; [10..12] partition searches, P = 2..4.
+    // refined, by P; [10..12] partition searches, P = 2..4; [13] candidates the refinement
+    // handed to its tail pass.
     unsigned long long* work;
     int front_threads;        // threads per front CTA: 128 (0 selects it), 64 or 32
     int refine_iters;         // refinement iterations (0 selects the reference's 6)
     int fixed;                // 1: FIXED semantics (ASTCB200_FLAG_FIXED_SEMANTICS), 0: the reference's
+    // Refinement tail (null: off): once a refinement CTA has at most spill_live candidates
+    // left, it writes their state here (kTailWords uint4 each, up to tail_cap entries,
+    // *tail_count reserved so far) and takes its next group; k_refine_tail finishes them.
+    uint4* tail;
+    int* tail_count;
+    int tail_cap;
+    int spill_live;
 };
+constexpr int kTailWords = 13;        // uint4 words of one refinement-tail entry
+constexpr int kTailMaxTexels = 36;    // blocks of more texels are never handed to the tail
 constexpr int kWorkCounters = 16;
 
 // Launch grid caps for kernels that walk device-side lists (grid-stride loops).
@@ -189,6 +199,8 @@ cudaError_t configure_kernels(const TableLayout& L);
 cudaError_t launch_partition_search(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_front(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s);
+// Finishes the candidates k_refine handed to the tail (a.tail, a.tail_count).
+cudaError_t launch_refine_tail(const KernelArgs& a, cudaStream_t s);
 cudaError_t launch_select_pack(const KernelArgs& a, cudaStream_t s);
 // Optional encodings over the chunk's blocks after the search (flags: bit 0 void extent,
 // bit 1 dual plane); nothing is launched when neither is set.

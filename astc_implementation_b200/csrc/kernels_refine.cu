@@ -622,6 +622,23 @@ __device__ bool refine_step(const KernelArgs& a, const PBRec& rec, const int P, 
     return moved;
 }
 
+// A refinement-tail entry: the partitioned block (lb * slots + slot), the candidate, the
+// next iteration, then the state an iteration carries over (endpoints, weights; the best
+// result so far is in the candidate's snapshot already).
+__device__ __forceinline__ void write_tail(const KernelArgs& a, const CandSmem& c, uint32_t pbi, int k, int it, int pos) {
+    uint4* e = a.tail + (size_t)pos * kTailWords;
+    e[0] = make_uint4(pbi, (uint32_t)k | (uint32_t)it << 8, 0u, 0u);
+    const uint8_t* ep = reinterpret_cast<const uint8_t*>(c.ep);
+#pragma unroll
+    for (int i = 0; i < 8; i++) e[1 + i] = ld_u4(ep + 16 * i);
+#pragma unroll
+    for (int i = 0; i < 4; i++) e[9 + i] = ld_u4(c.qw + 16 * i);
+}
+__device__ __forceinline__ void st_u4(uint8_t* p, uint4 v) {  // 4-byte aligned shared memory
+    uint32_t* w = reinterpret_cast<uint32_t*>(p);
+    w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+}
+
 // CPB: candidate threads per partitioned block (refine_cpb of the launch's top-N), a
 // template parameter so that the full search's instance (8) keeps constant indexing.
 // U8: texels staged as RGBA8 (refine_u8).  Registers are capped for five resident CTAs
@@ -648,7 +665,9 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
     const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
     __shared__ unsigned int refined[4];  // candidates refined by this CTA, by P (work counters)
     __shared__ int live_in_warp[kRefineThreads / 32];
+    __shared__ int spill_base;
     if (tid < 4) refined[tid] = 0;
+    bool spill = a.tail != nullptr && T <= kTailMaxTexels;  // until the tail is found full
     if (U8)
         for (int v = tid; v < 256; v += kRefineThreads) lut[v] = ((float)v / 255.0f) * 65536.0f;  // as src_texel
     // (the first group's barrier below orders these writes before any read)
@@ -727,7 +746,32 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
                 before += w < warp ? n : 0;
             }
             if (nlive == 0) break;
-            if (live) keys[before + __popc(bal & ((1u << lane) - 1u))] = cand;
+            const int rank = before + __popc(bal & ((1u << lane) - 1u));
+            if (spill && it > 0 && nlive <= a.spill_live) {
+                // Few candidates left: hand them to the tail pass, which runs them densely, and
+                // take the next group instead of holding the CTA for them.  The item words are
+                // read before the barrier: after it, threads that are done stage the next group.
+                uint32_t pbi = 0;
+                if (live) {
+                    const uint32_t item = cs[(cand / cpb) * cpb].item;
+                    pbi = (uint32_t)((int)(item & 0x07FFFFFFu) - 1) * (uint32_t)a.slots + (item >> 27);
+                }
+                if (tid == 0) {
+                    spill_base = atomicAdd(a.tail_count, nlive);
+                    if (a.work) atomicAdd(a.work + 13, (unsigned long long)nlive);
+                }
+                __syncthreads();
+                const int sb = spill_base, pos = sb + rank;
+                if (sb + nlive <= a.tail_cap) {
+                    // (the next group's staging writes no candidate state: ep and qw are first
+                    // written by its iteration 0, after its barriers)
+                    if (live) write_tail(a, cs[cand], pbi, cand % cpb, it, pos);
+                    break;
+                }
+                if (live && pos < a.tail_cap) a.tail[(size_t)pos * kTailWords].x = 0xFFFFFFFFu;  // reserved, left empty
+                spill = false;  // the tail is full: finish here
+            }
+            if (live) keys[rank] = cand;
             __syncthreads();
             cand = tid < nlive ? keys[tid] : -1;
             if (cand >= 0) {
@@ -747,6 +791,83 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
         }
     }
     if (a.work && tid < 4 && refined[tid]) atomicAdd(a.work + 6 + tid, (unsigned long long)refined[tid]);
+}
+
+// The candidates k_refine handed over, one per thread with its own staged texels (RGBA8
+// through the table of src_texel's values, so every texel value is the same), iterated
+// with the same gathering of live candidates onto the lowest threads.
+constexpr int kTailCtas = 4;
+__global__ void __launch_bounds__(kRefineThreads, kTailCtas) k_refine_tail(const __grid_constant__ KernelArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int T = a.L.T;
+    CandSmem* cs = reinterpret_cast<CandSmem*>(smem);
+    float* lut = reinterpret_cast<float*>(smem + sizeof(CandSmem) * kRefineThreads);
+    uchar4* pxs = reinterpret_cast<uchar4*>(smem + sizeof(CandSmem) * kRefineThreads + 256 * 4);
+    uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefineThreads * T);
+    int* keys = reinterpret_cast<int*>(tps + ((kRefineThreads * T + 15) & ~15));
+    int* next_it = keys + kRefineThreads;                                  // by position
+    uint32_t* pbi_of = reinterpret_cast<uint32_t*>(next_it + kRefineThreads);  // by position
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int live_in_warp[kRefineThreads / 32];
+    for (int v = tid; v < 256; v += kRefineThreads) lut[v] = ((float)v / 255.0f) * 65536.0f;  // as src_texel
+    const int total = min(*a.tail_count, a.tail_cap);
+    const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
+    for (int b0 = blockIdx.x * kRefineThreads; b0 < total; b0 += gridDim.x * kRefineThreads) {
+        int cand = -1;
+        if (b0 + tid < total) {
+            const uint4* e = a.tail + (size_t)(b0 + tid) * kTailWords;
+            const uint4 h = e[0];
+            if (h.x != 0xFFFFFFFFu) {
+                const int lb = (int)(h.x / (uint32_t)a.slots);
+                const PBRec& r = a.pbrec[h.x];
+                const int P = (int)r.P;
+                const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
+                const BlockSrc src = block_src(a, chunk_block(a, lb));
+                for (int t = 0; t < T; t++) {
+                    pxs[tid * T + t] = src_rgba8(src, a.L.bx, t);
+                    tps[tid * T + t] = P > 1 ? prow[t] : 0;
+                }
+                uint8_t* ep = reinterpret_cast<uint8_t*>(cs[tid].ep);
+                for (int i = 0; i < 8; i++) st_u4(ep + 16 * i, e[1 + i]);
+                for (int i = 0; i < 4; i++) st_u4(cs[tid].qw + 16 * i, e[9 + i]);
+                cs[tid].item = h.y & 0xFF;  // the candidate
+                next_it[tid] = (int)((h.y >> 8) & 0xFF);
+                pbi_of[tid] = h.x;
+                cand = tid;
+            }
+        }
+        for (;;) {
+            const bool live = cand >= 0;
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
+            if (lane == 0) live_in_warp[warp] = __popc(bal);
+            __syncthreads();  // also orders the staging and every earlier state write
+            int nlive = 0, before = 0;
+#pragma unroll
+            for (int w = 0; w < kRefineThreads / 32; w++) {
+                const int n = live_in_warp[w];
+                nlive += n;
+                before += w < warp ? n : 0;
+            }
+            if (nlive == 0) break;
+            if (live) keys[before + __popc(bal & ((1u << lane) - 1u))] = cand;
+            __syncthreads();
+            cand = tid < nlive ? keys[tid] : -1;
+            if (cand >= 0) {
+                const uint32_t pbi = pbi_of[cand];
+                const int k = (int)cs[cand].item, it = next_it[cand];
+                const PBRec& rec = a.pbrec[pbi];
+                Snap* snap = &a.snaps[(size_t)pbi * kNumCand + k];
+                const bool moved = refine_step(a, rec, (int)rec.P, k, TexelRow<true>{pxs + cand * T, lut}, tps + cand * T, cs[cand], snap, it);
+                next_it[cand] = it + 1;
+                if (!moved || it + 1 >= iters) cand = -1;
+            }
+        }
+    }
+}
+
+size_t refine_tail_smem_bytes(int T) {
+    return sizeof(CandSmem) * kRefineThreads + 256 * 4 + (size_t)kRefineThreads * T * 4 +
+           (((size_t)kRefineThreads * T + 15) & ~(size_t)15) + kRefineThreads * 4 * 3;
 }
 
 // ------------------------------------------------------------ k_select_pack
@@ -1305,7 +1426,7 @@ cudaError_t configure_kernels(const TableLayout& L) {
     for (auto f : {k_refine<1, false>, k_refine<2, false>, k_refine<4, false>, k_refine<8, false>, k_refine<1, true>,
                    k_refine<2, true>, k_refine<4, true>, k_refine<8, true>})
         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m[2])) != cudaSuccess) return e;
-    return cudaSuccess;
+    return cudaFuncSetAttribute(k_refine_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)refine_tail_smem_bytes(kTailMaxTexels));
 }
 
 cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
@@ -1325,6 +1446,13 @@ cudaError_t launch_refine(const KernelArgs& a, cudaStream_t s) {
         else if (cpb == 4) k_refine<4, false><<<grid, kRefineThreads, smem, s>>>(a);
         else k_refine<8, false><<<grid, kRefineThreads, smem, s>>>(a);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refine_tail(const KernelArgs& a, cudaStream_t s) {
+    if (!a.tail || a.L.T > kTailMaxTexels) return cudaSuccess;
+    const int grid = std::min((a.tail_cap + kRefineThreads - 1) / kRefineThreads, 148 * kTailCtas);
+    k_refine_tail<<<std::max(grid, 1), kRefineThreads, refine_tail_smem_bytes(a.L.T), s>>>(a);
     return cudaGetLastError();
 }
 

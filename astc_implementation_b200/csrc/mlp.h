@@ -91,7 +91,8 @@ struct Select {
 // Output of the selection kernel for one chunk.
 struct Routes {
     int* counts;          // [0] pruned blocks, [1] full-search blocks, [2..5] partitioned blocks
-                          // of P = 1..4 in pb_list (zeroed before the launch)
+                          // of P = 1..4 in pb_list, [6] refinement-tail entries of the proposal
+                          // pass (zeroed before the launch)
     int* pruned;          // [chunk] global block indices taking the proposal search
     int* full;            // [chunk] global block indices taking the full search
     float* full_err;      // [chunk] error of a result already written for full[i] (3e38: none)
@@ -102,7 +103,7 @@ struct Routes {
     int pb_stride;
 };
 
-constexpr int kRouteCounters = 8;  // ints per chunk: routes, then partitioned-block counts, padding
+constexpr int kRouteCounters = 8;  // ints per chunk: routes, partitioned-block counts, refinement-tail entries, padding
 // Textures of fewer texels take the (reference's) full search even with a network: their
 // blocks are mostly edge-clamped copies of a few texels, unlike what the networks learned
 // from, and searching them fully costs next to nothing.

@@ -39,6 +39,9 @@ int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const Fo
     if ((rc = ensure_buf(ctx, sc.prop, sc.cap_prop, blocks * sizeof(PropPicks), "cudaMalloc proposals"))) return rc;
     if ((rc = ensure_buf(ctx, sc.masks, sc.cap_masks, blocks * 4 * kMaskWords * sizeof(uint64_t), "cudaMalloc block-mode masks"))) return rc;
     if ((rc = ensure_buf(ctx, sc.full_err, sc.cap_ferr, blocks * sizeof(float), "cudaMalloc full-search errors"))) return rc;
+    if (ft->L.T <= kTailMaxTexels &&
+        (rc = ensure_buf(ctx, sc.tail, sc.cap_tail, blocks * kTailPerBlock * kTailWords * sizeof(uint4), "cudaMalloc refinement tail")))
+        return rc;
     return ensure_buf(ctx, sc.pbl, sc.cap_pbl, blocks * 4 * kMaxProposals * sizeof(uint32_t), "cudaMalloc work lists");
 }
 
@@ -142,19 +145,34 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     af.refine_iters = pr.fallback_iters;  // the candidates' serial refinement chain sets this pass's duration
     af.pbrec = sc.pbrec + n * kMaxSlots;
     af.snaps = sc.snaps + n * kMaxSlots * kNumCand;
+    if (sc.tail && ft->L.T <= kTailMaxTexels) {
+        // The proposal pass hands its last candidates to the tail.  The fallback pass does not:
+        // it holds few blocks, so its duration is one CTA's chain, which a second, serial
+        // kernel would only lengthen.
+        ap.tail = sc.tail;
+        ap.tail_cap = (int)std::min<size_t>(sc.cap_tail / (kTailWords * sizeof(uint4)), (size_t)1 << 30);
+        ap.spill_live = kSpillLive;
+        ap.tail_count = counts + 6;  // a free route counter
+    }
+    int tails = 0;  // tail launches (timed with their pass's refinement)
+    auto refine = [&](const KernelArgs& k) {
+        cudaError_t e = launch_refine(k, s);
+        if (e == cudaSuccess && k.tail) { e = launch_refine_tail(k, s); tails++; }
+        return e;
+    };
 
     CK(cudaMemsetAsync(counts, 0, mlp::kRouteCounters * sizeof(int), s), "reset route counters");
     if ((rc = done(mlp::launch_mlp_logits(a, nd->net, sc.logits, ctx->d_mlp_error, s), "k_mlp_logits", 0))) return rc;
     if ((rc = done(mlp::launch_select(a, nd->net, sc.logits, sel, r, s), "k_select", 0))) return rc;
     if ((rc = done(launch_front(ap, s), "k_front", 1))) return rc;
-    if ((rc = done(launch_refine(ap, s), "k_refine", 2))) return rc;
+    if ((rc = done(refine(ap), "k_refine", 2))) return rc;
     if ((rc = done(launch_select_pack(ap, s), "k_select_pack", 3))) return rc;
     if ((rc = done(launch_partition_search(af, s), "k_partition_search", 0))) return rc;
     if ((rc = done(launch_front(af, s), "k_front", 1))) return rc;
-    if ((rc = done(launch_refine(af, s), "k_refine", 2))) return rc;
+    if ((rc = done(refine(af), "k_refine", 2))) return rc;
     if ((rc = done(launch_select_pack(af, s), "k_select_pack", 3))) return rc;
     if (ext) { CK(launch_extend(a, ext, s), "k_extend"); ni++; }  // every block of the chunk, after both passes
-    if (launches) *launches += ni;
+    if (launches) *launches += ni + tails;
     return ASTCB200_OK;
 }
 

@@ -347,7 +347,9 @@ int astcb200_stage_times_detail(astcb200_ctx* ctx, float* ms9, int32_t* stage9);
 /* Work the search kernels did in the last encode with ASTCB200_FLAG_STAGE_TIMING (for
  * an operation-count roofline): [0..3] partitioned blocks searched by the front kernel by
  * partition count; [4] decimation modes and [5] block modes it evaluated; [6..9]
- * candidates refined by partition count; [10..12] partition searches for P = 2, 3, 4. */
+ * candidates refined by partition count; [10..12] partition searches for P = 2, 3, 4;
+ * [13] candidates whose last iterations the refinement left to its tail pass (reserved
+ * entries included). */
 int astcb200_work_counters(astcb200_ctx* ctx, uint64_t* counters16);
 
 const char* astcb200_status_string(int status);
