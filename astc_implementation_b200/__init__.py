@@ -277,7 +277,7 @@ class ASTCEncoder:
                           arrs["w3"].shape[0], *[arrs[k].ctypes.data for k in ("w1", "b1", "w2", "b2", "w3", "b3")])
         _check(load_library().astcb200_set_proposal_net(self._ctx, ctypes.byref(net)), self._ctx)
 
-    def set_pruning(self, enable=True, max_partitionings=0, block_modes=0, refine_candidates=0, coverage=0.9,
+    def set_pruning(self, enable=True, max_partitionings=0, block_modes=0, refine_candidates=0, coverage=0.8,
                     threshold=0.5, reroute_error=8.0, front_threads=0, refine_iterations=0,
                     single_partition_floor=0.0, fallback_iterations=0):
         """Proposal-search settings for later encodes of footprints with a network; 0 in the

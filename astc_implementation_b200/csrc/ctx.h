@@ -57,7 +57,7 @@ struct NetDev {
 struct Pruning {
     bool enable = false;
     int kmax = 0, kbm = 0, topn = 0;
-    float coverage = 0.9f, threshold = 0.5f;
+    float coverage = 0.8f, threshold = 0.5f;
     float reroute_error = 8.0f;  // per-texel weighted squared error (8-bit units) above which
                                  // a proposal-search block also takes the full search; 0: off
     int front_threads = 0;  // 0: by footprint (64 up to 16 texels, else 128)
@@ -68,15 +68,16 @@ struct Pruning {
 
 // The settings for a footprint of T texels, zeros replaced by its tuned values.  Tuned on
 // held-out 2048x2048 synthetic textures against the full search with FIXED semantics for
-// the least time at a mean PSNR loss below 0.1 dB (coverage 0.9): blocks of up to 16 texels
-// need nearly the whole refinement (8 partitionings, 32 block modes, 8 candidates, 6
-// iterations); larger blocks gain from the network's partitionings and need far less (3, 8,
-// 3, 6).
+// the least time at a mean PSNR loss below 0.1 dB with no image losing more (coverage 0.8):
+// blocks of up to 16 texels need the whole refinement (8 partitionings, 8 block modes, 8
+// candidates, 6 iterations); larger blocks gain from the network's partitionings and need
+// far less (3, 4, 3, 6).  The network's block-mode ranking is good enough that the front's
+// error estimate over more modes adds nothing.
 inline Pruning resolve_pruning(const Pruning& p, int T) {
     const bool small = T <= 16;
     Pruning r = p;
     if (!r.kmax) r.kmax = small ? 8 : 3;
-    if (!r.kbm) r.kbm = small ? 32 : 8;
+    if (!r.kbm) r.kbm = small ? 8 : 4;
     if (!r.topn) r.topn = small ? 8 : 3;
     if (!r.refine_iters) r.refine_iters = 6;
     if (!r.fallback_iters) r.fallback_iters = small ? 6 : 3;

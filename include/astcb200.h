@@ -216,8 +216,8 @@ int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* ne
 /* Zero in max_partitionings, block_modes, refine_candidates, refine_iterations or
  * fallback_iterations selects the footprint's tuned value, chosen on held-out synthetic
  * textures as the fastest setting within 0.1 dB mean PSNR of the full search with FIXED
- * semantics (with coverage 0.9): for blocks of up to 16 texels 8, 32, 8, 6 and 6; for larger
- * blocks 3, 8, 3, 6 and 3. */
+ * semantics, no image losing more (with coverage 0.8): for blocks of up to 16 texels 8, 8,
+ * 8, 6 and 6; for larger blocks 3, 4, 3, 6 and 3. */
 typedef struct astcb200_pruning {
     uint32_t struct_size;
     uint32_t enable;            /* 0: full search everywhere */
@@ -225,7 +225,7 @@ typedef struct astcb200_pruning {
     uint32_t block_modes;       /* block modes evaluated per partition count, at most 64 (0 = tuned) */
     uint32_t refine_candidates; /* refinement candidates per partitioned block, at most 8 (0 = tuned) */
     float coverage;             /* stop proposing once P=1 plus the proposed probability reaches this
-                                   (0.9 suggested) */
+                                   (0.8 suggested) */
     float threshold;            /* full search when P=1 plus the best max_partitionings carry less
                                    (textures of fewer than 1024 texels always take the full search,
                                    with the reference's 6 refinement iterations) */
