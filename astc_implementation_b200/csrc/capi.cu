@@ -298,14 +298,15 @@ int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* n4) {
     constexpr int E = kStageIntervals + 1;
     for (int c = 0; c < ctx->stage_chunks; c++)
         for (int i = 0; i < kStageIntervals; i++) {
-            const int k = ctx->stage_kind[(size_t)kStageIntervals * c + i];
-            if (k < 0) break;
+            const int kk = ctx->stage_kind[(size_t)kStageIntervals * c + i];
+            if (kk < 0) break;
+            const int k = kk & 3;
             cudaEvent_t e1 = ctx->stage_ev[(size_t)E * c + i + 1];
             CK(cudaEventSynchronize(e1), "stage event");
             float ms = 0.0f;
             CK(cudaEventElapsedTime(&ms, ctx->stage_ev[(size_t)E * c + i], e1), "cudaEventElapsedTime");
             ms4[k] += ms;
-            if (n4) n4[k]++;
+            if (n4) n4[k] += 1 + (kk >> 2);
         }
     return ASTCB200_OK;
 }
@@ -323,7 +324,7 @@ int astcb200_stage_times_detail(astcb200_ctx* ctx, float* ms9, int32_t* stage9) 
             float ms = 0.0f;
             CK(cudaEventElapsedTime(&ms, ctx->stage_ev[(size_t)E * c + i], e1), "cudaEventElapsedTime");
             ms9[i] += ms;
-            if (stage9) stage9[i] = k;
+            if (stage9) stage9[i] = k & 3;
         }
     return ASTCB200_OK;
 }

@@ -165,9 +165,10 @@ int begin_routes(astcb200_ctx* ctx, size_t chunks, cudaStream_t s);
 // The inference kernel's flag pair: [0] set by a CTA that gave up waiting, [1] the polls
 // per wait (0: the default 2^24).
 int ensure_error_flag(astcb200_ctx* ctx);
-// Stage timing: per chunk, an event before the first launch and after each launch
-// (at most kStageIntervals launches), and the stage (0 partition search or network, 1
-// front, 2 refine, 3 select-pack) of each launch, -1 past the last.
+// Stage timing: per chunk, an event before the first launch and after each timed interval
+// (at most kStageIntervals; an interval is one launch, or the refinement and its tail), and
+// per interval its stage (0 partition search or network, 1 front, 2 refine, 3 select-pack)
+// | (launches - 1) << 2, -1 past the last.
 constexpr int kStageIntervals = 9;
 // Queues the search of one chunk (base: addressing, block_first, nblocks) on s; ev and
 // kinds, when not null, receive kStageIntervals + 1 events and the launches' stages.

@@ -79,10 +79,10 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         for (int i = 0; i < kStageIntervals; i++) kinds[i] = -1;
         CK(cudaEventRecord(ev[0], s), "stage event");
     }
-    auto done = [&](cudaError_t e, const char* what, int kind) -> int {
+    auto done = [&](cudaError_t e, const char* what, int kind, int nl = 1) -> int {
         if (e != cudaSuccess) return cuda_fail(ctx, e, what);
         if (ev) {
-            kinds[ni] = (int8_t)kind;
+            kinds[ni] = (int8_t)(kind | (nl - 1) << 2);  // stage, then the interval's extra launches
             CK(cudaEventRecord(ev[ni + 1], s), "stage event");
         }
         ni++;
@@ -155,21 +155,22 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         ap.tail_count = counts + 6;  // a free route counter
     }
     int tails = 0;  // tail launches (timed with their pass's refinement)
-    auto refine = [&](const KernelArgs& k) {
+    auto refine = [&](const KernelArgs& k, const char* what) -> int {
         cudaError_t e = launch_refine(k, s);
+        const int nl = k.tail ? 2 : 1;
         if (e == cudaSuccess && k.tail) { e = launch_refine_tail(k, s); tails++; }
-        return e;
+        return done(e, what, 2, nl);
     };
 
     CK(cudaMemsetAsync(counts, 0, mlp::kRouteCounters * sizeof(int), s), "reset route counters");
     if ((rc = done(mlp::launch_mlp_logits(a, nd->net, sc.logits, ctx->d_mlp_error, s), "k_mlp_logits", 0))) return rc;
     if ((rc = done(mlp::launch_select(a, nd->net, sc.logits, sel, r, s), "k_select", 0))) return rc;
     if ((rc = done(launch_front(ap, s), "k_front", 1))) return rc;
-    if ((rc = done(refine(ap), "k_refine", 2))) return rc;
+    if ((rc = refine(ap, "k_refine"))) return rc;
     if ((rc = done(launch_select_pack(ap, s), "k_select_pack", 3))) return rc;
     if ((rc = done(launch_partition_search(af, s), "k_partition_search", 0))) return rc;
     if ((rc = done(launch_front(af, s), "k_front", 1))) return rc;
-    if ((rc = done(refine(af), "k_refine", 2))) return rc;
+    if ((rc = refine(af, "k_refine"))) return rc;
     if ((rc = done(launch_select_pack(af, s), "k_select_pack", 3))) return rc;
     if (ext) { CK(launch_extend(a, ext, s), "k_extend"); ni++; }  // every block of the chunk, after both passes
     if (launches) *launches += ni + tails;

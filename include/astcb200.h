@@ -334,7 +334,8 @@ int astcb200_decode_error_device(uint32_t block_x, uint32_t block_y, uint32_t di
 
 /* Device milliseconds spent in each of the four kernels (partition search, front,
  * refine, select/pack) by the last encode call, summed over chunks; needs
- * ASTCB200_FLAG_STAGE_TIMING.  launches[4] receives the launch counts (optional). */
+ * ASTCB200_FLAG_STAGE_TIMING.  launches[4] receives the launch counts (optional).  The
+ * proposal pass's refinement includes its tail pass, a second launch. */
 int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* launches4);
 
 /* Per-launch device milliseconds of the last encode, summed over chunks by the launch's
