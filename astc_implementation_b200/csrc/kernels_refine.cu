@@ -618,7 +618,9 @@ __device__ bool refine_step(const KernelArgs& a, const PBRec& rec, const int P, 
             else if ((ed < eb) && (uqw > 0)) { cs.qw[we] = (uint8_t)dn; moved |= (int32_t)dn != uqw; }
         }
     }
-    final_error();
+    // In iteration 0 a pass16 that moved no weight leaves the weights and endpoints of the
+    // error taken before it: the same total, which cannot improve the snapshot.
+    if (it > 0 || moved) final_error();
     return moved;
 }
 
