@@ -413,16 +413,38 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
     const int blk = chunk_block(a, lb);
     if (blk < 0) return;
     const float* z = logits + (size_t)lb * S.nout;
-    // one pass: the softmax maximum and this lane's K best partitionings (value desc, index asc)
-    float mx = -3.0e38f;
+    // First pass: the softmax maximum and each lane's best partitioning logit.  The kmax-th
+    // largest of the 32 lane maxima bounds the kmax-th largest logit from below (those lanes'
+    // maxima are kmax distinct logits at least that large), so only logits at or above it
+    // can be among the kmax best.
+    float mx = -3.0e38f, lm = -3.0e38f;
+    for (int c = lane; c <= S.p1; c += 32) {
+        const float v = z[c];
+        mx = fmaxf(mx, v);
+        if (c < S.p1) lm = fmaxf(lm, v);
+    }
+    mx = warp_max(mx);
+    float theta = 3.0e38f;
+    if (sel.kmax >= 1) {
+        int rank = 0;  // lanes ahead of this one in (maximum descending, lane ascending) order
+        for (int j = 0; j < 32; j++) {
+            const float o = __shfl_sync(kFull, lm, j);
+            rank += (o > lm || (o == lm && j < lane)) ? 1 : 0;
+        }
+        const uint32_t at = __ballot_sync(kFull, rank == sel.kmax - 1);
+        theta = __shfl_sync(kFull, lm, __ffs(at) - 1);
+    }
+    // Second pass: the softmax sum (in the same order as ever) and this lane's K best
+    // partitionings among those at or above the bound (value desc, index asc).
     float lv[K];
     int lc[K];
 #pragma unroll
     for (int k = 0; k < K; k++) { lv[k] = -3.0e38f; lc[k] = 0x7FFFFFFF; }
+    float se = 0.0f;
     for (int c = lane; c <= S.p1; c += 32) {
         const float v = z[c];
-        mx = fmaxf(mx, v);
-        if (c < S.p1 && v > lv[K - 1]) {  // a lane sees its classes in increasing order
+        se += __expf(v - mx);
+        if (c < S.p1 && v >= theta && v > lv[K - 1]) {  // a lane sees its classes in increasing order
             lv[K - 1] = v; lc[K - 1] = c;
 #pragma unroll
             for (int k = K - 1; k > 0; k--)
@@ -432,9 +454,6 @@ __global__ void __launch_bounds__(128) k_select(const __grid_constant__ KernelAr
                 }
         }
     }
-    mx = warp_max(mx);
-    float se = 0.0f;
-    for (int c = lane; c <= S.p1; c += 32) se += __expf(z[c] - mx);
     se = warp_sum(se);
     const float p1 = __expf(z[S.p1] - mx) / se;
     // the kmax best partitionings, merged from the lanes' lists
