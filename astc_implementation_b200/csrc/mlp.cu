@@ -321,6 +321,16 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
         }
         __syncthreads();
         if (*abort_flag) { failed = true; goto cleanup; }
+        // this thread's 32 biases of the chunk, loaded before the wait so that it hides them
+        float bv[32];
+        {
+            const float4* bias4 = reinterpret_cast<const float4*>(net.b3 + chunk_of(j) * kChunkN + half * 32);
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const float4 t = __ldg(bias4 + q);
+                bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
+            }
+        }
         ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1, wl);
         if (ok) m_done[1 + b]++;
         if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
@@ -336,13 +346,12 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
         float* st = reinterpret_cast<float*>(sm + kOffStage + b * kStageBuf) + m * kStageStride;
         {
             const int c = half * 32;
-            const float* bias = net.b3 + chunk_of(j) * kChunkN + c;
             float v[32];
             tmem_load32(tmem_row + b * kChunkN + c, v);
 #pragma unroll
             for (int q = 0; q < 8; q++)
-                reinterpret_cast<float4*>(st + c)[q] = make_float4(v[4 * q] + __ldg(bias + 4 * q), v[4 * q + 1] + __ldg(bias + 4 * q + 1),
-                                                                   v[4 * q + 2] + __ldg(bias + 4 * q + 2), v[4 * q + 3] + __ldg(bias + 4 * q + 3));
+                reinterpret_cast<float4*>(st + c)[q] = make_float4(v[4 * q] + bv[4 * q], v[4 * q + 1] + bv[4 * q + 1],
+                                                                   v[4 * q + 2] + bv[4 * q + 2], v[4 * q + 3] + bv[4 * q + 3]);
         }
         async_proxy_fence();
         tc_before();
