@@ -246,6 +246,17 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
 
     const uint32_t a_base = smem_u32(sA), w_base = smem_u32(sW);
     constexpr uint32_t kLboA = (kTileRows / 8) * 128, kLboW256 = (256 / 8) * 128, kLboW3 = (kChunkN / 8) * 128;
+    auto issue_chunk = [&](int jj) -> bool {  // thread 0: chunk jj's MMAs once its weights have landed
+        const int bb = jj & 1;
+        if (!mbar_wait(&bw[bb], w_done[bb] & 1, wl)) return false;
+        w_done[bb]++;
+        for (int kk = 0; kk < 16; kk++)
+            mma_bf16(tmem + bb * kChunkN, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
+                     smem_desc(w_base + bb * kW3Buf + kk * 2 * kLboW3, kLboW3, 128), instr_desc(128, kChunkN), kk > 0);
+        mma_commit(&bm[1 + bb]);
+        m_issued[1 + bb]++;
+        return true;
+    };
 
     // ---- layer 1: X (128 x k0p) . W1^T -> tensor memory columns [0, 256)
     if (tid == 0) {
@@ -302,25 +313,19 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
     tc_before();
     __syncthreads();
 
-    // ---- layer 3: H2 (128 x 256) . W3^T in chunks of 128 columns, accumulators
-    // alternating between tensor-memory columns [0, 128) and [128, 256)
+    // ---- layer 3: H2 (128 x 256) . W3^T in chunks of 64 columns, accumulators alternating
+    // between tensor-memory columns [0, 64) and [64, 128).  Chunk 0's MMAs are issued here;
+    // chunk j + 1's right after chunk j's have completed, into the accumulator buffer chunk
+    // j - 1's epilogue read before the previous staging barrier, so that they run while chunk
+    // j's epilogue reads its own.  Two barriers per chunk.
+    if (tid == 0) {
+        tc_after();
+        if (!issue_chunk(0)) *abort_flag = 1;
+    }
+    __syncthreads();
+    if (*abort_flag) { failed = true; goto cleanup; }
     for (int j = 0; j < nchunks; j++) {
         const int b = j & 1;
-        if (tid == 0) {
-            tc_after();
-            for (int jj = (j == 0 ? 0 : j + 1); jj <= j + 1 && jj < nchunks; jj++) {
-                const int bb = jj & 1;
-                if (!mbar_wait(&bw[bb], w_done[bb] & 1, wl)) { *abort_flag = 1; break; }
-                w_done[bb]++;
-                for (int kk = 0; kk < 16; kk++)
-                    mma_bf16(tmem + bb * kChunkN, smem_desc(a_base + kk * 2 * kLboA, kLboA, 128),
-                             smem_desc(w_base + bb * kW3Buf + kk * 2 * kLboW3, kLboW3, 128), instr_desc(128, kChunkN), kk > 0);
-                mma_commit(&bm[1 + bb]);
-                m_issued[1 + bb]++;
-            }
-        }
-        __syncthreads();
-        if (*abort_flag) { failed = true; goto cleanup; }
         // this thread's 32 biases of the chunk, loaded before the wait so that it hides them
         float bv[32];
         {
@@ -331,13 +336,16 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
                 bv[4 * q] = t.x; bv[4 * q + 1] = t.y; bv[4 * q + 2] = t.z; bv[4 * q + 3] = t.w;
             }
         }
-        ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1, wl);
+        ok = mbar_wait(&bm[1 + b], m_done[1 + b] & 1, wl);  // chunk j was issued before this iteration
         if (ok) m_done[1 + b]++;
         if (__syncthreads_or(!ok)) { failed = true; goto cleanup; }
         tc_after();
-        if (tid == 0 && j + 2 < nchunks) {
-            load_weights(sW + b * kW3Buf, net.w3 + (size_t)chunk_of(j + 2) * kChunkN * 256, kW3Buf, &bw[b]);
-            w_issued[b]++;
+        if (tid == 0) {
+            if (j + 2 < nchunks) {  // chunk j's MMAs are done with its weight buffer
+                load_weights(sW + b * kW3Buf, net.w3 + (size_t)chunk_of(j + 2) * kChunkN * 256, kW3Buf, &bw[b]);
+                w_issued[b]++;
+            }
+            if (j + 1 < nchunks && !issue_chunk(j + 1)) *abort_flag = 1;  // seen after the staging barrier
         }
         // the row's 64 logits go to padded shared memory (32 from each of its two threads),
         // then to global memory as one contiguous 256-byte bulk copy issued by the row's first
@@ -356,6 +364,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
         async_proxy_fence();
         tc_before();
         __syncthreads();  // the row is staged; every read of this accumulator buffer is done
+        if (*abort_flag) { failed = true; goto cleanup; }
         if (half == 0) {
             if (store) {
                 float* out = logits + (size_t)lb * S.nout + chunk_of(j) * kChunkN;
@@ -365,7 +374,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1)
                 asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             }
             // the other buffer, written next, must have been read by its copy (chunk j - 1);
-            // the barrier at the top of the next iteration orders this before those writes
+            // the barriers of the next iteration order this before those writes
             asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
         }
     }
