@@ -122,16 +122,18 @@ def test_batch_fixed_equals_single_images():
 def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by, topn, iters, fb):
     """The proposal search with FIXED semantics and the footprint's tuned settings: every
     proposal-search block equals the FIXED oracle restricted to the GPU's selection; every
-    other block equals the FIXED full search with the fallback's iteration count."""
+    other block equals the FIXED full search with the fallback's iteration count.  The image
+    is large enough that refinement CTAs hand their last candidates to the tail pass."""
     net = proposal.load_weights(bx, by)
-    w, h = 11 * bx + 3, 7 * by + 2
+    w, h = 40 * bx + 3, 24 * by + 2
     img = synth.make_texture(w, h, 190 + bx)
-    enc = ab.ASTCEncoder(device=0, fixed=True)
+    enc = ab.ASTCEncoder(device=0, fixed=True, stage_timing=True)
     enc.secondaryInit(w, h, bx, by)
     enc.set_proposal_net(net)
     enc.set_pruning(True, reroute_error=0.0)
     sym = enc.encode_symbolic(img)
     blocks = enc.encode(img).reshape(-1, 16)
+    tail = int(enc.work_counters()[13])
     route, picks, masks = enc.proposal_selection(img)
     enc.close()
     n = picks.shape[0]
@@ -147,3 +149,4 @@ def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by, topn,
     assert prop.sum() > 0.5 * n
     assert np.array_equal(sym[prop], r_sym[prop]) and np.array_equal(blocks[prop], r_out[prop])
     assert np.array_equal(sym[~prop], f_sym[~prop]) and np.array_equal(blocks[~prop], f_out[~prop])
+    assert tail > 0  # candidates finished by k_refine_tail are among those compared
