@@ -291,6 +291,35 @@ int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* 
     return encode_host(ctx, rgba8, nullptr, symbolic, nullptr);
 }
 
+int astcb200_search_stages(astcb200_ctx* ctx, const uint8_t* rgba8, void* picks, size_t picks_bytes, void* records,
+                           size_t records_bytes) {
+    if (!ctx || !rgba8 || !picks || !records) return ASTCB200_BAD_ARG;
+    if (!ctx->have_image) return ASTCB200_NO_IMAGE;
+    const size_t nb = ctx->nblocks;
+    if (nb > ctx->chunk || picks_bytes < nb * sizeof(PartPicks) || records_bytes < nb * kSlotsPerBlock * sizeof(PBRec))
+        return ASTCB200_BAD_ARG;
+    ASTCB200_DEVICE_SCOPE(ctx);
+    const size_t in_bytes = (size_t)ctx->width * ctx->height * 4;
+    int rc;
+    if ((rc = ensure_buf(ctx, ctx->d_img, ctx->img_cap, in_bytes, "cudaMalloc image"))) return rc;
+    if ((rc = ensure_scratch(ctx, ctx->scratch, nb, kSlotsPerBlock))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_img, rgba8, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D image");
+    KernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.img = ctx->d_img;
+    a.width = (int)ctx->width; a.height = (int)ctx->height; a.nbx = (int)ctx->nbx; a.nby = (int)ctx->nby;
+    a.block_first = 0; a.nblocks = (int)nb;
+    a.tables = ctx->cur->d; a.L = ctx->cur->L;
+    a.picks = ctx->scratch.picks; a.pbrec = ctx->scratch.pbrec; a.snaps = ctx->scratch.snaps;
+    a.slots = kSlotsPerBlock; a.topn = kNumCand;
+    a.fixed = (ctx->cfg.flags & ASTCB200_FLAG_FIXED_SEMANTICS) ? 1 : 0;
+    CK(launch_partition_search(a, ctx->stream), "k_partition_search");
+    CK(launch_front(a, ctx->stream), "k_front");
+    CK(cudaMemcpyAsync(picks, a.picks, nb * sizeof(PartPicks), cudaMemcpyDeviceToHost, ctx->stream), "D2H picks");
+    CK(cudaMemcpyAsync(records, a.pbrec, nb * kSlotsPerBlock * sizeof(PBRec), cudaMemcpyDeviceToHost, ctx->stream), "D2H records");
+    return wait_stream(ctx, ctx->stream);
+}
+
 int astcb200_stage_times(astcb200_ctx* ctx, float* ms4, uint32_t* n4) {
     if (!ctx || !ms4) return ASTCB200_BAD_ARG;
     for (int k = 0; k < 4; k++) { ms4[k] = 0.0f; if (n4) n4[k] = 0; }

@@ -332,6 +332,16 @@ int astcb200_decode_error_device(uint32_t block_x, uint32_t block_y, uint32_t di
                                  const uint8_t* d_blocks, const uint8_t* d_ref_rgba8, uint64_t* d_sse,
                                  void* cuda_stream);
 
+/* Test hook: the full search's first two stages for the image set by astcb200_set_image
+ * (host RGBA8, at most one chunk of blocks): the partition search's picks (per block, 32
+ * bytes: for P = 2, 3, 4 four table entries and their count, then padding) and the front's
+ * partitioned-block records (per block 13 slots -- P = 1, then four per P = 2, 3, 4 -- of
+ * 784 bytes: per partition the average, ep0 and ep1 as 4 floats each, then P, table entry,
+ * candidate count and seed, then 8 candidates of 72 bytes: trial block-mode index (uint16),
+ * colour quant level and its "mod" level, 4 endpoint formats, 64 quantised weights). */
+int astcb200_search_stages(astcb200_ctx* ctx, const uint8_t* rgba8, void* picks, size_t picks_bytes, void* records,
+                           size_t records_bytes);
+
 /* Device milliseconds spent in each of the four kernels (partition search, front,
  * refine, select/pack) by the last encode call, summed over chunks; needs
  * ASTCB200_FLAG_STAGE_TIMING.  launches[4] receives the launch counts (optional).  The

@@ -907,6 +907,7 @@ struct PBWork {
     Combo combo[21][13];
     std::vector<CCR> ccr;
     Cand cand[NUM_CAND], top[NUM_CAND];
+    int ncand;  // pass12's candidates (cand[0..ncand); slots whose error is ERR_DEFAULT stay inert)
     v4 rgbs[NUM_CAND][4];
     int32_t ue0[NUM_CAND][4][4], ue1[NUM_CAND][4][4];
 };
@@ -1826,6 +1827,7 @@ Sym process_pb(const Footprint& f, const InputBlock& b, int P, PBWork& w, const 
         for (int i = 0; i < MAX_WEIGHTS; i++) c.qw[i] = w.qr[tc[k].i].qw[i];
         ncand = k + 1;
     }
+    w.ncand = ncand;
     // compression_pipeline.cpp:473-484 refinement loop, one candidate at a time
     for (int k = 0; k < std::min(ncand, topn); k++) {
         Cand& c = w.cand[k];
@@ -2518,6 +2520,32 @@ int orc_partition_search(int bx, int by, const float* texels, int P, uint32_t* e
     flags_from_texels(b, f.T);
     std::unique_ptr<InputBlock[]> out(new InputBlock[4]);
     return partition_search(f, b, P, out.get(), entries);
+}
+int orc_front_candidates(int bx, int by, const float* texels, int P, int entry, float* ep, uint32_t* cands) {
+    if (!valid_footprint(bx, by) || P < 1 || P > 4 || entry < 0 || entry > 1023 || !ep || !cands) return -1;
+    const Footprint& f = *get_fp(bx, by);
+    InputBlock b; std::memset(&b, 0, sizeof(b));
+    for (int t = 0; t < f.T; t++) for (int c = 0; c < 4; c++) comp(b.px[t], c) = texels[t * 4 + c];
+    flags_from_texels(b, f.T);
+    InputBlock pb = b;
+    if (P > 1) make_pb(f, b, P, entry, pb);
+    std::unique_ptr<PBWork> w(new PBWork());
+    process_pb(f, pb, P, *w, nullptr, NUM_CAND, 0);  // passes 01-12, no refinement
+    for (int q = 0; q < 4; q++)
+        for (int c = 0; c < 4; c++) {
+            ep[q * 12 + c] = compc(w->ei.part[q].avg, c);
+            ep[q * 12 + 4 + c] = compc(w->ei.part[q].ep0, c);
+            ep[q * 12 + 8 + c] = compc(w->ei.part[q].ep1, c);
+        }
+    std::memset(cands, 0, sizeof(uint32_t) * NUM_CAND * 71);
+    for (int k = 0; k < w->ncand; k++) {
+        const Cand& c = w->cand[k];
+        uint32_t* o = cands + k * 71;
+        o[0] = c.bm_lookup; o[1] = c.ql; o[2] = c.qlm;
+        for (int q = 0; q < 4; q++) o[3 + q] = c.fmt[q];
+        for (int i = 0; i < 64; i++) o[7 + i] = i < MAX_WEIGHTS ? c.qw[i] : 0;
+    }
+    return w->ncand;
 }
 int orc_partition_order(int bx, int by, const float* texels, int P, uint32_t* mismatch, uint32_t* order) {
     if (!valid_footprint(bx, by) || P < 2 || P > 4 || !mismatch || !order) return -1;

@@ -94,6 +94,12 @@ int orc_partition_search(int bx, int by, const float* texels, int partition_coun
 // selected partitionings) and order[128] (pass005's first 128 table entries, in the
 // current semantics).  Returns the number of selected partitionings.
 int orc_partition_order(int bx, int by, const float* texels, int partition_count, uint32_t* mismatch, uint32_t* order);
+// Passes 01-12 of one partitioned block (P = 1, or table entry `entry` of P = 2..4) in the
+// current semantics, no refinement: ep[48] receives per partition the average, ep0 and ep1
+// (pass01; 4 floats each), cands[8][71] pass12's candidates (trial block-mode index, colour
+// quant level and its "mod" level, 4 endpoint formats, 64 quantised weights).  Returns the
+// number of candidates.
+int orc_front_candidates(int bx, int by, const float* texels, int partition_count, int entry, float* ep, uint32_t* cands);
 
 #ifdef __cplusplus
 }

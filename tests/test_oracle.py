@@ -140,3 +140,27 @@ def test_full_search_iteration_count():
             assert np.array_equal(sym, full_sym) and np.array_equal(out, full_out.reshape(n, 16))
         else:
             assert (sym[:, 0].view(np.float32) >= full_sym[:, 0].view(np.float32)).all()
+
+
+def test_front_candidates_are_well_formed():
+    """orc_front_candidates (passes 01-12 of one partitioned block, the GPU stage test's
+    checker): 1..8 candidates with distinct valid trial block modes, colour quant levels of
+    at least 4, and partition 0's average finite (its endpoints are NaN for a block with no
+    direction, as the shader's normalisation of a zero vector gives)."""
+    orc = _libs.oracle()
+    img = synth.make_texture(24, 24, 11)
+    for bx, by in [(4, 4), (6, 6)]:
+        c = np.zeros(13, np.uint32)
+        orc.orc_counts(bx, by, _libs.ptr(c))
+        nbm = int(c[1])
+        tex = synth.texel_blocks(img, bx, by)
+        for b in range(3):
+            for P, entry in [(1, 0), (2, 5), (3, 17)]:
+                ep = np.zeros(48, np.float32)
+                cands = np.zeros((8, 71), np.uint32)
+                n = orc.orc_front_candidates(bx, by, _libs.ptr(np.ascontiguousarray(tex[b])), P, entry, _libs.ptr(ep), _libs.ptr(cands))
+                assert 1 <= n <= 8
+                bms = [int(v) for v in cands[:n, 0]]
+                assert len(set(bms)) == n and all(m < nbm for m in bms)
+                assert all(int(v) >= 4 for v in cands[:n, 1])
+                assert np.all(np.isfinite(ep.reshape(4, 3, 4)[0, 0]))
