@@ -104,7 +104,7 @@ def load_library():
         "astcb200_encode": (I32, [P, P, P, SZ, ctypes.POINTER(Stats)]),
         "astcb200_encode_device": (I32, [P, P, P, P]),
         "astcb200_encode_symbolic": (I32, [P, P, P, SZ]),
-        "astcb200_search_stages": (I32, [P, P, P, SZ, P, SZ]),
+        "astcb200_search_stages": (I32, [P, P, P, SZ, P, SZ, P, SZ]),
         "astcb200_store_image": (I32, [U32, U32, U32, U32, P, SZ, ctypes.c_char_p]),
         "astcb200_astc_containers_device": (I32, [ctypes.POINTER(AstcImage), U32, P]),
         "astcb200_decode": (I32, [U32, U32, U32, U32, P, SZ, P]),
@@ -227,16 +227,22 @@ class ASTCEncoder:
     RECORD = np.dtype([("avg", "<f4", (4, 4)), ("ep0", "<f4", (4, 4)), ("ep1", "<f4", (4, 4)), ("P", "<u4"),
                        ("entry", "<u4"), ("ncand", "<u4"), ("seed", "<u4"), ("cand", CANDIDATE, (8,))])
 
+    SNAPSHOT = np.dtype([("err", "<f4"), ("bm", "<u2"), ("final_q", "u1"), ("matched", "u1"), ("ffmt", "u1", (4,)),
+                         ("pad", "u1", (4,)), ("packed", "u1", (32,)), ("qw", "u1", (64,))])
+
     def search_stages(self, imageData):
-        """Test hook: the full search's partition picks (numBlocks, 16) u16 and the front's
-        records (numBlocks, 13) of RECORD for an image of at most one chunk."""
+        """Test hook: the full search's partition picks (numBlocks, 16) u16, the front's records
+        (numBlocks, 13) of RECORD and, after 6 refinement iterations, every candidate's best
+        state (numBlocks, 13, 8) of SNAPSHOT, for an image of at most one chunk."""
         lib = load_library()
         img = self._image(imageData)
         picks = np.empty((self.numBlocks, 16), np.uint16)
         recs = np.empty((self.numBlocks, 13), self.RECORD)
-        assert self.RECORD.itemsize == 784
-        _check(lib.astcb200_search_stages(self._ctx, _ptr(img), _ptr(picks), picks.nbytes, _ptr(recs), recs.nbytes), self._ctx)
-        return picks, recs
+        snaps = np.empty((self.numBlocks, 13, 8), self.SNAPSHOT)
+        assert self.RECORD.itemsize == 784 and self.SNAPSHOT.itemsize == 112
+        _check(lib.astcb200_search_stages(self._ctx, _ptr(img), _ptr(picks), picks.nbytes, _ptr(recs), recs.nbytes,
+                                          _ptr(snaps), snaps.nbytes), self._ctx)
+        return picks, recs, snaps
 
     def encode_device(self, d_rgba8, d_out_blocks, stream=0):
         """Queues the search on device buffers (integer device addresses); does not wait."""

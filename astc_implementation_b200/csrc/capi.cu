@@ -292,11 +292,12 @@ int astcb200_encode_symbolic(astcb200_ctx* ctx, const uint8_t* rgba8, uint32_t* 
 }
 
 int astcb200_search_stages(astcb200_ctx* ctx, const uint8_t* rgba8, void* picks, size_t picks_bytes, void* records,
-                           size_t records_bytes) {
+                           size_t records_bytes, void* snapshots, size_t snapshots_bytes) {
     if (!ctx || !rgba8 || !picks || !records) return ASTCB200_BAD_ARG;
     if (!ctx->have_image) return ASTCB200_NO_IMAGE;
     const size_t nb = ctx->nblocks;
-    if (nb > ctx->chunk || picks_bytes < nb * sizeof(PartPicks) || records_bytes < nb * kSlotsPerBlock * sizeof(PBRec))
+    if (nb > ctx->chunk || picks_bytes < nb * sizeof(PartPicks) || records_bytes < nb * kSlotsPerBlock * sizeof(PBRec) ||
+        (snapshots && snapshots_bytes < nb * kSlotsPerBlock * kNumCand * sizeof(Snap)))
         return ASTCB200_BAD_ARG;
     ASTCB200_DEVICE_SCOPE(ctx);
     const size_t in_bytes = (size_t)ctx->width * ctx->height * 4;
@@ -315,6 +316,11 @@ int astcb200_search_stages(astcb200_ctx* ctx, const uint8_t* rgba8, void* picks,
     a.fixed = (ctx->cfg.flags & ASTCB200_FLAG_FIXED_SEMANTICS) ? 1 : 0;
     CK(launch_partition_search(a, ctx->stream), "k_partition_search");
     CK(launch_front(a, ctx->stream), "k_front");
+    if (snapshots) {
+        CK(launch_refine(a, ctx->stream), "k_refine");
+        CK(cudaMemcpyAsync(snapshots, a.snaps, nb * kSlotsPerBlock * kNumCand * sizeof(Snap), cudaMemcpyDeviceToHost, ctx->stream),
+           "D2H snapshots");
+    }
     CK(cudaMemcpyAsync(picks, a.picks, nb * sizeof(PartPicks), cudaMemcpyDeviceToHost, ctx->stream), "D2H picks");
     CK(cudaMemcpyAsync(records, a.pbrec, nb * kSlotsPerBlock * sizeof(PBRec), cudaMemcpyDeviceToHost, ctx->stream), "D2H records");
     return wait_stream(ctx, ctx->stream);

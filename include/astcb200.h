@@ -338,9 +338,13 @@ int astcb200_decode_error_device(uint32_t block_x, uint32_t block_y, uint32_t di
  * partitioned-block records (per block 13 slots -- P = 1, then four per P = 2, 3, 4 -- of
  * 784 bytes: per partition the average, ep0 and ep1 as 4 floats each, then P, table entry,
  * candidate count and seed, then 8 candidates of 72 bytes: trial block-mode index (uint16),
- * colour quant level and its "mod" level, 4 endpoint formats, 64 quantised weights). */
+ * colour quant level and its "mod" level, 4 endpoint formats, 64 quantised weights);
+ * snapshots (optional): after the refinement's 6 iterations, each candidate's best state
+ * (per block 13 x 8 records of 112 bytes: error, trial block-mode index (uint16), final quant
+ * level, matched flag, 4 endpoint formats, 4 padding bytes, 32 packed endpoint values, 64
+ * weights; inert slots have error 1e37). */
 int astcb200_search_stages(astcb200_ctx* ctx, const uint8_t* rgba8, void* picks, size_t picks_bytes, void* records,
-                           size_t records_bytes);
+                           size_t records_bytes, void* snapshots, size_t snapshots_bytes);
 
 /* Device milliseconds spent in each of the four kernels (partition search, front,
  * refine, select/pack) by the last encode call, summed over chunks; needs

@@ -2547,6 +2547,29 @@ int orc_front_candidates(int bx, int by, const float* texels, int P, int entry, 
     }
     return w->ncand;
 }
+int orc_refined_candidates(int bx, int by, const float* texels, int P, int entry, int iters, uint32_t* out) {
+    if (!valid_footprint(bx, by) || P < 1 || P > 4 || entry < 0 || entry > 1023 || iters < 1 || iters > 6 || !out) return -1;
+    const Footprint& f = *get_fp(bx, by);
+    InputBlock b; std::memset(&b, 0, sizeof(b));
+    for (int t = 0; t < f.T; t++) for (int c = 0; c < 4; c++) comp(b.px[t], c) = texels[t * 4 + c];
+    flags_from_texels(b, f.T);
+    InputBlock pb = b;
+    if (P > 1) make_pb(f, b, P, entry, pb);
+    std::unique_ptr<PBWork> w(new PBWork());
+    process_pb(f, pb, P, *w, nullptr, NUM_CAND, iters);
+    std::memset(out, 0, sizeof(uint32_t) * NUM_CAND * 104);
+    for (int k = 0; k < NUM_CAND; k++) {
+        const Cand& c = w->top[k];
+        uint32_t* o = out + k * 104;
+        std::memcpy(&o[0], &c.total_error, 4);
+        if (!(c.total_error < ERR_DEFAULT)) continue;
+        o[1] = c.bm_lookup; o[2] = c.final_q; o[3] = c.matched;
+        for (int q = 0; q < 4; q++) o[4 + q] = c.ffmt[q];
+        for (int i = 0; i < 32; i++) o[8 + i] = c.packed[i];
+        for (int i = 0; i < 64; i++) o[40 + i] = c.qw[i];
+    }
+    return w->ncand;
+}
 int orc_partition_order(int bx, int by, const float* texels, int P, uint32_t* mismatch, uint32_t* order) {
     if (!valid_footprint(bx, by) || P < 2 || P > 4 || !mismatch || !order) return -1;
     const Footprint& f = *get_fp(bx, by);

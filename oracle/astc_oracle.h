@@ -100,6 +100,11 @@ int orc_partition_order(int bx, int by, const float* texels, int partition_count
 // quant level and its "mod" level, 4 endpoint formats, 64 quantised weights).  Returns the
 // number of candidates.
 int orc_front_candidates(int bx, int by, const float* texels, int partition_count, int entry, float* ep, uint32_t* cands);
+// The same block refined `iters` times (1..6): out[8][104] receives each candidate's best
+// state (pass17's snapshot): error (float bits; ERR_DEFAULT for an inert slot, the rest then
+// 0), trial block-mode index, final quant level, matched flag, 4 endpoint formats, 32 packed
+// endpoint values, 64 weights.  Returns the number of candidates.
+int orc_refined_candidates(int bx, int by, const float* texels, int partition_count, int entry, int iters, uint32_t* out);
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,8 @@
-"""Per-stage parity of the full search: the GPU's partition picks (passes 001-007) and the
+"""Per-stage parity of the full search: the GPU's partition picks (passes 001-007), the
 front's partitioned-block records (pass01's averages and endpoints, pass12's candidates with
-their quant levels, formats and quantised weights) against the CPU oracle, block by block and
-slot by slot, in both semantics.  The end-to-end parity tests compare only the final blocks,
+their quant levels, formats and quantised weights) and every candidate's best state after the
+refinement (passes 13-17) against the CPU oracle, block by block, slot by slot and candidate
+by candidate, in both semantics.  The end-to-end parity tests compare only the final blocks,
 where a stage error that does not change the winning candidate would stay invisible."""
 import numpy as np
 import pytest
@@ -38,7 +39,7 @@ def test_partition_picks_and_front_records_match_the_oracle(bx, by, fixed):
     img = synth.make_texture(w, h, 700 + bx * 16 + by)
     enc = ab.ASTCEncoder(device=0, fixed=fixed)
     enc.secondaryInit(w, h, bx, by)
-    picks, recs = enc.search_stages(img)
+    picks, recs, snaps = enc.search_stages(img)
     enc.close()
     tex = synth.texel_blocks(img, bx, by)
     orc = _libs.oracle()
@@ -73,6 +74,18 @@ def test_partition_picks_and_front_records_match_the_oracle(bx, by, fixed):
                     assert (int(c["bm"]), int(c["ql"]), int(c["qlm"])) == (int(o[0]), int(o[1]), int(o[2])), (b, s, k)
                     assert [int(v) for v in c["fmt"]] == [int(v) for v in o[3:7]], (b, s, k)
                     assert np.array_equal(c["qw"].astype(np.uint32), o[7:71]), (b, s, k)
+                # passes 13-17: each candidate's best state after the reference's 6 iterations
+                ref = np.zeros((8, 104), np.uint32)
+                assert orc.orc_refined_candidates(bx, by, _libs.ptr(np.ascontiguousarray(tex[b])), P, entry, 6, _libs.ptr(ref)) == n
+                for k in range(8):
+                    g, o = snaps[b, s, k], ref[k]
+                    assert int(np.float32(g["err"]).view(np.uint32)) == int(o[0]), (b, s, k, "error")
+                    if k >= n:
+                        continue
+                    assert (int(g["bm"]), int(g["final_q"]), int(g["matched"])) == (int(o[1]), int(o[2]), int(o[3])), (b, s, k)
+                    assert [int(v) for v in g["ffmt"]] == [int(v) for v in o[4:8]], (b, s, k)
+                    assert np.array_equal(g["packed"].astype(np.uint32), o[8:40]), (b, s, k, "packed")
+                    assert np.array_equal(g["qw"].astype(np.uint32), o[40:104]), (b, s, k, "weights")
                 n_cands += n
         assert n_cands > 0
     finally:
