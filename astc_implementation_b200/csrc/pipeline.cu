@@ -31,7 +31,11 @@ const NetDev* net_for(const astcb200_ctx* ctx, const FootTables* ft) {
 
 int ensure_chunk_scratch(astcb200_ctx* ctx, Scratch& sc, size_t blocks, const FootTables* ft) {
     const NetDev* nd = net_for(ctx, ft);
-    if (!nd) return ensure_scratch(ctx, sc, blocks, kSlotsPerBlock);
+    if (!nd) {
+        const int rc = ensure_scratch(ctx, sc, blocks, kSlotsPerBlock);
+        if (rc || ft->L.T > kTailMaxTexels) return rc;
+        return ensure_buf(ctx, sc.tail, sc.cap_tail, blocks * kTailPerBlockFull * kTailWords * sizeof(uint4), "cudaMalloc refinement tail");
+    }
     int rc;
     if ((rc = ensure_scratch(ctx, sc, blocks, kSlotsPerBlock + kMaxSlots))) return rc;
     if ((rc = ensure_buf(ctx, sc.logits, sc.cap_logits, blocks * nd->net.s.nout * sizeof(float), "cudaMalloc logits"))) return rc;
@@ -93,12 +97,28 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     if (!nd) {
         a.slots = kSlotsPerBlock;
         a.topn = kNumCand;
+        int nl = 1;  // launches of the refinement interval
+        if (sc.tail && ft->L.T <= kTailMaxTexels &&
+            (ctx->counts_used + 1) * mlp::kRouteCounters <= ctx->counts_cap / sizeof(int)) {
+            // the refinement hands its last candidates to the tail, as in the proposal pass
+            int* counts = ctx->d_counts + mlp::kRouteCounters * ctx->counts_used++;
+            CK(cudaMemsetAsync(counts, 0, mlp::kRouteCounters * sizeof(int), s), "reset tail counter");
+            a.tail = sc.tail;
+            a.tail_cap = (int)std::min<size_t>(sc.cap_tail / (kTailWords * sizeof(uint4)), (size_t)1 << 30);
+            a.spill_live = kSpillLive;
+            a.tail_count = counts + 6;
+            nl = 2;
+        }
         if ((rc = done(launch_partition_search(a, s), "k_partition_search", 0))) return rc;
         if ((rc = done(launch_front(a, s), "k_front", 1))) return rc;
-        if ((rc = done(launch_refine(a, s), "k_refine", 2))) return rc;
+        {
+            cudaError_t e = launch_refine(a, s);
+            if (e == cudaSuccess && a.tail) e = launch_refine_tail(a, s);
+            if ((rc = done(e, "k_refine", 2, nl))) return rc;
+        }
         if ((rc = done(launch_select_pack(a, s), "k_select_pack", 3))) return rc;
         if (ext) { CK(launch_extend(a, ext, s), "k_extend"); ni++; }
-        if (launches) *launches += ni;
+        if (launches) *launches += ni + (nl - 1);
         return ASTCB200_OK;
     }
     const Pruning pr = resolve_pruning(ctx->pruning, ft->L.T);
