@@ -81,7 +81,7 @@ inline Pruning resolve_pruning(const Pruning& p, int T) {
     if (!r.kbm) r.kbm = small ? 8 : 4;
     if (!r.topn) r.topn = small ? 8 : 3;
     if (!r.refine_iters) r.refine_iters = 6;
-    if (!r.fallback_iters) r.fallback_iters = small ? 6 : 3;
+    if (!r.fallback_iters) r.fallback_iters = 3;
     return r;
 }
 

@@ -479,13 +479,13 @@ def run_settings(args):
 
 # ---------------------------------------------------------------- B200 arm
 # The library's tuned per-footprint proposal settings (astcb200_pruning zeros): for 4x4, 8
-# partitionings, 8 block modes per partition count, 8 candidates, 6 iterations (6 in the
+# partitionings, 8 block modes per partition count, 8 candidates, 6 iterations (3 in the
 # fallback); for 6x6, 3 partitionings, 4 block modes, 3 candidates, 6 iterations (3 in the
 # fallback); coverage 0.8, threshold 0.5, reroute above 8.  Chosen on held-out seeds 7-10
 # (this workload encodes seeds 1-4) as the fastest within 0.1 dB mean of the FIXED full
 # search with no image losing more.
 PRUNING = dict(coverage=0.8, threshold=0.5, reroute_error=8.0)
-TUNED = {"4x4": dict(max_partitionings=8, block_modes=8, refine_candidates=8, refine_iterations=6, fallback_iterations=6),
+TUNED = {"4x4": dict(max_partitionings=8, block_modes=8, refine_candidates=8, refine_iterations=6, fallback_iterations=3),
          "6x6": dict(max_partitionings=3, block_modes=4, refine_candidates=3, refine_iterations=6, fallback_iterations=3)}
 CHUNK = 262144  # blocks per launch sequence: one chunk per 2048x2048 image
 

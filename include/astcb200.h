@@ -217,7 +217,7 @@ int astcb200_set_proposal_net(astcb200_ctx* ctx, const astcb200_proposal_net* ne
  * fallback_iterations selects the footprint's tuned value, chosen on held-out synthetic
  * textures as the fastest setting within 0.1 dB mean PSNR of the full search with FIXED
  * semantics, no image losing more (with coverage 0.8): for blocks of up to 16 texels 8, 8,
- * 8, 6 and 6; for larger blocks 3, 4, 3, 6 and 3. */
+ * 8, 6 and 3; for larger blocks 3, 4, 3, 6 and 3. */
 typedef struct astcb200_pruning {
     uint32_t struct_size;
     uint32_t enable;            /* 0: full search everywhere */

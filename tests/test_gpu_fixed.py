@@ -118,7 +118,7 @@ def test_batch_fixed_equals_single_images():
     enc.close()
 
 
-@pytest.mark.parametrize("bx,by,topn,iters,fb", [(4, 4, 8, 6, 6), (6, 6, 3, 6, 3)])
+@pytest.mark.parametrize("bx,by,topn,iters,fb", [(4, 4, 8, 6, 3), (6, 6, 3, 6, 3)])
 def test_proposal_search_fixed_bit_exact_against_restricted_oracle(bx, by, topn, iters, fb):
     """The proposal search with FIXED semantics and the footprint's tuned settings: every
     proposal-search block equals the FIXED oracle restricted to the GPU's selection; every

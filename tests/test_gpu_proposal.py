@@ -179,7 +179,7 @@ def full_oracle(img, bx, by, iters=6):
 
 
 @pytest.mark.parametrize("bx,by,net_kind,prune", [
-    (4, 4, "shipped", dict(topn=8, iters=6, fb=6)),  # the tuned settings of 4x4 (all zeros: defaults)
+    (4, 4, "shipped", dict(topn=8, iters=6, fb=3)),  # the tuned settings of 4x4 (all zeros: defaults)
     (6, 6, "shipped", dict(topn=3, iters=6, fb=3)),  # and of 6x6
     (6, 6, "shipped", dict(max_partitionings=4, block_modes=16, refine_candidates=2, refine_iterations=3,
                            fallback_iterations=3, coverage=0.98, topn=2, iters=3, fb=3)),
