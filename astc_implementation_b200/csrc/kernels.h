@@ -90,6 +90,7 @@ struct KernelArgs {
     const uint32_t* pb_list;
     const int* pb_count;
     int pb_stride;
+    int pb_from, pb_to;       // the lists a launch takes: [pb_from, pb_to), pb_to 0 = up to the last
     // Work counters (null: not counted): [0..3] partitioned blocks searched by the front,
     // by P; [4] decimation modes and [5] block modes it evaluated; [6..9] candidates
     // refined, by P; [10..12] partition searches, P = 2..4; [13] candidates the refinement
@@ -131,11 +132,15 @@ __device__ __forceinline__ int list_blocks(const KernelArgs& a) {
 
 // Partitioned blocks of the proposal pass, and item i's list position and slot.
 __device__ __forceinline__ int pb_total(const KernelArgs& a) {
-    return a.pb_count[0] + a.pb_count[1] + a.pb_count[2] + a.pb_count[3];
+    const int to = a.pb_to ? a.pb_to : 4;
+    int n = 0;
+    for (int p = a.pb_from; p < to; p++) n += a.pb_count[p];
+    return n;
 }
 __device__ __forceinline__ void pb_item(const KernelArgs& a, int i, int& lb, int& slot) {
-    int p = 0;
-    while (p < 3 && i >= a.pb_count[p]) { i -= a.pb_count[p]; p++; }
+    const int last = (a.pb_to ? a.pb_to : 4) - 1;
+    int p = a.pb_from;
+    while (p < last && i >= a.pb_count[p]) { i -= a.pb_count[p]; p++; }
     const uint32_t v = a.pb_list[(size_t)p * a.pb_stride + i];
     lb = (int)(v >> 5);
     slot = (int)(v & 31);

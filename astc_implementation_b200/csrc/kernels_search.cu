@@ -739,9 +739,12 @@ __device__ __noinline__ void pass07_all_modes(const Tabs& tb, int T, int P, int 
     }
 }
 
-template <int NT>
-__device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, int slot_in_block, uint32_t entry, uint8_t* sm) {
+// P1: the instance for partitioned blocks of one partition only (the proposal pass's P = 1
+// list), with P a constant the compiler folds into every loop bound and branch.
+template <int NT, bool P1>
+__device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk, int slot_in_block, uint32_t entry, uint8_t* sm) {
     constexpr int kFrontThreads = NT, kFrontWarps = NT / 32;
+    const int P = P1 ? 1 : P_arg;
     const Tabs tb{a.tables, &a.L};
     const int T = a.L.T, ndm = a.L.ndm, nbm = a.L.nbm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1256,7 +1259,7 @@ __device__ void front_body(const KernelArgs& a, const int P, int lb, int blk, in
 // Resident CTAs of 128 threads the register budget is sized for (the proposal search's
 // compact layout lets that many fit in shared memory for the small footprints).
 constexpr int kFrontMinBlocks128 = 8;
-template <int NT>
+template <int NT, bool P1>
 __global__ void __launch_bounds__(NT, kFrontMinBlocks128 * 128 / NT > 32 ? 32 : kFrontMinBlocks128 * 128 / NT) k_front(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     // Items: every slot of every block in slot-major order (co-resident CTAs work on the
@@ -1286,7 +1289,7 @@ __global__ void __launch_bounds__(NT, kFrontMinBlocks128 * 128 / NT > 32 ? 32 : 
             if (threadIdx.x == 0) { PBRec& rec = a.pbrec[(size_t)lb * a.slots + k]; rec.P = P; rec.ncand = 0; rec.entry = 0; rec.seed = 0; }
             continue;  // uniform across the CTA
         }
-        front_body<NT>(a, P, lb, blk, k, entry, smem);
+        front_body<NT, P1>(a, P, lb, blk, k, entry, smem);
         __syncthreads();  // the next item reuses shared memory
     }
 }
@@ -1299,13 +1302,12 @@ size_t front_smem_bytes(const TableLayout& L, int nt, bool list) { return (size_
 // front_bytes: the 128-thread layout, the largest of the three.
 cudaError_t configure_search_kernels(size_t search_bytes, size_t front_bytes) {
     cudaError_t e = cudaFuncSetAttribute(k_partition_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)search_bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
     // the largest shared-memory carveout: occupancy of the front is bounded by shared memory
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<128>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<64>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_front<32>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    for (auto f : {k_front<128, false>, k_front<64, false>, k_front<32, false>, k_front<128, true>, k_front<64, true>,
+                   k_front<32, true>}) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_bytes);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
     return e;
 }
 
@@ -1322,9 +1324,21 @@ cudaError_t launch_front(const KernelArgs& a, cudaStream_t s) {
     int grid = a.nblocks * a.slots;
     if (a.block_list) grid = std::min(grid, kListGridFront * (128 / nt));
     const size_t smem = front_smem_bytes(a.L, nt, a.bm_mask != nullptr);
-    if (nt == 32) k_front<32><<<grid, 32, smem, s>>>(a);
-    else if (nt == 64) k_front<64><<<grid, 64, smem, s>>>(a);
-    else k_front<128><<<grid, 128, smem, s>>>(a);
+    auto go = [&](const KernelArgs& k, bool p1) {
+        if (nt == 32) { if (p1) k_front<32, true><<<grid, 32, smem, s>>>(k); else k_front<32, false><<<grid, 32, smem, s>>>(k); }
+        else if (nt == 64) { if (p1) k_front<64, true><<<grid, 64, smem, s>>>(k); else k_front<64, false><<<grid, 64, smem, s>>>(k); }
+        else { if (p1) k_front<128, true><<<grid, 128, smem, s>>>(k); else k_front<128, false><<<grid, 128, smem, s>>>(k); }
+    };
+    if (a.pb_list && a.pb_from == 0 && a.pb_to == 0) {
+        // the proposal pass's work lists: P = 1 by its own instance, then P = 2..4
+        KernelArgs k1 = a, k2 = a;
+        k1.pb_from = 0; k1.pb_to = 1;
+        k2.pb_from = 1; k2.pb_to = 4;
+        go(k1, true);
+        go(k2, false);
+    } else {
+        go(a, false);
+    }
     return cudaGetLastError();
 }
 

@@ -185,7 +185,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
     CK(cudaMemsetAsync(counts, 0, mlp::kRouteCounters * sizeof(int), s), "reset route counters");
     if ((rc = done(mlp::launch_mlp_logits(a, nd->net, sc.logits, ctx->d_mlp_error, s), "k_mlp_logits", 0))) return rc;
     if ((rc = done(mlp::launch_select(a, nd->net, sc.logits, sel, r, s), "k_select", 0))) return rc;
-    if ((rc = done(launch_front(ap, s), "k_front", 1))) return rc;
+    if ((rc = done(launch_front(ap, s), "k_front", 1, 2))) return rc;  // the P = 1 list, then the others
     if ((rc = refine(ap, "k_refine"))) return rc;
     if ((rc = done(launch_select_pack(ap, s), "k_select_pack", 3))) return rc;
     if ((rc = done(launch_partition_search(af, s), "k_partition_search", 0))) return rc;
