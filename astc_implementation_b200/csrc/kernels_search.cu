@@ -764,6 +764,23 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
     float* qfs = reinterpret_cast<float*>(sm + fl.qf);
     FrontMisc& M = *reinterpret_cast<FrontMisc*>(sm + fl.misc);
     const float4 cw = chan_w();
+    // Partition bytes of texels t..t+3 (t a multiple of 4 below Tp) and of texel t < T.  With one
+    // partition they are known, 0 for the block's texels and 0xFF (no partition) for the
+    // padding ones, and are not read from shared memory.
+    auto tp4 = [&](int t) -> uint32_t {
+        if constexpr (P1) {
+            uint32_t q = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) q |= (t + j < T ? 0u : 0xFFu) << (8 * j);
+            return q;
+        } else {
+            return *reinterpret_cast<const uint32_t*>(tp + t);
+        }
+    };
+    auto tp1 = [&](int t) -> int {
+        if constexpr (P1) return 0;
+        else return tp[t];
+    };
 
     // Per-partition sums over the texels are taken in ascending texel order, as the
     // oracle does, by one lane per (partition, channel or term) over the whole block:
@@ -800,7 +817,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         int n = 0;
         for (int t = 0; t < Tp; t += 4) {
             const float4 x = *reinterpret_cast<const float4*>(v + t);
-            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const uint32_t q = tp4(t);
             const bool m0 = (int)(q & 0xFF) == gp, m1 = (int)((q >> 8) & 0xFF) == gp;
             const bool m2 = (int)((q >> 16) & 0xFF) == gp, m3 = (int)(q >> 24) == gp;
             s = s + (m0 ? x.x : 0.0f); s = s + (m1 ? x.y : 0.0f);
@@ -817,7 +834,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         float dd = 0.0f;
         for (int t = 0; t < Tp; t += 4) {
             const float4 x = *reinterpret_cast<const float4*>(v + t);
-            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const uint32_t q = tp4(t);
             const float p0 = fmaxf(x.x - avg_c, 0.0f), p1 = fmaxf(x.y - avg_c, 0.0f);
             const float p2 = fmaxf(x.z - avg_c, 0.0f), p3 = fmaxf(x.w - avg_c, 0.0f);
             dd = dd + ((int)(q & 0xFF) == gp ? p0 * p0 : 0.0f);
@@ -834,7 +851,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         __syncwarp();
         for (int t = lane; t < Tp; t += 32) {
             float pr = 0.0f;
-            if (t < T) { const int p = tp[t]; pr = dot4(px[t] - M.avg[p], M.dir[p]); }
+            if (t < T) { const int p = tp1(t); pr = dot4(px[t] - M.avg[p], M.dir[p]); }
             prj[t] = pr;
         }
         __syncwarp();
@@ -842,7 +859,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         float mn = 1e10f, mx = -1e10f;
         for (int t = 0; t < Tp; t += 4) {
             const float4 x = *reinterpret_cast<const float4*>(prj + t);
-            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const uint32_t q = tp4(t);
             if ((int)(q & 0xFF) == gp) { mn = fminf(mn, x.x); mx = fmaxf(mx, x.x); }
             if ((int)((q >> 8) & 0xFF) == gp) { mn = fminf(mn, x.y); mx = fmaxf(mx, x.y); }
             if ((int)((q >> 16) & 0xFF) == gp) { mn = fminf(mn, x.z); mx = fmaxf(mx, x.z); }
@@ -874,7 +891,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         float sum = 0.0f;
         for (int t = 0; t < Tp; t += 4) {
             const float4 vs = *reinterpret_cast<const float4*>(xs + t), vc = *reinterpret_cast<const float4*>(xc + t);
-            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const uint32_t q = tp4(t);
             sum = sum + (((int)(q & 0xFF) == p && vs.x - as > 0.0f) ? vc.x - ac : 0.0f);
             sum = sum + (((int)((q >> 8) & 0xFF) == p && vs.y - as > 0.0f) ? vc.y - ac : 0.0f);
             sum = sum + (((int)((q >> 16) & 0xFF) == p && vs.z - as > 0.0f) ? vc.z - ac : 0.0f);
@@ -896,7 +913,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
     const bool is_const = M.is_const != 0;
     const float ew = (((cw.x + cw.y) + cw.z) + cw.w) / 4.0f;
     for (int t = tid; t < T; t += kFrontThreads) {
-        const int p = tp[t];
+        const int p = tp1(t);
         const float span = fmaxf(M.mx[p] - M.mn[p], 1e-6f);
         iw[t] = clampf((prj[t] - M.mn[p]) / span, 0.0f, 1.0f);
         wes[t] = M.lsq[p] * ew;
@@ -958,7 +975,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
     for (int t = tid; t < Tp; t += kFrontThreads) {
         float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f, t4 = 0.0f;
         if (t < T) {
-            const int p = tp[t];
+            const int p = tp1(t);
             const float4 ub = M.axes[p][0], ua = M.axes[p][1], sb = M.axes[p][2], la = M.axes[p][3];
             const float4 lbv = normalize4(make_float4(1.0f, 1.0f, 1.0f, 0.0f));
             float4 rgb = px[t]; rgb.w = 0.0f;
@@ -998,7 +1015,7 @@ __device__ void front_body(const KernelArgs& a, const int P_arg, int lb, int blk
         float s = 0.0f;
         for (int t = 0; t < Tp; t += 4) {
             const float4 y = *reinterpret_cast<const float4*>(x + t);
-            const uint32_t q = *reinterpret_cast<const uint32_t*>(tp + t);
+            const uint32_t q = tp4(t);
             s = s + ((int)(q & 0xFF) == p ? y.x : 0.0f); s = s + ((int)((q >> 8) & 0xFF) == p ? y.y : 0.0f);
             s = s + ((int)((q >> 16) & 0xFF) == p ? y.z : 0.0f); s = s + ((int)(q >> 24) == p ? y.w : 0.0f);
         }
