@@ -101,7 +101,8 @@ struct KernelArgs {
     int fixed;                // 1: FIXED semantics (ASTCB200_FLAG_FIXED_SEMANTICS), 0: the reference's
     // Refinement tail (null: off): once a refinement CTA has at most spill_live candidates
     // left, it writes their state here (kTailWords uint4 each, up to tail_cap entries,
-    // *tail_count reserved so far) and takes its next group; k_refine_tail finishes them.
+    // tail_count[0] reserved so far) and takes its next group; k_refine_tail finishes them,
+    // claiming entries from tail_count[1] (zero at its launch).
     uint4* tail;
     int* tail_count;
     int tail_cap;

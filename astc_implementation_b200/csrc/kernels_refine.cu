@@ -797,8 +797,14 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
 
 // The candidates k_refine handed over, one per thread with its own staged texels (RGBA8
 // through the table of src_texel's values, so every texel value is the same), iterated
-// with the same gathering of live candidates onto the lowest threads.
+// with the same gathering of live candidates onto the lowest threads.  The CTAs stay
+// resident: a CTA's 128 slots are refilled whenever at most kTailRefillAt of them hold a
+// live candidate, each warp claiming list entries for its own free slots from
+// tail_count[1], and the new candidates join the live list behind the running ones.  (A CTA
+// that finished fixed batches of 128 entries held its SM until its slowest candidate of
+// each batch ended.)
 constexpr int kTailCtas = 4;
+constexpr int kTailRefillAt = 64;
 __global__ void __launch_bounds__(kRefineThreads, kTailCtas) k_refine_tail(const __grid_constant__ KernelArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int T = a.L.T;
@@ -807,61 +813,99 @@ __global__ void __launch_bounds__(kRefineThreads, kTailCtas) k_refine_tail(const
     uchar4* pxs = reinterpret_cast<uchar4*>(smem + sizeof(CandSmem) * kRefineThreads + 256 * 4);
     uint8_t* tps = reinterpret_cast<uint8_t*>(pxs + kRefineThreads * T);
     int* keys = reinterpret_cast<int*>(tps + ((kRefineThreads * T + 15) & ~15));
-    int* next_it = keys + kRefineThreads;                                  // by position
-    uint32_t* pbi_of = reinterpret_cast<uint32_t*>(next_it + kRefineThreads);  // by position
+    int* next_it = keys + kRefineThreads;                                  // by slot
+    uint32_t* pbi_of = reinterpret_cast<uint32_t*>(next_it + kRefineThreads);  // by slot
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __shared__ int live_in_warp[kRefineThreads / 32];
+    const unsigned below = (1u << lane) - 1u;
+    __shared__ int live_in_warp[kRefineThreads / 32], new_in_warp[kRefineThreads / 32];
+    __shared__ uint8_t busy[kRefineThreads];  // slot holds a candidate that has not ended
+    __shared__ int dry_flag;                  // the list has no unclaimed entry left
     for (int v = tid; v < 256; v += kRefineThreads) lut[v] = ((float)v / 255.0f) * 65536.0f;  // as src_texel
+    busy[tid] = 0;
+    if (tid == 0) dry_flag = 0;
     const int total = min(*a.tail_count, a.tail_cap);
+    int* claim = a.tail_count + 1;
     const int iters = a.refine_iters > 0 ? a.refine_iters : 6;
-    for (int b0 = blockIdx.x * kRefineThreads; b0 < total; b0 += gridDim.x * kRefineThreads) {
-        int cand = -1;
-        if (b0 + tid < total) {
-            const uint4* e = a.tail + (size_t)(b0 + tid) * kTailWords;
-            const uint4 h = e[0];
-            if (h.x != 0xFFFFFFFFu) {
-                const int lb = (int)(h.x / (uint32_t)a.slots);
-                const PBRec& r = a.pbrec[h.x];
-                const int P = (int)r.P;
-                const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
-                const BlockSrc src = block_src(a, chunk_block(a, lb));
-                for (int t = 0; t < T; t++) {
-                    pxs[tid * T + t] = src_rgba8(src, a.L.bx, t);
-                    tps[tid * T + t] = P > 1 ? prow[t] : 0;
-                }
-                uint8_t* ep = reinterpret_cast<uint8_t*>(cs[tid].ep);
-                for (int i = 0; i < 8; i++) st_u4(ep + 16 * i, e[1 + i]);
-                for (int i = 0; i < 4; i++) st_u4(cs[tid].qw + 16 * i, e[9 + i]);
-                cs[tid].item = h.y & 0xFF;  // the candidate
-                next_it[tid] = (int)((h.y >> 8) & 0xFF);
-                pbi_of[tid] = h.x;
-                cand = tid;
-            }
+    int cand = -1;     // the slot whose candidate this thread runs
+    bool dry = false;  // CTA-uniform
+    for (;;) {
+        const bool live = cand >= 0;
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
+        if (lane == 0) live_in_warp[warp] = __popc(bal);
+        __syncthreads();  // also orders the last step's state writes and slot releases
+        int nlive = 0, before = 0;
+#pragma unroll
+        for (int w = 0; w < kRefineThreads / 32; w++) {
+            const int n = live_in_warp[w];
+            nlive += n;
+            before += w < warp ? n : 0;
         }
-        for (;;) {
-            const bool live = cand >= 0;
-            const unsigned bal = __ballot_sync(0xFFFFFFFFu, live);
-            if (lane == 0) live_in_warp[warp] = __popc(bal);
-            __syncthreads();  // also orders the staging and every earlier state write
-            int nlive = 0, before = 0;
+        int nnew = 0, new_before = 0, staged = -1;
+        unsigned bnew = 0;
+        if (!dry && nlive <= kTailRefillAt) {
+            // Thread tid stages into slot tid when that slot is free and its warp's claim
+            // reached an entry for it.
+            const bool fr = busy[tid] == 0;
+            const unsigned fb = __ballot_sync(0xFFFFFFFFu, fr);
+            const int nfree = __popc(fb);
+            int base = 0;
+            if (lane == 0 && nfree > 0) base = atomicAdd(claim, nfree);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (lane == 0 && nfree > 0 && base + nfree >= total) dry_flag = 1;
+            const int idx = base + __popc(fb & below);
+            if (fr && idx < total) {
+                const uint4* e = a.tail + (size_t)idx * kTailWords;
+                const uint4 h = e[0];
+                if (h.x != 0xFFFFFFFFu) {
+                    const int lb = (int)(h.x / (uint32_t)a.slots);
+                    const PBRec& r = a.pbrec[h.x];
+                    const int P = (int)r.P;
+                    const uint8_t* prow = P > 1 ? a.tables + a.L.off_part_texel + ((size_t)(P - 2) * 1024 + r.entry) * T : nullptr;
+                    const BlockSrc src = block_src(a, chunk_block(a, lb));
+                    for (int t = 0; t < T; t++) {
+                        pxs[tid * T + t] = src_rgba8(src, a.L.bx, t);
+                        tps[tid * T + t] = P > 1 ? prow[t] : 0;
+                    }
+                    uint8_t* ep = reinterpret_cast<uint8_t*>(cs[tid].ep);
+                    for (int i = 0; i < 8; i++) st_u4(ep + 16 * i, e[1 + i]);
+                    for (int i = 0; i < 4; i++) st_u4(cs[tid].qw + 16 * i, e[9 + i]);
+                    cs[tid].item = h.y & 0xFF;  // the candidate
+                    next_it[tid] = (int)((h.y >> 8) & 0xFF);
+                    pbi_of[tid] = h.x;
+                    busy[tid] = 1;
+                    staged = tid;
+                }
+            }
+            bnew = __ballot_sync(0xFFFFFFFFu, staged >= 0);
+            if (lane == 0) new_in_warp[warp] = __popc(bnew);
+            __syncthreads();  // the staged slots, the new counts and the flag
 #pragma unroll
             for (int w = 0; w < kRefineThreads / 32; w++) {
-                const int n = live_in_warp[w];
-                nlive += n;
-                before += w < warp ? n : 0;
+                const int n = new_in_warp[w];
+                nnew += n;
+                new_before += w < warp ? n : 0;
             }
-            if (nlive == 0) break;
-            if (live) keys[before + __popc(bal & ((1u << lane) - 1u))] = cand;
-            __syncthreads();
-            cand = tid < nlive ? keys[tid] : -1;
-            if (cand >= 0) {
-                const uint32_t pbi = pbi_of[cand];
-                const int k = (int)cs[cand].item, it = next_it[cand];
-                const PBRec& rec = a.pbrec[pbi];
-                Snap* snap = &a.snaps[(size_t)pbi * kNumCand + k];
-                const bool moved = refine_step(a, rec, (int)rec.P, k, TexelRow<true>{pxs + cand * T, lut}, tps + cand * T, cs[cand], snap, it);
-                next_it[cand] = it + 1;
-                if (!moved || it + 1 >= iters) cand = -1;
+            dry = dry_flag != 0;
+        }
+        const int n = nlive + nnew;
+        if (n == 0) {
+            if (dry) break;
+            continue;  // every claimed entry was a reservation left empty: claim again
+        }
+        if (live) keys[before + __popc(bal & below)] = cand;
+        if (staged >= 0) keys[nlive + new_before + __popc(bnew & below)] = staged;
+        __syncthreads();
+        cand = tid < n ? keys[tid] : -1;
+        if (cand >= 0) {
+            const uint32_t pbi = pbi_of[cand];
+            const int k = (int)cs[cand].item, it = next_it[cand];
+            const PBRec& rec = a.pbrec[pbi];
+            Snap* snap = &a.snaps[(size_t)pbi * kNumCand + k];
+            const bool moved = refine_step(a, rec, (int)rec.P, k, TexelRow<true>{pxs + cand * T, lut}, tps + cand * T, cs[cand], snap, it);
+            next_it[cand] = it + 1;
+            if (!moved || it + 1 >= iters) {
+                busy[cand] = 0;  // released: read by the next refill, after the next barrier
+                cand = -1;
             }
         }
     }

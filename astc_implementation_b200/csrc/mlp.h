@@ -103,7 +103,7 @@ struct Routes {
     int pb_stride;
 };
 
-constexpr int kRouteCounters = 8;  // ints per chunk: routes, partitioned-block counts, refinement-tail entries, padding
+constexpr int kRouteCounters = 8;  // ints per chunk: routes, partitioned-block counts, refinement-tail entries and claims
 // Textures of fewer texels take the (reference's) full search even with a network: their
 // blocks are mostly edge-clamped copies of a few texels, unlike what the networks learned
 // from, and searching them fully costs next to nothing.

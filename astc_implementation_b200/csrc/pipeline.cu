@@ -106,7 +106,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
             a.tail = sc.tail;
             a.tail_cap = (int)std::min<size_t>(sc.cap_tail / (kTailWords * sizeof(uint4)), (size_t)1 << 30);
             a.spill_live = kSpillLive;
-            a.tail_count = counts + 6;
+            a.tail_count = counts + 6;  // and its claim counter, counts[7]
             nl = 2;
         }
         if ((rc = done(launch_partition_search(a, s), "k_partition_search", 0))) return rc;
@@ -172,7 +172,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         ap.tail = sc.tail;
         ap.tail_cap = (int)std::min<size_t>(sc.cap_tail / (kTailWords * sizeof(uint4)), (size_t)1 << 30);
         ap.spill_live = kSpillLive;
-        ap.tail_count = counts + 6;  // a free route counter
+        ap.tail_count = counts + 6;  // two free route counters: reservations, claims
     }
     int tails = 0;  // tail launches (timed with their pass's refinement)
     auto refine = [&](const KernelArgs& k, const char* what) -> int {
