@@ -42,9 +42,10 @@ struct Scratch {
 // Refinement-tail entries per block of a chunk (a CTA that finds the tail full finishes its
 // candidates itself), and the live candidates at or below which a refinement CTA hands
 // them to the tail.
-constexpr size_t kTailPerBlock = 4;       // proposal search (about 1.5 spilled per 4x4 block)
+constexpr size_t kTailPerBlock = 4;       // proposal search (about 2.5 spilled per 4x4 block)
 constexpr size_t kTailPerBlockFull = 16;  // full search (104 candidates per block)
-constexpr int kSpillLive = 32;
+constexpr int kSpillLive = 32;            // full search
+constexpr int kSpillLiveProposal = 64;    // proposal pass
 
 // A footprint's proposal network on the device.
 struct NetDev {

@@ -171,7 +171,7 @@ int enqueue_chunk(astcb200_ctx* ctx, const KernelArgs& base, const FootTables* f
         // kernel would only lengthen.
         ap.tail = sc.tail;
         ap.tail_cap = (int)std::min<size_t>(sc.cap_tail / (kTailWords * sizeof(uint4)), (size_t)1 << 30);
-        ap.spill_live = kSpillLive;
+        ap.spill_live = kSpillLiveProposal;
         ap.tail_count = counts + 6;  // two free route counters: reservations, claims
     }
     int tails = 0;  // tail launches (timed with their pass's refinement)
