@@ -800,9 +800,8 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_refine(const __grid_const
 // with the same gathering of live candidates onto the lowest threads.  The CTAs stay
 // resident: a CTA's 128 slots are refilled whenever at most kTailRefillAt of them hold a
 // live candidate, each warp claiming list entries for its own free slots from
-// tail_count[1], and the new candidates join the live list behind the running ones.  (A CTA
-// that finished fixed batches of 128 entries held its SM until its slowest candidate of
-// each batch ended.)
+// tail_count[1], and the new candidates join the live list behind the running ones.  (Fixed
+// batches of 128 entries would hold each CTA until the slowest candidate of its batch ended.)
 constexpr int kTailCtas = 4;
 constexpr int kTailRefillAt = 64;
 __global__ void __launch_bounds__(kRefineThreads, kTailCtas) k_refine_tail(const __grid_constant__ KernelArgs a) {
