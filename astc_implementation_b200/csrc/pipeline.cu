@@ -22,6 +22,10 @@ using namespace astcb200;
 
 namespace astcb200 {
 
+// A chunk's route counters: [0, 1] routes, [2, 5] partitioned blocks by P, [6] refinement-tail
+// entries reserved, [7] entries claimed by k_refine_tail.
+static_assert(mlp::kRouteCounters >= 8, "the refinement tail uses route counters 6 and 7");
+
 const NetDev* net_for(const astcb200_ctx* ctx, const FootTables* ft) {
     if (!ctx->pruning.enable) return nullptr;
     for (const NetDev* n : ctx->nets)
